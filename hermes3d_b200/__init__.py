@@ -1,0 +1,17 @@
+"""B200-native hp-FEM hexahedral assembly with the Hermes3D call surface.
+
+Host objects (Mesh, H1Space, Discretization) run their one-time set-up in
+C++ (libh3dg.so); assembly runs as sm_100a kernels.  See include/h3dg.h for
+the C ABI.
+"""
+from . import _capi
+from .discretization import (BC_ESSENTIAL, BC_NATURAL, BC_NONE, Discretization, H1Space, UMFPackMatrix,
+                             UMFPackVector, UnsupportedForm, int_F_v, int_grad_u_grad_v,
+                             int_grad_u_grad_v_plus_u_v)
+from .mesh import Mesh, load_mesh3d, permute_vertices, unit_cube
+
+__all__ = [
+    "Mesh", "load_mesh3d", "unit_cube", "permute_vertices", "H1Space", "Discretization", "UMFPackMatrix",
+    "UMFPackVector", "int_grad_u_grad_v", "int_grad_u_grad_v_plus_u_v", "int_F_v", "UnsupportedForm",
+    "BC_ESSENTIAL", "BC_NATURAL", "BC_NONE",
+]

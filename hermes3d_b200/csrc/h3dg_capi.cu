@@ -1,0 +1,534 @@
+// C-ABI implementation: handles, device plan, kernel dispatch.
+#include "../../include/h3dg.h"
+#include "host/h3dg_host.h"
+#include "host/lobatto.h"
+#include "kernels/asm_fp64.cuh"
+#include "kernels/geom.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+struct h3dg_mesh {
+	h3dg::Mesh m;
+};
+
+struct h3dg_space {
+	h3dg_mesh *mesh = nullptr;
+	h3dg::Space s;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+h3dg_status fail(h3dg_status s, const std::string &msg) {
+	g_err = msg;
+	return s;
+}
+
+#define H3DG_CUDA_TRY(call)                                                                              \
+	do {                                                                                                 \
+		cudaError_t e_ = (call);                                                                         \
+		if (e_ != cudaSuccess) return fail(H3DG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+	} while (0)
+
+template <class T>
+struct DBuf {
+	T *p = nullptr;
+	size_t n = 0;
+	~DBuf() { release(); }
+	void release() {
+		if (p) cudaFree(p);
+		p = nullptr;
+		n = 0;
+	}
+	cudaError_t alloc(size_t count) {
+		release();
+		n = count;
+		if (count == 0) return cudaSuccess;
+		return cudaMalloc((void **) &p, sizeof(T) * count);
+	}
+	cudaError_t upload(const std::vector<T> &v) {
+		cudaError_t e = alloc(v.size());
+		if (e != cudaSuccess || v.empty()) return e;
+		return cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+	}
+};
+
+} // namespace
+
+struct h3dg_disc {
+	int device = 0;
+	h3dg_space *space = nullptr;
+	int bf = 0;
+	std::vector<double> ecoef;       // per element id
+	int lf = H3DG_LF_NONE;
+	double lf_value = 0.0;
+	int qmode = H3DG_QUAD_FIXED, qn = 0;
+	bool have_plan = false;
+	bool on_device = false;
+	h3dg::Plan plan;
+	int32_t last_launches = 0;
+
+	// device plan
+	DBuf<double> xyz, coef, tables, qx, qy, qz, Ax, rhs;
+	DBuf<int64_t> Ap;
+	DBuf<int32_t> Ai, el_vtx, el_cnt, el_dof, el_id;
+	DBuf<uint16_t> el_s, el_off;
+	DBuf<double> el_coef;
+	DBuf<int> status;
+	int table_bytes = 0;
+	double *h_pin_scratch = nullptr;
+};
+
+extern "C" {
+
+int h3dg_version(void) { return 1; }
+
+const char *h3dg_status_string(h3dg_status s) {
+	switch (s) {
+		case H3DG_OK: return "ok";
+		case H3DG_ERR_INVALID_ARG: return "invalid argument";
+		case H3DG_ERR_CUDA: return "CUDA error";
+		case H3DG_ERR_OUT_OF_MEMORY: return "out of memory";
+		case H3DG_ERR_UNSUPPORTED_FORM: return "unsupported form";
+		case H3DG_ERR_MESH: return "mesh error";
+		case H3DG_ERR_STATE: return "call out of order";
+		case H3DG_ERR_TIMEOUT: return "device wait timed out";
+		case H3DG_ERR_TOO_LARGE: return "size limit exceeded";
+		default: return "unknown status";
+	}
+}
+
+const char *h3dg_last_error(void) { return g_err.c_str(); }
+
+// ---------------------------------------------------------------- mesh
+
+h3dg_status h3dg_mesh_create(h3dg_mesh **mesh) {
+	if (!mesh) return fail(H3DG_ERR_INVALID_ARG, "mesh: null output pointer");
+	*mesh = new (std::nothrow) h3dg_mesh();
+	return *mesh ? H3DG_OK : fail(H3DG_ERR_OUT_OF_MEMORY, "mesh: allocation failed");
+}
+
+h3dg_status h3dg_mesh_destroy(h3dg_mesh *mesh) {
+	delete mesh;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_mesh_add_vertices(h3dg_mesh *mesh, const double *xyz, int64_t n) {
+	if (!mesh || (n > 0 && !xyz) || n < 0) return fail(H3DG_ERR_INVALID_ARG, "add_vertices: bad arguments");
+	if (mesh->m.finalized) return fail(H3DG_ERR_STATE, "add_vertices: mesh already finalized");
+	mesh->m.xyz.insert(mesh->m.xyz.end(), xyz, xyz + 3 * n);
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_mesh_add_hexes(h3dg_mesh *mesh, const int64_t *vtx, int64_t n) {
+	if (!mesh || (n > 0 && !vtx) || n < 0) return fail(H3DG_ERR_INVALID_ARG, "add_hexes: bad arguments");
+	if (mesh->m.finalized) return fail(H3DG_ERR_STATE, "add_hexes: mesh already finalized");
+	for (int64_t i = 0; i < 8 * n; i++) mesh->m.hex.push_back(vtx[i] - 1);
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_mesh_add_quad_boundaries(h3dg_mesh *mesh, const int64_t *vtx, const int32_t *marker, int64_t n) {
+	if (!mesh || (n > 0 && (!vtx || !marker)) || n < 0) return fail(H3DG_ERR_INVALID_ARG, "add_quad_boundaries: bad arguments");
+	if (mesh->m.finalized) return fail(H3DG_ERR_STATE, "add_quad_boundaries: mesh already finalized");
+	for (int64_t i = 0; i < n; i++) {
+		mesh->m.bquad.push_back({ vtx[4 * i] - 1, vtx[4 * i + 1] - 1, vtx[4 * i + 2] - 1, vtx[4 * i + 3] - 1 });
+		mesh->m.bmarker.push_back(marker[i]);
+	}
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_mesh_finalize(h3dg_mesh *mesh) {
+	if (!mesh) return fail(H3DG_ERR_INVALID_ARG, "finalize: null mesh");
+	std::string err;
+	if (mesh->m.finalize(err) != 0) return fail(H3DG_ERR_MESH, err);
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_mesh_counts(const h3dg_mesh *mesh, int64_t *nv, int64_t *ne, int64_t *nfacets, int64_t *nedges) {
+	if (!mesh) return fail(H3DG_ERR_INVALID_ARG, "counts: null mesh");
+	if (nv) *nv = mesh->m.nv();
+	if (ne) *ne = mesh->m.ne();
+	if (nfacets) *nfacets = mesh->m.nfacets;
+	if (nedges) *nedges = mesh->m.nedges;
+	return H3DG_OK;
+}
+
+// ---------------------------------------------------------------- space
+
+h3dg_status h3dg_space_create(h3dg_mesh *mesh, h3dg_space **space) {
+	if (!mesh || !space) return fail(H3DG_ERR_INVALID_ARG, "space_create: bad arguments");
+	if (!mesh->m.finalized) return fail(H3DG_ERR_STATE, "space_create: mesh not finalized");
+	h3dg_space *s = new (std::nothrow) h3dg_space();
+	if (!s) return fail(H3DG_ERR_OUT_OF_MEMORY, "space_create: allocation failed");
+	s->mesh = mesh;
+	s->s.mesh = &mesh->m;
+	*space = s;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_space_destroy(h3dg_space *space) {
+	delete space;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_space_set_bc_types(h3dg_space *space, h3dg_bc_type_fn fn, void *ctx) {
+	if (!space) return fail(H3DG_ERR_INVALID_ARG, "set_bc_types: null space");
+	space->s.bc_type_fn = fn;
+	space->s.bc_type_ctx = ctx;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_space_set_bc_values(h3dg_space *space, h3dg_bc_value_fn fn, void *ctx) {
+	if (!space) return fail(H3DG_ERR_INVALID_ARG, "set_bc_values: null space");
+	space->s.bc_value_fn = fn;
+	space->s.bc_value_ctx = ctx;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_space_set_uniform_order(h3dg_space *space, int px, int py, int pz) {
+	if (!space) return fail(H3DG_ERR_INVALID_ARG, "set_uniform_order: null space");
+	if (px < 1 || py < 1 || pz < 1 || px > h3dg::kMaxOrder || py > h3dg::kMaxOrder || pz > h3dg::kMaxOrder)
+		return fail(H3DG_ERR_INVALID_ARG, "set_uniform_order: order out of range 1..10");
+	int64_t ne = space->s.mesh->ne();
+	space->s.order.resize(3 * ne);
+	for (int64_t e = 0; e < ne; e++) {
+		space->s.order[3 * e] = px;
+		space->s.order[3 * e + 1] = py;
+		space->s.order[3 * e + 2] = pz;
+	}
+	space->s.assigned = false;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_space_set_element_orders(h3dg_space *space, const int32_t *orders, int64_t ne) {
+	if (!space || !orders || ne != space->s.mesh->ne()) return fail(H3DG_ERR_INVALID_ARG, "set_element_orders: bad arguments");
+	for (int64_t i = 0; i < 3 * ne; i++)
+		if (orders[i] < 1 || orders[i] > h3dg::kMaxOrder) return fail(H3DG_ERR_INVALID_ARG, "set_element_orders: order out of range 1..10");
+	space->s.order.assign(orders, orders + 3 * ne);
+	space->s.assigned = false;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_space_assign_dofs(h3dg_space *space, int first_dof, int stride, int64_t *ndof) {
+	if (!space || stride < 1 || first_dof < 0) return fail(H3DG_ERR_INVALID_ARG, "assign_dofs: bad arguments");
+	std::string err;
+	if (space->s.assign_dofs(first_dof, stride, err) != 0) return fail(H3DG_ERR_STATE, "assign_dofs: " + err);
+	if (ndof) *ndof = space->s.ndof();
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_space_get_element_assembly_list(const h3dg_space *space, int64_t elem_id, int64_t *idx, int32_t *dof,
+                                                 double *coef, int32_t cap, int32_t *cnt) {
+	if (!space || !space->s.assigned) return fail(H3DG_ERR_STATE, "get_element_assembly_list: assign_dofs() first");
+	if (elem_id < 1 || elem_id > space->s.mesh->ne()) return fail(H3DG_ERR_INVALID_ARG, "get_element_assembly_list: element id out of range");
+	std::vector<h3dg::AsmEntry> al;
+	space->s.element_assembly_list(elem_id - 1, al);
+	if (cnt) *cnt = (int32_t) al.size();
+	for (int32_t i = 0; i < cap && i < (int32_t) al.size(); i++) {
+		if (idx) idx[i] = al[i].idx;
+		if (dof) dof[i] = al[i].dof;
+		if (coef) coef[i] = al[i].coef;
+	}
+	return H3DG_OK;
+}
+
+// ---------------------------------------------------------------- discretization
+
+h3dg_status h3dg_disc_create(h3dg_disc **disc, int device) {
+	if (!disc) return fail(H3DG_ERR_INVALID_ARG, "disc_create: null output pointer");
+	h3dg_disc *d = new (std::nothrow) h3dg_disc();
+	if (!d) return fail(H3DG_ERR_OUT_OF_MEMORY, "disc_create: allocation failed");
+	d->device = device;
+	*disc = d;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_destroy(h3dg_disc *disc) {
+	if (!disc) return H3DG_OK;
+	cudaSetDevice(disc->device);
+	delete disc;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_set_space(h3dg_disc *disc, h3dg_space *space) {
+	if (!disc || !space) return fail(H3DG_ERR_INVALID_ARG, "set_space: bad arguments");
+	disc->space = space;
+	disc->have_plan = false;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_set_bilinear_form(h3dg_disc *disc, int form, const double *elem_coef, int64_t ne) {
+	if (!disc) return fail(H3DG_ERR_INVALID_ARG, "set_bilinear_form: null disc");
+	if (form != H3DG_BF_GRAD_GRAD && form != H3DG_BF_GRAD_GRAD_MASS)
+		return fail(H3DG_ERR_UNSUPPORTED_FORM, "set_bilinear_form: only int_grad_u_grad_v and int_grad_u_grad_v + int_u_v run on the device");
+	disc->bf = form;
+	if (elem_coef) {
+		if (!disc->space || ne != disc->space->s.mesh->ne()) return fail(H3DG_ERR_INVALID_ARG, "set_bilinear_form: coefficient count != elements");
+		disc->ecoef.assign(elem_coef, elem_coef + ne);
+	}
+	else disc->ecoef.clear();
+	disc->have_plan = false;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_set_linear_form(h3dg_disc *disc, int form, double value) {
+	if (!disc) return fail(H3DG_ERR_INVALID_ARG, "set_linear_form: null disc");
+	if (form != H3DG_LF_NONE && form != H3DG_LF_CONST && form != H3DG_LF_SIN)
+		return fail(H3DG_ERR_UNSUPPORTED_FORM, "set_linear_form: unknown linear form");
+	disc->lf = form;
+	disc->lf_value = value;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_set_quadrature(h3dg_disc *disc, int mode, int n) {
+	if (!disc || (mode != H3DG_QUAD_FIXED && mode != H3DG_QUAD_P_PLUS) || n < 0 || n > h3dg::kMaxQuadPoints)
+		return fail(H3DG_ERR_INVALID_ARG, "set_quadrature: bad arguments");
+	disc->qmode = mode;
+	disc->qn = n;
+	disc->have_plan = false;
+	return H3DG_OK;
+}
+
+static void build_table_blob(const h3dg::Plan &P, std::vector<double> &blob) {
+	// layout of SfShape: Vx Dx Vy Dy Vz Dz, then qx wx qy wy qz wz; padded to 16 bytes
+	blob.clear();
+	auto put_dir = [&](int p, const std::vector<double> &q) {
+		for (int k = 0; k <= p; k++)
+			for (size_t i = 0; i < q.size(); i++) blob.push_back(h3dg::lobatto_value(k, q[i]));
+		for (int k = 0; k <= p; k++)
+			for (size_t i = 0; i < q.size(); i++) blob.push_back(h3dg::lobatto_deriv(k, q[i]));
+	};
+	put_dir(P.px, P.qx);
+	put_dir(P.py, P.qy);
+	put_dir(P.pz, P.qz);
+	blob.insert(blob.end(), P.qx.begin(), P.qx.end());
+	blob.insert(blob.end(), P.wx.begin(), P.wx.end());
+	blob.insert(blob.end(), P.qy.begin(), P.qy.end());
+	blob.insert(blob.end(), P.wy.begin(), P.wy.end());
+	blob.insert(blob.end(), P.qz.begin(), P.qz.end());
+	blob.insert(blob.end(), P.wz.begin(), P.wz.end());
+	if (blob.size() % 2) blob.push_back(0.0);
+}
+
+h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nnz) {
+	if (!disc || !disc->space) return fail(H3DG_ERR_STATE, "create_pattern: set_space() first");
+	if (!disc->space->s.assigned) return fail(H3DG_ERR_STATE, "create_pattern: assign_dofs() first");
+	if (!disc->bf) return fail(H3DG_ERR_STATE, "create_pattern: set_bilinear_form() first");
+	const h3dg::Space &sp = disc->space->s;
+	int nq[3];
+	for (int d = 0; d < 3; d++) nq[d] = disc->qmode == H3DG_QUAD_FIXED ? disc->qn : sp.order[d] + disc->qn;
+	std::string err;
+	if (h3dg::build_plan(sp, nq[0], nq[1], nq[2], disc->plan, err) != 0) return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
+	const h3dg::Plan &P = disc->plan;
+	disc->on_device = false;
+	disc->have_plan = true;
+	if (ndof) *ndof = P.ndof;
+	if (nnz) *nnz = P.nnz;
+	return H3DG_OK;
+}
+
+// Device copy of the plan, made on the first device call (create() itself
+// is host work, as in the reference).
+static h3dg_status ensure_device(h3dg_disc *disc) {
+	if (disc->on_device) return H3DG_OK;
+	const h3dg::Space &sp = disc->space->s;
+	const h3dg::Plan &P = disc->plan;
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	H3DG_CUDA_TRY(disc->xyz.upload(sp.mesh->xyz));
+	H3DG_CUDA_TRY(disc->Ap.upload(P.Ap));
+	H3DG_CUDA_TRY(disc->Ai.upload(P.Ai));
+	H3DG_CUDA_TRY(disc->el_vtx.upload(P.el_vtx));
+	H3DG_CUDA_TRY(disc->el_cnt.upload(P.el_cnt));
+	H3DG_CUDA_TRY(disc->el_s.upload(P.el_s));
+	H3DG_CUDA_TRY(disc->el_dof.upload(P.el_dof));
+	H3DG_CUDA_TRY(disc->el_coef.upload(P.el_coef));
+	H3DG_CUDA_TRY(disc->el_off.upload(P.el_off));
+	H3DG_CUDA_TRY(disc->el_id.upload(P.el_id));
+	std::vector<double> blob;
+	build_table_blob(P, blob);
+	disc->table_bytes = (int) (blob.size() * sizeof(double));
+	H3DG_CUDA_TRY(disc->tables.upload(blob));
+	H3DG_CUDA_TRY(disc->qx.upload(P.qx));
+	H3DG_CUDA_TRY(disc->qy.upload(P.qy));
+	H3DG_CUDA_TRY(disc->qz.upload(P.qz));
+	if (!disc->ecoef.empty()) H3DG_CUDA_TRY(disc->coef.upload(disc->ecoef));
+	else disc->coef.release();
+	H3DG_CUDA_TRY(disc->status.alloc(1));
+	H3DG_CUDA_TRY(cudaMemset(disc->status.p, 0, sizeof(int)));
+	disc->on_device = true;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_get_pattern(const h3dg_disc *disc, int64_t *Ap, int32_t *Ai) {
+	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "get_pattern: create_pattern() first");
+	if (Ap) std::memcpy(Ap, disc->plan.Ap.data(), sizeof(int64_t) * disc->plan.Ap.size());
+	if (Ai) std::memcpy(Ai, disc->plan.Ai.data(), sizeof(int32_t) * disc->plan.Ai.size());
+	return H3DG_OK;
+}
+
+} // extern "C"
+
+namespace {
+
+using KernelFn = void (*)(h3dg::KArgs, int64_t, int64_t);
+
+struct KernelSpec {
+	int p, nq;
+	KernelFn fn;
+	int threads;
+	size_t smem;
+};
+
+template <int P, int NQ, int NT>
+KernelSpec spec() {
+	return KernelSpec { P, NQ, &h3dg::k_assemble_fp64<P, P, P, NQ, NQ, NQ, NT>, NT, h3dg::SfShape<P, P, P, NQ, NQ, NQ>::SMEM_BYTES };
+}
+
+const std::vector<KernelSpec> &kernel_table() {
+	static std::vector<KernelSpec> t = {
+		spec<1, 2, 128>(), spec<1, 3, 128>(), spec<2, 3, 128>(), spec<2, 4, 128>(), spec<2, 5, 128>(),
+		spec<3, 4, 256>(), spec<3, 5, 256>(), spec<3, 6, 256>(),
+	};
+	return t;
+}
+
+} // namespace
+
+extern "C" {
+
+h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream) {
+	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "assemble: create_pattern() first");
+	if (precision != H3DG_PREC_FP64) return fail(H3DG_ERR_INVALID_ARG, "assemble: unknown precision");
+	const h3dg::Plan &P = disc->plan;
+	if (P.px != P.py || P.px != P.pz || P.nqx != P.nqy || P.nqx != P.nqz)
+		return fail(H3DG_ERR_INVALID_ARG, "assemble: anisotropic orders need the batched path");
+	const KernelSpec *ks = nullptr;
+	for (auto &k : kernel_table())
+		if (k.p == P.px && k.nq == P.nqx) ks = &k;
+	if (!ks) return fail(H3DG_ERR_INVALID_ARG, "assemble: no FP64 kernel instantiated for this order / rule");
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	cudaStream_t st = (cudaStream_t) stream;
+	h3dg::KArgs a;
+	a.xyz = disc->xyz.p;
+	a.el_vtx = disc->el_vtx.p;
+	a.el_cnt = disc->el_cnt.p;
+	a.el_s = disc->el_s.p;
+	a.el_dof = disc->el_dof.p;
+	a.el_coef = disc->el_coef.p;
+	a.el_off = disc->el_off.p;
+	a.el_id = disc->el_id.p;
+	a.ecoef = disc->coef.p;
+	a.Ap = disc->Ap.p;
+	a.tables = disc->tables.p;
+	a.table_bytes = disc->table_bytes;
+	a.mass = disc->bf == H3DG_BF_GRAD_GRAD_MASS;
+	a.lf = disc->lf;
+	a.lf_value = disc->lf_value;
+	a.Ax = d_Ax;
+	a.rhs = disc->lf ? d_rhs : nullptr;
+	a.status = disc->status.p;
+	if (d_Ax) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
+	if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
+	static int configured[64] = { 0 };
+	int kidx = (int) (ks - kernel_table().data());
+	if (!configured[kidx]) {
+		H3DG_CUDA_TRY(cudaFuncSetAttribute(ks->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) ks->smem));
+		configured[kidx] = 1;
+	}
+	int nsm = 148, per_sm = 1;
+	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks->fn, ks->threads, ks->smem);
+	if (per_sm < 1) per_sm = 1;
+	int32_t launches = 0;
+	for (int c = 0; c < P.ncolors; c++) {
+		int64_t kb = P.color_ptr[c], ke = P.color_ptr[c + 1];
+		if (ke <= kb) continue;
+		int64_t grid = std::min<int64_t>(ke - kb, (int64_t) nsm * per_sm);
+		ks->fn<<<(unsigned) grid, ks->threads, ks->smem, st>>>(a, kb, ke);
+		launches++;
+	}
+	H3DG_CUDA_TRY(cudaGetLastError());
+	disc->last_launches = launches;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_assemble_host(h3dg_disc *disc, int precision, double *Ax, double *rhs) {
+	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "assemble_host: create_pattern() first");
+	const h3dg::Plan &P = disc->plan;
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	if (Ax && disc->Ax.n != (size_t) P.nnz) H3DG_CUDA_TRY(disc->Ax.alloc(P.nnz));
+	if (rhs && disc->rhs.n != (size_t) P.ndof) H3DG_CUDA_TRY(disc->rhs.alloc(P.ndof));
+	h3dg_status s = h3dg_disc_assemble(disc, precision, Ax ? disc->Ax.p : nullptr, rhs ? disc->rhs.p : nullptr, nullptr);
+	if (s != H3DG_OK) return s;
+	if (Ax) H3DG_CUDA_TRY(cudaMemcpy(Ax, disc->Ax.p, sizeof(double) * P.nnz, cudaMemcpyDeviceToHost));
+	if (rhs) H3DG_CUDA_TRY(cudaMemcpy(rhs, disc->rhs.p, sizeof(double) * P.ndof, cudaMemcpyDeviceToHost));
+	int st = 0;
+	H3DG_CUDA_TRY(cudaMemcpy(&st, disc->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+	if (st) {
+		cudaMemset(disc->status.p, 0, sizeof(int));
+		return fail(H3DG_ERR_TIMEOUT, "assemble_host: a device wait gave up");
+	}
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_update_vertices(h3dg_disc *disc, const double *xyz, int64_t nv) {
+	if (!disc || !disc->have_plan || !xyz || nv != disc->space->s.mesh->nv())
+		return fail(H3DG_ERR_INVALID_ARG, "update_vertices: bad arguments or no plan");
+	{ h3dg_status s0 = ensure_device(disc); if (s0 != H3DG_OK) return s0; }
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	H3DG_CUDA_TRY(cudaMemcpy(disc->xyz.p, xyz, sizeof(double) * 3 * nv, cudaMemcpyHostToDevice));
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_update_coefficients(h3dg_disc *disc, const double *elem_coef, int64_t ne) {
+	if (!disc || !disc->have_plan || !elem_coef || ne != disc->plan.ne)
+		return fail(H3DG_ERR_INVALID_ARG, "update_coefficients: bad arguments or no plan");
+	{ h3dg_status s0 = ensure_device(disc); if (s0 != H3DG_OK) return s0; }
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	if (disc->coef.n != (size_t) ne) H3DG_CUDA_TRY(disc->coef.alloc(ne));
+	H3DG_CUDA_TRY(cudaMemcpy(disc->coef.p, elem_coef, sizeof(double) * ne, cudaMemcpyHostToDevice));
+	disc->ecoef.assign(elem_coef, elem_coef + ne);
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_last_launch_count(const h3dg_disc *disc, int32_t *count) {
+	if (!disc || !count) return fail(H3DG_ERR_INVALID_ARG, "last_launch_count: bad arguments");
+	*count = disc->last_launches;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_geometry(h3dg_disc *disc, double *d_jac, double *d_irm, double *d_xyz, void *stream) {
+	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "geometry: create_pattern() first");
+	const h3dg::Plan &P = disc->plan;
+	{ h3dg_status s0 = ensure_device(disc); if (s0 != H3DG_OK) return s0; }
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	h3dg::GeomArgs g;
+	g.xyz = disc->xyz.p;
+	g.el_vtx = disc->el_vtx.p;
+	g.el_id = disc->el_id.p;
+	g.qx = disc->qx.p;
+	g.qy = disc->qy.p;
+	g.qz = disc->qz.p;
+	g.nqx = P.nqx;
+	g.nqy = P.nqy;
+	g.nqz = P.nqz;
+	g.ne = P.ne;
+	g.jac = d_jac;
+	g.irm = d_irm;
+	g.xphys = d_xyz;
+	int64_t total = P.ne * (int64_t) P.nqx * P.nqy * P.nqz;
+	if (total == 0) return H3DG_OK;
+	h3dg::k_geometry<<<(unsigned) ((total + 255) / 256), 256, 0, (cudaStream_t) stream>>>(g);
+	H3DG_CUDA_TRY(cudaGetLastError());
+	disc->last_launches = 1;
+	return H3DG_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,141 @@
+// Host-side mesh, H1 Lobatto space and assembly plan.
+//
+// This is the part of the assembly path that runs once per mesh/space on
+// the CPU: topology, orientations, DOF numbering, Dirichlet lifting
+// coefficients, assembly lists, the CSC sparsity pattern and the per-element
+// tables the GPU kernels consume.  The numbering rules reproduce the
+// reference's bit for bit (checked against the reference itself by the
+// parity tests); each routine cites the reference code it follows.
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace h3dg {
+
+// ---------------------------------------------------------------- reference tables
+// RefHex (src/refdomain.cc:96-130)
+extern const int kHexEdgeVtx[12][2];
+extern const int kHexFaceVtx[6][4];
+extern const int kHexFaceEdges[6][4];
+extern const int kVertexXYZ[8][3];   // Lobatto vertex indices (h1lobattohex.cc:68-73)
+
+enum BcType { BC_ESSENTIAL = 0, BC_NATURAL = 1, BC_NONE = 2 };   // src/space.h:44-48
+constexpr int DIRICHLET_DOF = -1;                                  // src/common.h:187
+constexpr int MARKER_UNDEFINED = -1;
+
+enum ShfnType { SHFN_VERTEX = 0, SHFN_EDGE = 1, SHFN_FACE = 2, SHFN_BUBBLE = 3 };
+
+// h1_hex_index_t bit layout (src/shapeset/h1lobattohex.cc:36-65)
+inline int64_t encode_index(int type, int ef, int x, int y, int z, int ori) {
+	return ((int64_t) type << 19) | ((int64_t) ef << 15) | ((int64_t) ori << 12) | (x << 8) | (y << 4) | z;
+}
+
+// Decoded form of a shape index: tensor indices (a,b,c) of the canonical
+// basis L_a(xi) L_b(eta) L_c(zeta) and the sign that orientation flips
+// introduce (decompose(), h1lobattohex.cc:98-130; L_k(-x) = (-1)^k L_k(x)).
+struct Canon {
+	int a, b, c;
+	int sign;
+};
+Canon decode_index(int64_t idx);
+
+// ---------------------------------------------------------------- mesh
+struct Mesh {
+	// input (vertex and element ids are 1-based in the reference; stored 0-based here)
+	std::vector<double> xyz;                 // nv x 3
+	std::vector<int64_t> hex;                // ne x 8 (0-based vertex index, RefHex order)
+	std::vector<std::array<int64_t, 4>> bquad;
+	std::vector<int> bmarker;
+
+	// derived by finalize()
+	int64_t nfacets = 0, nedges = 0;
+	std::vector<int64_t> elem_face;          // ne x 6 -> facet id (creation order)
+	std::vector<int64_t> elem_edge;          // ne x 12 -> edge id
+	std::vector<int64_t> facet_left, facet_left_face, facet_right;  // right = -1 if none
+	std::vector<int> facet_outer;            // 1 if boundary facet
+	std::vector<int> facet_marker;           // boundary marker (outer facets)
+	std::vector<int> edge_bnd;
+	bool finalized = false;
+
+	int64_t nv() const { return (int64_t) xyz.size() / 3; }
+	int64_t ne() const { return (int64_t) hex.size() / 8; }
+
+	int finalize(std::string &err);
+	int edge_orientation(int64_t e, int iedge) const;
+	int face_orientation(int64_t e, int iface) const;
+};
+
+// ---------------------------------------------------------------- space
+typedef int (*BcTypeFn)(int marker, void *ctx);
+typedef double (*BcValueFn)(int marker, double x, double y, double z, void *ctx);
+
+struct AsmEntry {
+	int64_t idx;     // reference shape index (h1_hex_index_t encoding)
+	int dof;         // global DOF, or DIRICHLET_DOF
+	double coef;     // 1.0, or the Dirichlet lifting coefficient
+};
+
+struct Space {
+	const Mesh *mesh = nullptr;
+	std::vector<int> order;                  // ne x 3 element orders
+	BcTypeFn bc_type_fn = nullptr;
+	void *bc_type_ctx = nullptr;
+	BcValueFn bc_value_fn = nullptr;
+	void *bc_value_ctx = nullptr;
+
+	// node data (src/space.h:110-300)
+	struct VData { int bc = BC_NONE, marker = MARKER_UNDEFINED, dof = -2; double proj = 0.0; };
+	struct EData { int bc = BC_NONE, marker = MARKER_UNDEFINED, order = -1, dof = -2, n = -1; std::vector<double> proj; bool has_proj = false; };
+	struct FData { int bc = BC_NONE, marker = MARKER_UNDEFINED, ox = -1, oy = -1, dof = -2, n = -1; std::vector<double> proj; bool has_proj = false; };
+	struct BData { int dof = -2, n = -1; };
+	std::vector<VData> vd;
+	std::vector<EData> ed;
+	std::vector<FData> fd;
+	std::vector<BData> bd;
+	int first_dof = 0, next_dof = 0, stride = 1;
+	bool assigned = false;
+
+	int ndof() const { return (next_dof - first_dof) / stride; }
+	int assign_dofs(int first, int stride, std::string &err);
+	void element_assembly_list(int64_t e, std::vector<AsmEntry> &al) const;
+
+private:
+	void lift_edge(int64_t e, int iedge);
+	void lift_face(int64_t e, int iface);
+};
+
+// ---------------------------------------------------------------- assembly plan
+// Everything the device kernels need for one (space, quadrature) pair.
+struct Plan {
+	int64_t ne = 0, ndof = 0, nnz = 0;
+	int px = 0, py = 0, pz = 0;              // uniform element order of this plan
+	int nl = 0;                              // (px+1)(py+1)(pz+1)
+	int nqx = 0, nqy = 0, nqz = 0;           // Gauss points per direction
+
+	// CSC pattern, == Discretization::create + UMFPackMatrix::alloc
+	std::vector<int64_t> Ap;                 // ndof + 1
+	std::vector<int32_t> Ai;                 // nnz
+
+	// per element (assembly order), padded to nl entries
+	std::vector<int32_t> el_vtx;             // ne x 8
+	std::vector<int32_t> el_cnt;             // ne x 2: matrix entries m, lifting entries l
+	std::vector<uint16_t> el_s;              // ne x nl canonical index (a*(py+1)+b)*(pz+1)+c
+	std::vector<int32_t> el_dof;             // ne x nl
+	std::vector<double> el_coef;             // ne x nl (orientation sign x AsmList coef)
+	std::vector<uint16_t> el_off;            // ne x nl x nl: row position of dof_a in column dof_b
+	std::vector<int32_t> el_id;              // reference element id - 1 of each assembly slot
+
+	// element colouring: no two elements of a colour share a DOF
+	int ncolors = 0;
+	std::vector<int64_t> color_ptr;          // ncolors + 1 (ranges in assembly order)
+
+	// 1D tables (b): per direction, V[k][q] and D[k][q] (k <= p, q < nq) and rule
+	std::vector<double> qx, wx, qy, wy, qz, wz;
+};
+
+int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &plan, std::string &err);
+
+} // namespace h3dg

@@ -1,0 +1,253 @@
+"""Reference-shaped host API over the C ABI: H1Space, weak-form descriptors,
+Discretization, UMFPackMatrix / UMFPackVector.
+
+Mirrors src/space.h, src/space/h1.h, src/discretization.h and
+src/linsolver/umfpack.h of the reference: the same method names, argument
+meaning and call order (set_* -> assign_dofs -> create -> assemble).  The
+reference's forms are C function pointers evaluated on the CPU; here the
+stock forms of src/integrals/h1.h are named by descriptor objects and run
+on the GPU.  An unknown form raises UnsupportedForm; nothing falls back
+to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import _capi as capi
+
+BC_ESSENTIAL = capi.BC_ESSENTIAL
+BC_NATURAL = capi.BC_NATURAL
+BC_NONE = capi.BC_NONE
+
+
+class UnsupportedForm(capi.H3dgError):
+    pass
+
+
+class H1Space:
+    """H1 space on hexahedra with the hierarchical Lobatto shapeset
+    (H1Space + H1ShapesetLobattoHex, src/space/h1.h, src/shapeset/h1lobattohex.h)."""
+
+    def __init__(self, mesh):
+        if mesh.handle is None:
+            mesh.ugh()
+        self.mesh = mesh
+        h = C.c_void_p()
+        capi.call("h3dg_space_create", mesh.handle, C.byref(h))
+        self.handle = h
+        self._cb = []
+        self.ndof = None
+
+    def set_bc_types(self, fn: Optional[Callable[[int], int]]):
+        """Space::set_bc_types; fn(marker) -> BC_ESSENTIAL / BC_NATURAL / BC_NONE."""
+        if fn is None:
+            capi.call("h3dg_space_set_bc_types", self.handle, capi.BC_TYPE_FN(), None)
+            return
+        cb = capi.BC_TYPE_FN(lambda marker, ctx: int(fn(marker)))
+        self._cb.append(cb)
+        capi.call("h3dg_space_set_bc_types", self.handle, cb, None)
+
+    def set_bc_values(self, fn: Optional[Callable[[int, float, float, float], float]]):
+        """Space::set_bc_values; fn(marker, x, y, z) -> Dirichlet value."""
+        if fn is None:
+            capi.call("h3dg_space_set_bc_values", self.handle, capi.BC_VALUE_FN(), None)
+            return
+        cb = capi.BC_VALUE_FN(lambda marker, x, y, z, ctx: float(fn(marker, x, y, z)))
+        self._cb.append(cb)
+        capi.call("h3dg_space_set_bc_values", self.handle, cb, None)
+
+    def set_uniform_order(self, order):
+        px, py, pz = (order, order, order) if np.isscalar(order) else order
+        capi.call("h3dg_space_set_uniform_order", self.handle, int(px), int(py), int(pz))
+
+    def set_element_orders(self, orders):
+        o = np.ascontiguousarray(orders, dtype=np.int32).reshape(-1, 3)
+        capi.call("h3dg_space_set_element_orders", self.handle, capi.ptr(o, C.c_int32), len(o))
+
+    def assign_dofs(self, first_dof=0, stride=1):
+        n = C.c_int64()
+        capi.call("h3dg_space_assign_dofs", self.handle, int(first_dof), int(stride), C.byref(n))
+        self.ndof = n.value
+        return n.value
+
+    def get_dof_count(self):
+        return self.ndof
+
+    def get_element_assembly_list(self, elem_id):
+        """AsmList of element ``elem_id`` (1-based): (idx, dof, coef) arrays."""
+        cnt = C.c_int32()
+        capi.call("h3dg_space_get_element_assembly_list", self.handle, int(elem_id), None, None, None, 0, C.byref(cnt))
+        n = cnt.value
+        idx = np.zeros(n, np.int64)
+        dof = np.zeros(n, np.int32)
+        coef = np.zeros(n, np.float64)
+        capi.call("h3dg_space_get_element_assembly_list", self.handle, int(elem_id), capi.ptr(idx, C.c_int64),
+                  capi.ptr(dof, C.c_int32), capi.ptr(coef, C.c_double), n, C.byref(cnt))
+        return idx, dof, coef
+
+    def __del__(self):
+        if getattr(self, "handle", None) and capi._lib is not None:
+            capi.lib().h3dg_space_destroy(self.handle)
+            self.handle = None
+
+
+# ---------------------------------------------------------------- form descriptors
+
+@dataclass(frozen=True)
+class BilinearForm:
+    kind: int
+    name: str
+
+
+@dataclass(frozen=True)
+class LinearForm:
+    kind: int
+    value: float
+    name: str
+
+
+int_grad_u_grad_v = BilinearForm(capi.BF_GRAD_GRAD, "int_grad_u_grad_v")
+int_grad_u_grad_v_plus_u_v = BilinearForm(capi.BF_GRAD_GRAD_MASS, "int_grad_u_grad_v + int_u_v")
+
+
+def int_F_v(F):
+    """Linear form int F v for a constant F or F = "sin" (sin(pi x) sin(pi y) sin(pi z))."""
+    if isinstance(F, str) and F == "sin":
+        return LinearForm(capi.LF_SIN, 0.0, "int_F_v(sin)")
+    if np.isscalar(F):
+        return LinearForm(capi.LF_CONST, float(F), "int_F_v(%g)" % F)
+    raise UnsupportedForm(capi.H3DG_OK + 4, "only constant or 'sin' sources run on the device")
+
+
+# ---------------------------------------------------------------- matrix / vector sinks
+
+class UMFPackMatrix:
+    """CSC sink with the reference's arrays (src/linsolver/umfpack.h:26-47).
+    Ap is int64 here (nnz may exceed INT_MAX)."""
+
+    def __init__(self):
+        self.Ap = None
+        self.Ai = None
+        self.Ax = None
+        self.ndofs = 0
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        return sp.csc_matrix((self.Ax, self.Ai, self.Ap), shape=(self.ndofs, self.ndofs))
+
+
+class UMFPackVector:
+    def __init__(self):
+        self.v = None
+
+
+class Discretization:
+    """Single-equation Discretization (src/discretization.h:39-101) on one GPU."""
+
+    def __init__(self, device=0):
+        h = C.c_void_p()
+        capi.call("h3dg_disc_create", C.byref(h), int(device))
+        self.handle = h
+        self.device = device
+        self.space = None
+        self.ndof = None
+        self.nnz = None
+        self._quad = (capi.QUAD_P_PLUS, 2)
+
+    def set_num_equations(self, neq):
+        if neq != 1:
+            raise capi.H3dgError(1, "only one equation is supported")
+
+    def set_spaces(self, space):
+        self.space = space
+        capi.call("h3dg_disc_set_space", self.handle, space.handle)
+
+    def set_pss(self, *args):
+        pass  # the precalculated shapeset is the device's 1D tables
+
+    def set_bilinear_form(self, form, coef=None):
+        if not isinstance(form, BilinearForm):
+            raise UnsupportedForm(4, "bilinear form %r is not one of the device forms" % (form,))
+        c = None if coef is None else np.ascontiguousarray(coef, dtype=np.float64)
+        capi.call("h3dg_disc_set_bilinear_form", self.handle, form.kind,
+                  capi.ptr(c, C.c_double), 0 if c is None else len(c))
+        self._coef = c
+
+    def set_linear_form(self, form):
+        if form is None:
+            capi.call("h3dg_disc_set_linear_form", self.handle, capi.LF_NONE, 0.0)
+            return
+        if not isinstance(form, LinearForm):
+            raise UnsupportedForm(4, "linear form %r is not one of the device forms" % (form,))
+        capi.call("h3dg_disc_set_linear_form", self.handle, form.kind, form.value)
+
+    def set_quadrature(self, points=None, p_plus=None):
+        """Fixed Gauss points per direction, or p_d + p_plus per direction."""
+        if points is not None:
+            self._quad = (capi.QUAD_FIXED, int(points))
+        else:
+            self._quad = (capi.QUAD_P_PLUS, int(p_plus))
+        capi.call("h3dg_disc_set_quadrature", self.handle, *self._quad)
+
+    def create(self, matrix: Optional[UMFPackMatrix] = None, rhs: Optional[UMFPackVector] = None):
+        """Discretization::create: sparsity pattern (+ device plan)."""
+        capi.call("h3dg_disc_set_quadrature", self.handle, *self._quad)
+        nd, nz = C.c_int64(), C.c_int64()
+        capi.call("h3dg_disc_create_pattern", self.handle, C.byref(nd), C.byref(nz))
+        self.ndof, self.nnz = nd.value, nz.value
+        if matrix is not None:
+            matrix.Ap = np.zeros(self.ndof + 1, np.int64)
+            matrix.Ai = np.zeros(self.nnz, np.int32)
+            capi.call("h3dg_disc_get_pattern", self.handle, capi.ptr(matrix.Ap, C.c_int64), capi.ptr(matrix.Ai, C.c_int32))
+            matrix.Ax = np.zeros(self.nnz, np.float64)
+            matrix.ndofs = self.ndof
+        if rhs is not None:
+            rhs.v = np.zeros(self.ndof, np.float64)
+
+    def assemble(self, matrix: Optional[UMFPackMatrix] = None, rhs: Optional[UMFPackVector] = None):
+        """Discretization::assemble into the host sinks (copies inside)."""
+        ax = None if matrix is None else matrix.Ax
+        rv = None if rhs is None else rhs.v
+        capi.call("h3dg_disc_assemble_host", self.handle, capi.PREC_FP64, capi.ptr(ax, C.c_double), capi.ptr(rv, C.c_double))
+
+    def assemble_device(self, Ax, rhs=None, stream=None):
+        """Assemble into device tensors (torch CUDA float64) on ``stream``
+        (default: torch's current stream)."""
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream(Ax.device if Ax is not None else rhs.device)
+        sp = C.c_void_p(stream.cuda_stream)
+        capi.call("h3dg_disc_assemble", self.handle, capi.PREC_FP64,
+                  C.c_void_p(Ax.data_ptr()) if Ax is not None else None,
+                  C.c_void_p(rhs.data_ptr()) if rhs is not None else None, sp)
+
+    def geometry(self, jac=None, irm=None, xyz=None, stream=None):
+        import torch
+        t = jac if jac is not None else (irm if irm is not None else xyz)
+        if stream is None:
+            stream = torch.cuda.current_stream(t.device)
+        capi.call("h3dg_disc_geometry", self.handle,
+                  *[C.c_void_p(x.data_ptr()) if x is not None else None for x in (jac, irm, xyz)],
+                  C.c_void_p(stream.cuda_stream))
+
+    def update_vertices(self, xyz):
+        a = np.ascontiguousarray(xyz, dtype=np.float64)
+        capi.call("h3dg_disc_update_vertices", self.handle, capi.ptr(a, C.c_double), len(a.reshape(-1, 3)))
+
+    def update_coefficients(self, coef):
+        a = np.ascontiguousarray(coef, dtype=np.float64)
+        capi.call("h3dg_disc_update_coefficients", self.handle, capi.ptr(a, C.c_double), len(a))
+
+    def last_launch_count(self):
+        n = C.c_int32()
+        capi.call("h3dg_disc_last_launch_count", self.handle, C.byref(n))
+        return n.value
+
+    def __del__(self):
+        if getattr(self, "handle", None) and capi._lib is not None:
+            capi.lib().h3dg_disc_destroy(self.handle)
+            self.handle = None

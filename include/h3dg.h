@@ -1,0 +1,150 @@
+/*
+ * h3dg.h -- C ABI of the B200 hp-FEM hexahedral assembly path.
+ *
+ * Plain C, extern "C", plain pointers and sizes; no torch or C++ types.
+ * Every call returns an h3dg_status and never aborts; h3dg_last_error()
+ * returns a message for the last failing call on the calling thread.
+ *
+ * Each entry point replaces one piece of the Hermes3D reference's call
+ * surface for assembling a linear system (cited as file:line within the
+ * reference project).  The reference's own C++ objects are
+ *   Mesh          src/mesh.h:522-698      (+ Mesh3DReader, src/loader/mesh3d.cc)
+ *   H1Space       src/space.h:76-458, src/space/h1.h
+ *   Discretization src/discretization.h:39-101
+ *   UMFPackMatrix / UMFPackVector  src/linsolver/umfpack.h:26-64 (CSC Ap/Ai/Ax, v)
+ * and weak forms are C function pointers (src/integrals/h1.h).  A GPU
+ * cannot run opaque CPU form callbacks, so the stock forms are selected
+ * by descriptor (H3DG_BF_*, H3DG_LF_*); anything else is rejected with
+ * H3DG_ERR_UNSUPPORTED_FORM.  There is no CPU fallback: assembly calls
+ * fail with H3DG_ERR_CUDA when no device is usable.
+ */
+#ifndef H3DG_H
+#define H3DG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int h3dg_status;
+#define H3DG_OK                   0
+#define H3DG_ERR_INVALID_ARG      1
+#define H3DG_ERR_CUDA             2
+#define H3DG_ERR_OUT_OF_MEMORY    3
+#define H3DG_ERR_UNSUPPORTED_FORM 4
+#define H3DG_ERR_MESH             5
+#define H3DG_ERR_STATE            6
+#define H3DG_ERR_TIMEOUT          7
+#define H3DG_ERR_TOO_LARGE        8
+
+/* boundary-condition types, as EBCType (src/space.h:44-48) */
+#define H3DG_BC_ESSENTIAL 0
+#define H3DG_BC_NATURAL   1
+#define H3DG_BC_NONE      2
+
+/* bilinear forms (src/integrals/h1.h:115-177) */
+#define H3DG_BF_GRAD_GRAD       1   /* int_grad_u_grad_v, optionally times a per-element coefficient */
+#define H3DG_BF_GRAD_GRAD_MASS  2   /* int_grad_u_grad_v + int_u_v */
+
+/* linear forms (int_F_v, src/integrals/h1.h:136-152) */
+#define H3DG_LF_NONE   0
+#define H3DG_LF_CONST  1   /* F(x,y,z) = c */
+#define H3DG_LF_SIN    2   /* F(x,y,z) = sin(pi x) sin(pi y) sin(pi z) */
+
+/* volume quadrature: n Gauss points per direction, or p_d + n per direction */
+#define H3DG_QUAD_FIXED   0
+#define H3DG_QUAD_P_PLUS  1
+
+/* arithmetic of the element-matrix contraction */
+#define H3DG_PREC_FP64    0
+
+typedef struct h3dg_mesh h3dg_mesh;
+typedef struct h3dg_space h3dg_space;
+typedef struct h3dg_disc h3dg_disc;
+
+typedef int (*h3dg_bc_type_fn)(int marker, void *ctx);
+typedef double (*h3dg_bc_value_fn)(int marker, double x, double y, double z, void *ctx);
+
+int h3dg_version(void);
+const char *h3dg_status_string(h3dg_status s);
+const char *h3dg_last_error(void);
+
+/* ---------------------------------------------------------------- mesh */
+/* new Mesh (src/mesh.h:522) */
+h3dg_status h3dg_mesh_create(h3dg_mesh **mesh);
+h3dg_status h3dg_mesh_destroy(h3dg_mesh *mesh);
+/* Mesh::add_vertex (src/mesh.cc:915-920), n vertices, ids 1..n in order */
+h3dg_status h3dg_mesh_add_vertices(h3dg_mesh *mesh, const double *xyz, int64_t n);
+/* Mesh::add_hex (src/mesh.cc:975-1000); vtx is n x 8, 1-based, RefHex order */
+h3dg_status h3dg_mesh_add_hexes(h3dg_mesh *mesh, const int64_t *vtx, int64_t n);
+/* Mesh::add_quad_boundary (src/mesh.cc:1061-1078); vtx is n x 4, 1-based */
+h3dg_status h3dg_mesh_add_quad_boundaries(h3dg_mesh *mesh, const int64_t *vtx, const int32_t *marker, int64_t n);
+/* Mesh::ugh (src/mesh.cc:1080-1102) + Mesh3DReader's outer-face check (src/loader/mesh3d.cc:272-282) */
+h3dg_status h3dg_mesh_finalize(h3dg_mesh *mesh);
+/* sizes: vertices, elements, facets, edges */
+h3dg_status h3dg_mesh_counts(const h3dg_mesh *mesh, int64_t *nv, int64_t *ne, int64_t *nfacets, int64_t *nedges);
+
+/* ---------------------------------------------------------------- space */
+/* H1Space(mesh, H1ShapesetLobattoHex) (src/space/h1.cc:33-37) */
+h3dg_status h3dg_space_create(h3dg_mesh *mesh, h3dg_space **space);
+h3dg_status h3dg_space_destroy(h3dg_space *space);
+/* Space::set_bc_types / set_bc_values (src/space.cc:2087-2098); NULL = reference defaults
+ * (every marker essential, value 0) */
+h3dg_status h3dg_space_set_bc_types(h3dg_space *space, h3dg_bc_type_fn fn, void *ctx);
+h3dg_status h3dg_space_set_bc_values(h3dg_space *space, h3dg_bc_value_fn fn, void *ctx);
+/* Space::set_uniform_order / set_element_order (src/space.cc:108-150); orders is ne x 3 */
+h3dg_status h3dg_space_set_uniform_order(h3dg_space *space, int px, int py, int pz);
+h3dg_status h3dg_space_set_element_orders(h3dg_space *space, const int32_t *orders, int64_t ne);
+/* Space::assign_dofs (src/space.cc:1991-2028), returns get_dof_count() */
+h3dg_status h3dg_space_assign_dofs(h3dg_space *space, int first_dof, int stride, int64_t *ndof);
+/* H1Space::get_element_assembly_list (src/space/h1.cc:130-137); elem_id is 1-based.
+ * Writes min(cap, cnt) entries; *cnt receives the full length. */
+h3dg_status h3dg_space_get_element_assembly_list(const h3dg_space *space, int64_t elem_id,
+	int64_t *idx, int32_t *dof, double *coef, int32_t cap, int32_t *cnt);
+
+/* ---------------------------------------------------------------- discretization */
+/* Discretization() + set_num_equations(1) (src/discretization.cc:36-88); device = CUDA ordinal */
+h3dg_status h3dg_disc_create(h3dg_disc **disc, int device);
+h3dg_status h3dg_disc_destroy(h3dg_disc *disc);
+/* set_spaces(1, &space) + set_pss (src/discretization.cc:102-134) */
+h3dg_status h3dg_disc_set_space(h3dg_disc *disc, h3dg_space *space);
+/* set_bilinear_form(0, 0, form) (src/discretization.cc:136-148); elem_coef: one value per
+ * element id (ne values, multiplies the grad-grad term), or NULL for 1 */
+h3dg_status h3dg_disc_set_bilinear_form(h3dg_disc *disc, int form, const double *elem_coef, int64_t ne);
+/* set_linear_form(0, lf) (src/discretization.cc:151-161); value is the constant for H3DG_LF_CONST */
+h3dg_status h3dg_disc_set_linear_form(h3dg_disc *disc, int form, double value);
+/* quadrature of the forms: mode H3DG_QUAD_FIXED (n points per direction) or
+ * H3DG_QUAD_P_PLUS (p_d + n points per direction); the reference's forms fix the
+ * order inside the form (tests/integrals/hex-h1-real/h1-hex-real.cc:55-103) */
+h3dg_status h3dg_disc_set_quadrature(h3dg_disc *disc, int mode, int n);
+/* Discretization::create (src/discretization.cc:164-230) + UMFPackMatrix::alloc
+ * (src/linsolver/umfpack.cc:46-71): builds the CSC pattern and the device plan */
+h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nnz);
+/* UMFPackMatrix Ap (ndof+1, widened to int64: nnz can exceed INT_MAX) and Ai (nnz) */
+h3dg_status h3dg_disc_get_pattern(const h3dg_disc *disc, int64_t *Ap, int32_t *Ai);
+/* Discretization::assemble (src/discretization.cc:232-422) into device arrays
+ * d_Ax (nnz, CSC order of the pattern) and d_rhs (ndof); either may be NULL.
+ * stream: a cudaStream_t, or NULL for the default stream. */
+h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream);
+/* the same into host arrays (UMFPackMatrix::Ax / UMFPackVector::v); copies inside */
+h3dg_status h3dg_disc_assemble_host(h3dg_disc *disc, int precision, double *Ax, double *rhs);
+/* replace the vertex coordinates (same topology) from host memory, nv x 3 */
+h3dg_status h3dg_disc_update_vertices(h3dg_disc *disc, const double *xyz, int64_t nv);
+/* replace the per-element coefficient (ne values, element-id order) from host memory */
+h3dg_status h3dg_disc_update_coefficients(h3dg_disc *disc, const double *elem_coef, int64_t ne);
+/* number of kernels launched by the last assemble call */
+h3dg_status h3dg_disc_last_launch_count(const h3dg_disc *disc, int32_t *count);
+
+/* RefMap (src/refmap.cc:177-231, 265-316): per element (id order) and per point of the
+ * disc's volume rule, the signed Jacobian determinant (get_jacobian without the
+ * weight), the transposed inverse Jacobian irm[r][c] = (J^-1)[c][r] (get_inv_ref_map)
+ * and the physical coordinates (get_phys_x/y/z).  Device arrays: d_jac ne*nq,
+ * d_irm ne*nq*9, d_xyz ne*nq*3 (any may be NULL). */
+h3dg_status h3dg_disc_geometry(h3dg_disc *disc, double *d_jac, double *d_irm, double *d_xyz, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* H3DG_H */
