@@ -1,0 +1,316 @@
+"""Benchmark: hp-FEM hexahedral assembly on B200 (elements/s).
+
+Workload (one "step" = one full assembly): the 64^3 = 262,144-hexahedra unit
+cube with interior vertices jittered by U(+-0.2h) (seeded), uniform p=2,
+4 Gauss points per direction, grad.grad + mass with f = sin(pi x) sin(pi y)
+sin(pi z): full CSC matrix (127,263,527 nonzeros) + RHS, FP64.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value: elements assembled per second, inputs resident in HBM, device time
+(CUDA events on the launch stream), max over ranks.  With N > 1 every rank
+assembles its own 64^3 subdomain (different seed): weak scaling, no
+collective on the data path.  e2e: the same through the C ABI call with host
+buffers: per step the vertex coordinates go host->device from pinned memory
+and Ax + rhs come back device->host into pinned memory.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_ELEM_SIDE = 64
+P_ORDER = 2
+N_POINTS = 4
+METRIC = "hp assembly elements/s (FP64, C2: 64^3 jittered, p=2, 4^3 pts, grad+mass, sin source, full CSC+RHS)"
+CPU_SAMPLE_SIDE = 16
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        import statistics
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def build_problem(h, seed, device):
+    mesh = h.unit_cube(N_ELEM_SIDE, 0.2, seed)
+    mesh.ugh()
+    sp = h.H1Space(mesh)
+    sp.set_uniform_order(P_ORDER)
+    sp.assign_dofs()
+    d = h.Discretization(device)
+    d.set_spaces(sp)
+    d.set_bilinear_form(h.int_grad_u_grad_v_plus_u_v)
+    d.set_linear_form(h.int_F_v("sin"))
+    d.set_quadrature(points=N_POINTS)
+    d.create()
+    return mesh, sp, d
+
+
+def algorithmic_bytes(nnz, ndof, nv, ne):
+    # 8 nnz (Ax written) + 8 ndof (rhs) + 24 nv (coordinates read) + 32 ne (connectivity)
+    return 8 * nnz + 8 * ndof + 24 * nv + 32 * ne
+
+
+def dense_flops_per_element():
+    nl = (P_ORDER + 1) ** 3
+    nq = N_POINTS ** 3
+    return 2 * nl * nl * 3 * nq + 2 * nl * nl * nq + 2 * nl * nq
+
+
+def cpu_baseline(repeat=3):
+    """The reference (oracle/_ref, built from the reference's sources) on one
+    host core, on a bounded sample of the same workload."""
+    from hermes3d_b200.mesh import unit_cube
+    from oracle import ref_driver
+    if not ref_driver.available():
+        return None
+    n = CPU_SAMPLE_SIDE
+    r = ref_driver.run(unit_cube(n, 0.2, 0), p=P_ORDER, qmode="fixed:%d" % N_POINTS, mass=True, source="sin",
+                       repeat=repeat)
+    t = r["timing"]["t_assemble_median"]
+    return {"value": n ** 3 / t, "unit": "elements/s", "cores": 1, "kind": "reference",
+            "sample": "%d^3 jittered sub-mesh (%d elements) of the same workload, Discretization::assemble, "
+                      "median of %d" % (n, n ** 3, repeat)}
+
+
+def run_reference_arm(args):
+    """--impl reference: the reference's own CPU assembly on all host cores
+    (one single-threaded process per core, each on a bounded sample)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from hermes3d_b200.mesh import unit_cube
+    from oracle import ref_driver
+    if not ref_driver.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference oracle binary oracle/_ref/h3d_ref_driver not built"}))
+        return 0
+    import tempfile
+    ncores = os.cpu_count() or 1
+    n = CPU_SAMPLE_SIDE
+    steps = args.warmup + args.steps
+    with tempfile.TemporaryDirectory() as td:
+        mf = os.path.join(td, "m.bin")
+        unit_cube(n, 0.2, 0).save_bin(mf)
+        procs = []
+        t0 = time.time()
+        for c in range(ncores):
+            procs.append(subprocess.Popen([ref_driver.DRIVER, "--mesh", mf, "--out", os.path.join(td, "o%d.bin" % c),
+                                           "--p", str(P_ORDER), "--qmode", "fixed:%d" % N_POINTS, "--mass",
+                                           "--source", "sin", "--repeat", str(steps)],
+                                          stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+        outs = [p.communicate() for p in procs]
+        wall = time.time() - t0
+    times = []
+    for o, e in outs:
+        line = o.strip().splitlines()[-1] if o.strip() else "{}"
+        times.append(json.loads(line).get("t_assemble_median", float("nan")))
+    t_step = max(times)
+    value = ncores * n ** 3 / t_step
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": "C2 sample: %d^3 jittered hexahedra per process, p=2, 4^3 Gauss points, grad+mass, "
+                               "sin source" % n, "processes": ncores},
+        "cpu_baseline": {"value": value, "unit": "elements/s", "cores": ncores, "kind": "reference",
+                         "sample": "%d processes x %d^3 elements, %d assemblies each, wall %.1fs" % (ncores, n, steps, wall)},
+        "e2e": {"value": value, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import hermes3d_b200 as h
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    t_setup = time.time()
+    mesh, sp, d = build_problem(h, seed=rank, device=local)
+    t_setup = time.time() - t_setup
+    ne, ndof, nnz, nv = mesh.num_elements, d.ndof, d.nnz, mesh.num_vertices
+    stream = torch.cuda.current_stream()
+    Ax = torch.empty(nnz, dtype=torch.float64, device="cuda")
+    rhs = torch.empty(ndof, dtype=torch.float64, device="cuda")
+
+    for _ in range(max(3, args.warmup)):
+        d.assemble_device(Ax, rhs, stream)
+    torch.cuda.synchronize()
+    launches_per_step = d.last_launch_count()
+
+    d.enable_kernel_timing(args.steps)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            d.assemble_device(Ax, rhs, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    kt = d.kernel_times()
+    kernel_ms = float(np.mean(kt)) if kt else None
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_per_step = ms_max / args.steps
+    value = world * ne / (ms_per_step * 1e-3)
+
+    # ---- e2e through the C ABI with pinned host buffers
+    xyz_pin = torch.from_numpy(np.ascontiguousarray(mesh.xyz)).pin_memory()
+    Ax_pin = torch.empty(nnz, dtype=torch.float64).pin_memory()
+    rhs_pin = torch.empty(ndof, dtype=torch.float64).pin_memory()
+    xyz_np, Ax_np, rhs_np = xyz_pin.numpy(), Ax_pin.numpy(), rhs_pin.numpy()
+    M, V = h.UMFPackMatrix(), h.UMFPackVector()
+    M.Ax, V.v = Ax_np, rhs_np
+    d.update_vertices(xyz_np)
+    d.assemble(M, V)
+    barrier()
+    torch.cuda.synchronize()
+    c0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        d.update_vertices(xyz_np)
+        d.assemble(M, V)
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - c0) / args.e2e_steps
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * ne / float(te.item())
+    ok = bool(np.all(np.isfinite(Ax_np))) and bool(np.all(np.isfinite(rhs_np)))
+
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        B = algorithmic_bytes(nnz, ndof, nv, ne)
+        kms = kernel_ms if kernel_ms else ms_per_step
+        achieved = B / (kms * 1e-3) / 1e9
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "traffic_c2_assemble_fp64.json")
+        if os.path.exists(tf):
+            try:
+                traffic = json.load(open(tf)).get("bytes_per_step")
+            except Exception:
+                traffic = None
+        out = {
+            "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded jittered unit-cube mesh)",
+            "config": {"workload": "C2: 64^3=262144 jittered (+-0.2h) hexahedra, p=2, 4^3 Gauss points, "
+                                   "grad.grad+mass, f=sin(pi x)sin(pi y)sin(pi z), full CSC+RHS",
+                       "ndof": ndof, "nnz": nnz, "elements_per_gpu": ne, "l2": "inputs larger than L2 (Ax alone 1.0 GB)",
+                       "parallelism": "replicas: one 64^3 subdomain per GPU" if world > 1 else "single GPU",
+                       "setup_s": round(t_setup, 2)},
+            "nnz_per_s": world * nnz / (ms_per_step * 1e-3),
+            "kernel_ms_per_step": kernel_ms,
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": traffic, "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind,
+                         "algorithmic_bytes_per_step": B,
+                         "fp64_dense_equiv_tflops": ne * dense_flops_per_element() / (kms * 1e-3) / 1e12},
+            "e2e": {"value": e2e_value, "unit": "elements/s", "h2d_bytes_per_step": 24 * nv,
+                    "d2h_bytes_per_step": 8 * nnz + 8 * ndof, "ms_per_step": 1e3 * float(te.item())},
+            "clocks": clk.summary(),
+            "finite": ok,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            try:
+                out["cpu_baseline"] = cpu_baseline()
+            except Exception as ex:  # report, do not fail the GPU number
+                out["cpu_baseline"] = {"error": str(ex)[:200]}
+        print(json.dumps(out))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -83,7 +83,12 @@ struct h3dg_disc {
 	DBuf<double> el_coef;
 	DBuf<int> status;
 	int table_bytes = 0;
-	double *h_pin_scratch = nullptr;
+	// kernel-only timing records
+	std::vector<cudaEvent_t> tev;
+	int tcap = 0, tn = 0;
+	~h3dg_disc() {
+		for (auto e : tev) cudaEventDestroy(e);
+	}
 };
 
 extern "C" {
@@ -447,6 +452,8 @@ h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, dou
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks->fn, ks->threads, ks->smem);
 	if (per_sm < 1) per_sm = 1;
 	int32_t launches = 0;
+	const bool rec = disc->tn < disc->tcap;
+	if (rec) H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn], st));
 	for (int c = 0; c < P.ncolors; c++) {
 		int64_t kb = P.color_ptr[c], ke = P.color_ptr[c + 1];
 		if (ke <= kb) continue;
@@ -455,7 +462,35 @@ h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, dou
 		launches++;
 	}
 	H3DG_CUDA_TRY(cudaGetLastError());
+	if (rec) {
+		H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn + 1], st));
+		disc->tn++;
+	}
 	disc->last_launches = launches;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_enable_kernel_timing(h3dg_disc *disc, int32_t n) {
+	if (!disc || n < 0) return fail(H3DG_ERR_INVALID_ARG, "enable_kernel_timing: bad arguments");
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	for (auto e : disc->tev) cudaEventDestroy(e);
+	disc->tev.assign(2 * (size_t) n, nullptr);
+	for (auto &e : disc->tev) H3DG_CUDA_TRY(cudaEventCreate(&e));
+	disc->tcap = n;
+	disc->tn = 0;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_kernel_times(h3dg_disc *disc, float *ms, int32_t cap, int32_t *n) {
+	if (!disc || !n) return fail(H3DG_ERR_INVALID_ARG, "kernel_times: bad arguments");
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	int k = 0;
+	for (; k < disc->tn && k < cap; k++) {
+		H3DG_CUDA_TRY(cudaEventSynchronize(disc->tev[2 * k + 1]));
+		H3DG_CUDA_TRY(cudaEventElapsedTime(&ms[k], disc->tev[2 * k], disc->tev[2 * k + 1]));
+	}
+	*n = k;
+	disc->tn = 0;
 	return H3DG_OK;
 }
 

@@ -242,6 +242,15 @@ class Discretization:
         a = np.ascontiguousarray(coef, dtype=np.float64)
         capi.call("h3dg_disc_update_coefficients", self.handle, capi.ptr(a, C.c_double), len(a))
 
+    def enable_kernel_timing(self, n):
+        capi.call("h3dg_disc_enable_kernel_timing", self.handle, int(n))
+
+    def kernel_times(self, cap=4096):
+        buf = (C.c_float * cap)()
+        n = C.c_int32()
+        capi.call("h3dg_disc_kernel_times", self.handle, buf, cap, C.byref(n))
+        return [buf[i] for i in range(n.value)]
+
     def last_launch_count(self):
         n = C.c_int32()
         capi.call("h3dg_disc_last_launch_count", self.handle, C.byref(n))

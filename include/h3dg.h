@@ -136,6 +136,14 @@ h3dg_status h3dg_disc_update_coefficients(h3dg_disc *disc, const double *elem_co
 /* number of kernels launched by the last assemble call */
 h3dg_status h3dg_disc_last_launch_count(const h3dg_disc *disc, int32_t *count);
 
+/* Kernel-only timing (no reference counterpart; a measurement hook): when
+ * enabled with capacity n, each assemble call records a CUDA event pair on its
+ * launch stream around its kernel launches (after the output zeroing), up to
+ * n calls.  h3dg_disc_kernel_times synchronises those events and returns the
+ * elapsed milliseconds of each recorded call, then clears the records. */
+h3dg_status h3dg_disc_enable_kernel_timing(h3dg_disc *disc, int32_t n);
+h3dg_status h3dg_disc_kernel_times(h3dg_disc *disc, float *ms, int32_t cap, int32_t *n);
+
 /* RefMap (src/refmap.cc:177-231, 265-316): per element (id order) and per point of the
  * disc's volume rule, the signed Jacobian determinant (get_jacobian without the
  * weight), the transposed inverse Jacobian irm[r][c] = (J^-1)[c][r] (get_inv_ref_map)

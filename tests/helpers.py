@@ -1,0 +1,93 @@
+"""Shared test helpers: golden fixtures and building the product objects
+from a fixture's parameters."""
+import ast
+import glob
+import os
+
+import numpy as np
+
+import hermes3d_b200 as h
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+# relative tolerance of FP64 values vs the reference (sum order and the
+# reference's 14-digit Gauss tables differ at ~1e-14)
+FP64_RTOL = 1e-12
+
+
+def golden_names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"), allow_pickle=False)
+    d = {k: z[k] for k in z.files}
+    d["params"] = ast.literal_eval(str(d["params"]))
+    return d
+
+
+def mesh_of(g):
+    return h.Mesh().set_arrays(g["xyz"], g["hexes"], g["bquads"], g["bmarkers"])
+
+
+def space_of(g, mesh=None):
+    p = g["params"]
+    mesh = mesh or mesh_of(g)
+    mesh.ugh()
+    sp = h.H1Space(mesh)
+    bc = p.get("bc", "dirichlet0")
+    if bc == "natural":
+        sp.set_bc_types(lambda m: h.BC_NATURAL)
+    if bc == "dirichlet_poly":
+        sp.set_bc_values(lambda m, x, y, z: x * x + y * y + z * z)
+    if len(g["orders"]):
+        sp.set_element_orders(g["orders"])
+    else:
+        sp.set_uniform_order(p["p"])
+    sp.assign_dofs()
+    return sp
+
+
+def quad_of(g):
+    q = g["params"]["qmode"]
+    kind, n = q.split(":")
+    return kind, int(n)
+
+
+def disc_of(g, sp, device=0):
+    p = g["params"]
+    d = h.Discretization(device)
+    d.set_spaces(sp)
+    form = h.int_grad_u_grad_v_plus_u_v if p.get("mass") else h.int_grad_u_grad_v
+    d.set_bilinear_form(form, g["gradcoef"] if len(g["gradcoef"]) else None)
+    src = p.get("source", "one")
+    if src == "one":
+        d.set_linear_form(h.int_F_v(1.0))
+    elif src == "sin":
+        d.set_linear_form(h.int_F_v("sin"))
+    elif src == "poly":
+        d.set_linear_form(h.int_F_v(-6.0))
+    kind, n = quad_of(g)
+    if kind == "fixed":
+        d.set_quadrature(points=n)
+    else:
+        d.set_quadrature(p_plus=n)
+    return d
+
+
+def lf_of(g):
+    src = g["params"].get("source", "one")
+    return {"one": (1, 1.0), "sin": (2, 0.0), "poly": (1, -6.0), "none": (0, 0.0)}[src]
+
+
+def nq_of(g):
+    kind, n = quad_of(g)
+    ne = len(g["hexes"])
+    if kind == "fixed":
+        return np.full((ne, 3), n, np.int32)
+    o = g["orders"] if len(g["orders"]) else np.full((ne, 3), g["params"]["p"], np.int32)
+    return (np.asarray(o) + n).astype(np.int32)
+
+
+def rel_err(a, b):
+    s = max(float(np.max(np.abs(b))) if len(b) else 0.0, 1e-300)
+    return float(np.max(np.abs(a - b))) / s if len(a) else 0.0
