@@ -508,6 +508,7 @@ h3dg_status h3dg_disc_assemble_host(h3dg_disc *disc, int precision, double *Ax, 
 	H3DG_CUDA_TRY(cudaMemcpy(&st, disc->status.p, sizeof(int), cudaMemcpyDeviceToHost));
 	if (st) {
 		cudaMemset(disc->status.p, 0, sizeof(int));
+		if (st & h3dg::kErrBounds) return fail(H3DG_ERR_STATE, "assemble_host: a scatter target fell outside its column (plan corrupt)");
 		return fail(H3DG_ERR_TIMEOUT, "assemble_host: a device wait gave up");
 	}
 	return H3DG_OK;

@@ -702,7 +702,7 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 				for (int a = 0; a < mc; a++) {
 					int row = dofs[(size_t) e * nl + a];
 					const int32_t *pos = std::lower_bound(c0, c1, row);
-					P.el_off[((size_t) k * nl + a) * nl + b] = (uint16_t) (pos - c0);
+					P.el_off[((size_t) k * nl + b) * nl + a] = (uint16_t) (pos - c0);
 				}
 			}
 		}

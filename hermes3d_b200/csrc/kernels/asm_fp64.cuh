@@ -223,8 +223,9 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 				const int b = p / mcnt, a = p % mcnt;
 				const int sa = es[a], sb = es[b];
 				const double v = ec[a] * ec[b] * (A[sa * NL + sb] + A[sb * NL + sa]);
-				double *dst = args.Ax + args.Ap[edof[b]] + off[b * NL + a];
-				*dst += v;
+				const int64_t c0 = args.Ap[edof[b]], pos = c0 + off[b * NL + a];
+				if (pos < args.Ap[edof[b] + 1]) args.Ax[pos] += v;
+				else atomicOr(args.status, kErrBounds);
 			}
 		}
 		if (args.rhs && args.lf) {

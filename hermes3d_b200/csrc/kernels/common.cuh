@@ -9,6 +9,7 @@ namespace h3dg {
 
 // error bits written to the plan's device status word
 constexpr int kErrTimeout = 1;
+constexpr int kErrBounds = 2;    // a scatter target fell outside its CSC column (store skipped)
 
 // Everything a fused assembly kernel reads, as device pointers.
 struct KArgs {
