@@ -418,6 +418,12 @@ h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, dou
 	for (auto &k : kernel_table())
 		if (k.p == P.px && k.nq == P.nqx) ks = &k;
 	if (!ks) return fail(H3DG_ERR_INVALID_ARG, "assemble: no FP64 kernel instantiated for this order / rule");
+	{
+		h3dg_status s0 = ensure_device(disc);
+		if (s0 != H3DG_OK) return s0;
+	}
+	if (!disc->xyz.p || !disc->el_vtx.p || !disc->el_off.p || !disc->Ap.p || !disc->tables.p || !disc->status.p)
+		return fail(H3DG_ERR_STATE, "assemble: device plan missing");
 	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
 	cudaStream_t st = (cudaStream_t) stream;
 	h3dg::KArgs a;
