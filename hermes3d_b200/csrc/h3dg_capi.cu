@@ -400,6 +400,7 @@ const std::vector<KernelSpec> &kernel_table() {
 	static std::vector<KernelSpec> t = {
 		spec<1, 2, 128>(), spec<1, 3, 128>(), spec<2, 3, 128>(), spec<2, 4, 128>(), spec<2, 5, 128>(),
 		spec<3, 4, 256>(), spec<3, 5, 256>(), spec<3, 6, 256>(),
+		spec<4, 5, 512>(), spec<4, 6, 512>(),
 	};
 	return t;
 }
