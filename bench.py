@@ -91,8 +91,8 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def build_problem(h, seed, device):
-    mesh = h.unit_cube(N_ELEM_SIDE, 0.2, seed)
+def build_problem(h, seed, device, side=N_ELEM_SIDE):
+    mesh = h.unit_cube(side, 0.2, seed)
     mesh.ugh()
     sp = h.H1Space(mesh)
     sp.set_uniform_order(P_ORDER)
@@ -187,6 +187,7 @@ def main():
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--side", type=int, default=N_ELEM_SIDE, help="elements per cube side (profiling runs only)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -210,7 +211,7 @@ def main():
             dist.barrier()
 
     t_setup = time.time()
-    mesh, sp, d = build_problem(h, seed=rank, device=local)
+    mesh, sp, d = build_problem(h, seed=rank, device=local, side=args.side)
     t_setup = time.time() - t_setup
     ne, ndof, nnz, nv = mesh.num_elements, d.ndof, d.nnz, mesh.num_vertices
     stream = torch.cuda.current_stream()
@@ -256,11 +257,11 @@ def main():
     barrier()
     torch.cuda.synchronize()
     c0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
+    for _ in range(max(1, args.e2e_steps)):
         d.update_vertices(xyz_np)
         d.assemble(M, V)
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - c0) / args.e2e_steps
+    e2e_s = (time.perf_counter() - c0) / max(1, args.e2e_steps)
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
