@@ -291,6 +291,7 @@ def main():
                        "setup_s": round(t_setup, 2)},
             "nnz_per_s": world * nnz / (ms_per_step * 1e-3),
             "kernel_ms_per_step": kernel_ms,
+            "autotuned_variant": d.tuning(),
             "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind,

@@ -72,6 +72,8 @@ struct h3dg_disc {
 	int qmode = H3DG_QUAD_FIXED, qn = 0;
 	bool have_plan = false;
 	bool on_device = false;
+	int variant = -1;          // autotuned kernel variant (index into the kernel table)
+	float variant_ms = 0.0f;
 	h3dg::Plan plan;
 	int32_t last_launches = 0;
 
@@ -334,6 +336,7 @@ h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nn
 	const h3dg::Plan &P = disc->plan;
 	disc->on_device = false;
 	disc->have_plan = true;
+	disc->variant = -1;
 	if (ndof) *ndof = P.ndof;
 	if (nnz) *nnz = P.nnz;
 	return H3DG_OK;
@@ -387,20 +390,29 @@ using KernelFn = void (*)(h3dg::KArgs, int64_t, int64_t);
 struct KernelSpec {
 	int p, nq;
 	KernelFn fn;
-	int threads;
+	int threads, eb;
 	size_t smem;
+	bool configured;
 };
 
-template <int P, int NQ, int NT>
+template <int P, int NQ, int NT, int EB>
 KernelSpec spec() {
-	return KernelSpec { P, NQ, &h3dg::k_assemble_fp64<P, P, P, NQ, NQ, NQ, NT>, NT, h3dg::SfShape<P, P, P, NQ, NQ, NQ>::SMEM_BYTES };
+	return KernelSpec { P, NQ, &h3dg::k_assemble_fp64<P, P, P, NQ, NQ, NQ, NT, EB>, NT, EB,
+	                    h3dg::SfShape<P, P, P, NQ, NQ, NQ, EB>::SMEM_BYTES, false };
 }
 
-const std::vector<KernelSpec> &kernel_table() {
+// FP64 kernel variants per (order, points); the autotuner times each on the
+// actual plan at the first assembly and keeps the fastest.
+std::vector<KernelSpec> &kernel_table() {
 	static std::vector<KernelSpec> t = {
-		spec<1, 2, 128>(), spec<1, 3, 128>(), spec<2, 3, 128>(), spec<2, 4, 128>(), spec<2, 5, 128>(),
-		spec<3, 4, 256>(), spec<3, 5, 256>(), spec<3, 6, 256>(),
-		spec<4, 5, 512>(), spec<4, 6, 512>(),
+		spec<1, 2, 128, 8>(), spec<1, 3, 128, 8>(),
+		spec<2, 3, 128, 2>(), spec<2, 3, 256, 4>(),
+		spec<2, 4, 128, 1>(), spec<2, 4, 128, 2>(), spec<2, 4, 256, 4>(), spec<2, 4, 256, 8>(),
+		spec<2, 5, 128, 2>(), spec<2, 5, 256, 4>(),
+		spec<3, 4, 256, 1>(), spec<3, 4, 256, 2>(),
+		spec<3, 5, 256, 1>(), spec<3, 5, 256, 2>(), spec<3, 5, 512, 2>(),
+		spec<3, 6, 256, 1>(), spec<3, 6, 256, 2>(),
+		spec<4, 5, 512, 1>(), spec<4, 6, 512, 1>(),
 	};
 	return t;
 }
@@ -415,9 +427,10 @@ h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, dou
 	const h3dg::Plan &P = disc->plan;
 	if (P.px != P.py || P.px != P.pz || P.nqx != P.nqy || P.nqx != P.nqz)
 		return fail(H3DG_ERR_INVALID_ARG, "assemble: anisotropic orders need the batched path");
-	const KernelSpec *ks = nullptr;
-	for (auto &k : kernel_table())
-		if (k.p == P.px && k.nq == P.nqx) ks = &k;
+	std::vector<int> cands;
+	for (size_t i = 0; i < kernel_table().size(); i++)
+		if (kernel_table()[i].p == P.px && kernel_table()[i].nq == P.nqx) cands.push_back((int) i);
+	const KernelSpec *ks = cands.empty() ? nullptr : &kernel_table()[cands[0]];
 	if (!ks) return fail(H3DG_ERR_INVALID_ARG, "assemble: no FP64 kernel instantiated for this order / rule");
 	{
 		h3dg_status s0 = ensure_device(disc);
@@ -448,32 +461,81 @@ h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, dou
 	a.status = disc->status.p;
 	if (d_Ax) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
 	if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
-	static int configured[64] = { 0 };
-	int kidx = (int) (ks - kernel_table().data());
-	if (!configured[kidx]) {
-		H3DG_CUDA_TRY(cudaFuncSetAttribute(ks->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) ks->smem));
-		configured[kidx] = 1;
-	}
-	int nsm = 148, per_sm = 1;
+	int nsm = 148;
 	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks->fn, ks->threads, ks->smem);
-	if (per_sm < 1) per_sm = 1;
+	auto prepare = [&](KernelSpec &k, int &grid_per_sm) -> h3dg_status {
+		if (!k.configured) {
+			H3DG_CUDA_TRY(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) k.smem));
+			k.configured = true;
+		}
+		grid_per_sm = 1;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid_per_sm, k.fn, k.threads, k.smem);
+		if (grid_per_sm < 1) grid_per_sm = 1;
+		return H3DG_OK;
+	};
+	auto sweep = [&](const KernelSpec &k, int per_sm) -> int32_t {
+		int32_t n = 0;
+		for (int c = 0; c < P.ncolors; c++) {
+			int64_t kb = P.color_ptr[c], ke = P.color_ptr[c + 1];
+			if (ke <= kb) continue;
+			int64_t nb = (ke - kb + k.eb - 1) / k.eb;
+			int64_t grid = std::min<int64_t>(nb, (int64_t) nsm * per_sm);
+			k.fn<<<(unsigned) grid, k.threads, k.smem, st>>>(a, kb, ke);
+			n++;
+		}
+		return n;
+	};
+	// autotune once per plan: time one colour sweep of every variant (results are
+	// bitwise identical across variants; the outputs are re-zeroed afterwards)
+	if (disc->variant < 0 && cands.size() > 1) {
+		cudaEvent_t e0, e1;
+		H3DG_CUDA_TRY(cudaEventCreate(&e0));
+		H3DG_CUDA_TRY(cudaEventCreate(&e1));
+		float best = 1e30f;
+		int besti = cands[0];
+		for (int ci : cands) {
+			KernelSpec &k = kernel_table()[ci];
+			int per_sm;
+			if (prepare(k, per_sm) != H3DG_OK) continue;
+			sweep(k, per_sm);
+			H3DG_CUDA_TRY(cudaEventRecord(e0, st));
+			for (int r = 0; r < 2; r++) sweep(k, per_sm);
+			H3DG_CUDA_TRY(cudaEventRecord(e1, st));
+			H3DG_CUDA_TRY(cudaEventSynchronize(e1));
+			float ms = 0;
+			H3DG_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+			if (ms < best) { best = ms; besti = ci; }
+		}
+		cudaEventDestroy(e0);
+		cudaEventDestroy(e1);
+		disc->variant = besti;
+		disc->variant_ms = best / 2;
+		if (d_Ax) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
+		if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
+	}
+	if (disc->variant >= 0) ks = &kernel_table()[disc->variant];
+	KernelSpec &K = *const_cast<KernelSpec *>(ks);
+	int per_sm = 1;
+	if (prepare(K, per_sm) != H3DG_OK) return H3DG_ERR_CUDA;
 	int32_t launches = 0;
 	const bool rec = disc->tn < disc->tcap;
 	if (rec) H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn], st));
-	for (int c = 0; c < P.ncolors; c++) {
-		int64_t kb = P.color_ptr[c], ke = P.color_ptr[c + 1];
-		if (ke <= kb) continue;
-		int64_t grid = std::min<int64_t>(ke - kb, (int64_t) nsm * per_sm);
-		ks->fn<<<(unsigned) grid, ks->threads, ks->smem, st>>>(a, kb, ke);
-		launches++;
-	}
+	launches = sweep(K, per_sm);
 	H3DG_CUDA_TRY(cudaGetLastError());
 	if (rec) {
 		H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn + 1], st));
 		disc->tn++;
 	}
 	disc->last_launches = launches;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_get_tuning(const h3dg_disc *disc, int32_t *threads, int32_t *elems_per_cta, float *ms) {
+	if (!disc) return fail(H3DG_ERR_INVALID_ARG, "get_tuning: null disc");
+	const KernelSpec *k = disc->variant >= 0 ? &kernel_table()[disc->variant] : nullptr;
+	if (threads) *threads = k ? k->threads : -1;
+	if (elems_per_cta) *elems_per_cta = k ? k->eb : -1;
+	if (ms) *ms = disc->variant_ms;
 	return H3DG_OK;
 }
 

@@ -1,4 +1,4 @@
-// FP64 element-matrix + deterministic scatter, one element per CTA pass.
+// FP64 element-matrix + deterministic scatter, EB elements per CTA pass.
 //
 // Replaces the per-pair form calls of Discretization::assemble
 // (src/discretization.cc:290-325) with int_grad_u_grad_v / int_u_v / int_F_v
@@ -16,20 +16,24 @@
 // d_r phi_i(q) is a product of 1D table entries.  Work per element is
 // O(nq p^6) instead of the O(nq^3 p^6) of the dense per-pair loops.
 //
+// A CTA works on EB elements at once: every stage is one flat loop over
+// (element, item), so each block barrier is paid once per batch.
+//
 // Scatter.  Entry (a, b) of the element's assembly list goes to
 // Ax[Ap[dof_b] + off[b][a]] (CSC: column = trial DOF).  Elements of one
 // colour share no DOF, so the read-modify-write needs no atomics and the
 // summation order of every entry (colour order) is fixed: bitwise
-// reproducible.  Dirichlet lifting follows src/discretization.cc:316-317,
-// RHS follows :329-338 (lifting only enters the RHS when a linear form is
-// set, as in the reference).
+// reproducible.  Each thread issues the loads of a chunk of targets before
+// any store.  Dirichlet lifting follows src/discretization.cc:316-317, the
+// RHS :329-338 (lifting only enters the RHS when a linear form is set, as
+// in the reference).
 #pragma once
 
 #include "common.cuh"
 
 namespace h3dg {
 
-template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ>
+template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ, int EB>
 struct SfShape {
 	static constexpr int NX = PX + 1, NY = PY + 1, NZ = PZ + 1;
 	static constexpr int NL = NX * NY * NZ;
@@ -45,18 +49,20 @@ struct SfShape {
 	static constexpr int WX = 4 * NX * NX * NQX, WY = 4 * NY * NY * NQY, WZ = 4 * NZ * NZ * NQZ;
 	static constexpr int T1N = NQX * NQY * NZ * NZ;
 	static constexpr int T2N = NQX * NY * NY * NZ * NZ;
-	// shared memory in doubles
+	// per-element work area: [G (8 NQ) | T1 | T2] during the terms, reused for A (NL^2) after
+	static constexpr int WORK = (8 * NQ + T1N + T2N) > NL * NL ? (8 * NQ + T1N + T2N) : NL * NL;
+	static constexpr int E_G = 0, E_T1 = 8 * NQ, E_T2 = E_T1 + T1N, E_A = 0;
+	static constexpr int E_F = WORK;            // NL
+	static constexpr int E_X = E_F + NL;        // 24
+	static constexpr int E_C = E_X + 24;        // NL coefficients
+	static constexpr int E_CS = E_C + NL;       // NL column starts (int64)
+	static constexpr int E_CE = E_CS + NL;      // NL column ends (int64)
+	static constexpr int E_I = E_CE + NL;       // ints: dof NL, s NL (NL doubles)
+	static constexpr int E_SIZE = (E_I + NL + 1) & ~1;
 	static constexpr int S_TAB = 0;
 	static constexpr int S_W = S_TAB + TABP;
-	static constexpr int S_G = S_W + WX + WY + WZ;          // 8 x NQ
-	static constexpr int S_T1 = S_G + 8 * NQ;
-	static constexpr int S_T2 = S_T1 + T1N;
-	static constexpr int S_A = S_T2 + T2N;                  // NL x NL
-	static constexpr int S_F = S_A + NL * NL;
-	static constexpr int S_X = S_F + NL;                    // 24
-	static constexpr int S_C = S_X + 24;                    // NL coefs
-	static constexpr int S_I = S_C + NL;                    // ints: dof NL, s NL
-	static constexpr int SMEM_DOUBLES = S_I + NL;           // 2 NL ints = NL doubles
+	static constexpr int S_E = S_W + WX + WY + WZ;
+	static constexpr int SMEM_DOUBLES = S_E + EB * E_SIZE;
 	static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES;
 };
 
@@ -68,20 +74,20 @@ __device__ __constant__ int kTermFlags[7][3] = {
 	{ 0, 0, 0 }                               // mass
 };
 
-template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ, int NT>
+template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ, int NT, int EB>
 __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, int64_t kend) {
-	using S = SfShape<PX, PY, PZ, NQX, NQY, NQZ>;
+	using S = SfShape<PX, PY, PZ, NQX, NQY, NQZ, EB>;
 	constexpr int NX = S::NX, NY = S::NY, NZ = S::NZ, NL = S::NL, NQ = S::NQ;
-	constexpr int NACC = (NL * NL + NT - 1) / NT;
-	extern __shared__ __align__(16) double sm[];
+	constexpr int NL2 = NL * NL;
+	constexpr int NACC = (EB * NL2 + NT - 1) / NT;
+	constexpr int CH = 8;   // scatter chunk: loads in flight per thread
+	extern __shared__ __align__(128) double sm[];
 	__shared__ uint64_t bar;
+	__shared__ int s_m[EB], s_l[EB];
+	__shared__ double s_cg[EB];
 	double *tab = sm + S::S_TAB;
 	double *Wx = sm + S::S_W, *Wy = Wx + S::WX, *Wz = Wy + S::WY;
-	double *G = sm + S::S_G;
-	double *T1 = sm + S::S_T1, *T2 = sm + S::S_T2;
-	double *A = sm + S::S_A, *F = sm + S::S_F, *X = sm + S::S_X, *ec = sm + S::S_C;
-	int *edof = reinterpret_cast<int *>(sm + S::S_I);
-	int *es = edof + NL;
+	double *E0 = sm + S::S_E;
 	const int tid = threadIdx.x;
 
 	if (!stage_tables(tab, args.tables, args.table_bytes, &bar, args.status)) return;
@@ -108,20 +114,43 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 	__syncthreads();
 
 	const int nterms = args.mass ? 7 : 6;
-	for (int64_t k = kbeg + blockIdx.x; k < kend; k += gridDim.x) {
+	const bool do_rhs = args.rhs && args.lf;
+	const int64_t nbatch = (kend - kbeg + EB - 1) / EB;
+	for (int64_t bt = blockIdx.x; bt < nbatch; bt += gridDim.x) {
+		const int64_t k0 = kbeg + bt * EB;
+		const int ne = (int) (kend - k0 < EB ? kend - k0 : EB);
+
 		// ---- element data
-		if (tid < 24) X[tid] = args.xyz[3 * (int64_t) args.el_vtx[8 * k + tid / 3] + tid % 3];
-		for (int i = tid; i < NL; i += NT) {
-			ec[i] = args.el_coef[k * NL + i];
-			edof[i] = args.el_dof[k * NL + i];
-			es[i] = args.el_s[k * NL + i];
+		if (tid < EB) {
+			const bool live = tid < ne;
+			s_m[tid] = live ? args.el_cnt[2 * (k0 + tid)] : 0;
+			s_l[tid] = live ? args.el_cnt[2 * (k0 + tid) + 1] : 0;
+			s_cg[tid] = live && args.ecoef ? args.ecoef[args.el_id[k0 + tid]] : 1.0;
 		}
-		const int mcnt = args.el_cnt[2 * k], lcnt = args.el_cnt[2 * k + 1];
-		const double cgrad = args.ecoef ? args.ecoef[args.el_id[k]] : 1.0;
+		for (int i = tid; i < EB * 24; i += NT) {
+			const int e = i / 24, r = i % 24;
+			E0[e * S::E_SIZE + S::E_X + r] = e < ne ? args.xyz[3 * (int64_t) args.el_vtx[8 * (k0 + e) + r / 3] + r % 3] : 0.0;
+		}
+		for (int i = tid; i < EB * NL; i += NT) {
+			const int e = i / NL, j = i % NL;
+			double *Eb = E0 + e * S::E_SIZE;
+			int *ei = reinterpret_cast<int *>(Eb + S::E_I);
+			const int64_t g = (k0 + e) * NL + j;
+			const int dof = e < ne ? args.el_dof[g] : -1;
+			Eb[S::E_C + j] = e < ne ? args.el_coef[g] : 0.0;
+			ei[j] = dof;
+			ei[NL + j] = e < ne ? args.el_s[g] : 0;
+			int64_t *cs = reinterpret_cast<int64_t *>(Eb + S::E_CS);
+			cs[j] = dof >= 0 ? args.Ap[dof] : 0;
+			cs[NL + j] = dof >= 0 ? args.Ap[dof + 1] : 0;
+		}
 		__syncthreads();
 
 		// ---- geometry at the quadrature points -> term weights
-		for (int q = tid; q < NQ; q += NT) {
+		for (int i = tid; i < EB * NQ; i += NT) {
+			const int e = i / NQ, q = i % NQ;
+			double *Eb = E0 + e * S::E_SIZE;
+			double *G = Eb + S::E_G;
 			const int q1 = q / (NQY * NQZ), q2 = (q / NQZ) % NQY, q3 = q % NQZ;
 			const double vx[2] = { tab[S::OVX + q1], tab[S::OVX + NQX + q1] };
 			const double dx[2] = { tab[S::ODX + q1], tab[S::ODX + NQX + q1] };
@@ -130,14 +159,14 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 			const double vz[2] = { tab[S::OVZ + q3], tab[S::OVZ + NQZ + q3] };
 			const double dz[2] = { tab[S::ODZ + q3], tab[S::ODZ + NQZ + q3] };
 			double m[3][3], det, irm[3][3], xp[3];
-			refmap_point(X, vx, dx, vy, dy, vz, dz, m, det, irm, xp);
+			refmap_point(Eb + S::E_X, vx, dx, vy, dy, vz, dz, m, det, irm, xp);
 			const double wd = tab[S::OWX + q1] * tab[S::OWY + q2] * tab[S::OWZ + q3] * det;
 			double g[3][3];
 #pragma unroll
 			for (int c = 0; c < 3; c++)
 #pragma unroll
 				for (int d = c; d < 3; d++) g[c][d] = irm[0][c] * irm[0][d] + irm[1][c] * irm[1][d] + irm[2][c] * irm[2][d];
-			const double s = wd * cgrad;
+			const double s = wd * s_cg[e];
 			G[0 * NQ + q] = 0.5 * s * g[0][0];
 			G[1 * NQ + q] = 0.5 * s * g[1][1];
 			G[2 * NQ + q] = 0.5 * s * g[2][2];
@@ -149,46 +178,72 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 		}
 		__syncthreads();
 
+		// element load vectors F_i = sum_q (w det f)(q) phi_i(q)
+		if (do_rhs) {
+			for (int i = tid; i < EB * NL; i += NT) {
+				const int e = i / NL, j = i % NL;
+				double *Eb = E0 + e * S::E_SIZE;
+				const double *src = Eb + S::E_G + 7 * NQ;
+				const int a = j / (NY * NZ), b = (j / NZ) % NY, c = j % NZ;
+				double s = 0.0;
+				for (int q1 = 0; q1 < NQX; q1++) {
+					double s1 = 0.0;
+					for (int q2 = 0; q2 < NQY; q2++) {
+						double s2 = 0.0;
+#pragma unroll
+						for (int q3 = 0; q3 < NQZ; q3++) s2 += src[(q1 * NQY + q2) * NQZ + q3] * tab[S::OVZ + c * NQZ + q3];
+						s1 += s2 * tab[S::OVY + b * NQY + q2];
+					}
+					s += s1 * tab[S::OVX + a * NQX + q1];
+				}
+				Eb[S::E_F + j] = s;
+			}
+		}
+
 		double acc[NACC];
 #pragma unroll
 		for (int r = 0; r < NACC; r++) acc[r] = 0.0;
 
 		for (int t = 0; t < nterms; t++) {
 			const int fx = kTermFlags[t][0], fy = kTermFlags[t][1], fz = kTermFlags[t][2];
-			const double *Gt = G + t * NQ;
 			const double *wx = Wx + fx * NX * NX * NQX;
 			const double *wy = Wy + fy * NY * NY * NQY;
 			const double *wz = Wz + fz * NZ * NZ * NQZ;
 			// stage 1: T1[q1][q2][c][c'] = sum_q3 G[q1][q2][q3] Wz[c][c'][q3]
-			for (int i = tid; i < S::T1N; i += NT) {
-				const int cc = i % (NZ * NZ), q12 = i / (NZ * NZ);
-				const double *gp = Gt + q12 * NQZ, *wp = wz + cc * NQZ;
+			for (int i = tid; i < EB * S::T1N; i += NT) {
+				const int e = i / S::T1N, ii = i % S::T1N;
+				double *Eb = E0 + e * S::E_SIZE;
+				const int cc = ii % (NZ * NZ), q12 = ii / (NZ * NZ);
+				const double *gp = Eb + S::E_G + t * NQ + q12 * NQZ, *wp = wz + cc * NQZ;
 				double s = 0.0;
 #pragma unroll
 				for (int q3 = 0; q3 < NQZ; q3++) s += gp[q3] * wp[q3];
-				T1[i] = s;
+				Eb[S::E_T1 + ii] = s;
 			}
 			__syncthreads();
 			// stage 2: T2[q1][b][b'][c][c'] = sum_q2 Wy[b][b'][q2] T1[q1][q2][c][c']
-			for (int i = tid; i < S::T2N; i += NT) {
-				const int cc = i % (NZ * NZ), bb = (i / (NZ * NZ)) % (NY * NY), q1 = i / (NZ * NZ * NY * NY);
-				const double *wp = wy + bb * NQY, *tp = T1 + q1 * NQY * NZ * NZ + cc;
+			for (int i = tid; i < EB * S::T2N; i += NT) {
+				const int e = i / S::T2N, ii = i % S::T2N;
+				double *Eb = E0 + e * S::E_SIZE;
+				const int cc = ii % (NZ * NZ), bb = (ii / (NZ * NZ)) % (NY * NY), q1 = ii / (NZ * NZ * NY * NY);
+				const double *wp = wy + bb * NQY, *tp = Eb + S::E_T1 + q1 * NQY * NZ * NZ + cc;
 				double s = 0.0;
 #pragma unroll
 				for (int q2 = 0; q2 < NQY; q2++) s += wp[q2] * tp[q2 * NZ * NZ];
-				T2[i] = s;
+				Eb[S::E_T2 + ii] = s;
 			}
 			__syncthreads();
 			// stage 3: A[(a,b,c)][(a',b',c')] += sum_q1 Wx[a][a'][q1] T2[q1][b][b'][c][c']
 #pragma unroll
 			for (int r = 0; r < NACC; r++) {
 				const int idx = tid + r * NT;
-				if (NL * NL % NT == 0 || idx < NL * NL) {
-					const int i = idx / NL, j = idx % NL;
+				if ((EB * NL2) % NT == 0 || idx < EB * NL2) {
+					const int e = idx / NL2, ij = idx % NL2;
+					const int i = ij / NL, j = ij % NL;
 					const int a = i / (NY * NZ), b = (i / NZ) % NY, c = i % NZ;
 					const int a2 = j / (NY * NZ), b2 = (j / NZ) % NY, c2 = j % NZ;
 					const double *wp = wx + (a * NX + a2) * NQX;
-					const double *tp = T2 + ((b * NY + b2) * NZ + c) * NZ + c2;
+					const double *tp = E0 + e * S::E_SIZE + S::E_T2 + ((b * NY + b2) * NZ + c) * NZ + c2;
 					double s = acc[r];
 #pragma unroll
 					for (int q1 = 0; q1 < NQX; q1++) s += wp[q1] * tp[q1 * NY * NY * NZ * NZ];
@@ -197,47 +252,68 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 			}
 			__syncthreads();
 		}
+		// A overwrites the G/T1/T2 work area (F already computed)
 #pragma unroll
 		for (int r = 0; r < NACC; r++) {
 			const int idx = tid + r * NT;
-			if (NL * NL % NT == 0 || idx < NL * NL) A[idx] = acc[r];
-		}
-		// element load vector F_i = sum_q (w det f)(q) phi_i(q)
-		if (args.rhs && args.lf) {
-			for (int i = tid; i < NL; i += NT) {
-				const int a = i / (NY * NZ), b = (i / NZ) % NY, c = i % NZ;
-				double s = 0.0;
-				for (int q = 0; q < NQ; q++) {
-					const int q1 = q / (NQY * NQZ), q2 = (q / NQZ) % NQY, q3 = q % NQZ;
-					s += G[7 * NQ + q] * tab[S::OVX + a * NQX + q1] * tab[S::OVY + b * NQY + q2] * tab[S::OVZ + c * NQZ + q3];
-				}
-				F[i] = s;
+			if ((EB * NL2) % NT == 0 || idx < EB * NL2) {
+				const int e = idx / NL2, ij = idx % NL2;
+				E0[e * S::E_SIZE + S::E_A + ij] = acc[r];
 			}
 		}
 		__syncthreads();
 
 		// ---- scatter into the CSC matrix (exclusive within a colour)
 		if (args.Ax) {
-			const uint16_t *off = args.el_off + k * NL * NL;
-			for (int p = tid; p < mcnt * mcnt; p += NT) {
-				const int b = p / mcnt, a = p % mcnt;
-				const int sa = es[a], sb = es[b];
-				const double v = ec[a] * ec[b] * (A[sa * NL + sb] + A[sb * NL + sa]);
-				const int64_t c0 = args.Ap[edof[b]], pos = c0 + off[b * NL + a];
-				if (pos < args.Ap[edof[b] + 1]) args.Ax[pos] += v;
-				else atomicOr(args.status, kErrBounds);
+			double *__restrict__ Ax = args.Ax;
+			for (int base = 0; base < EB * NL2; base += NT * CH) {
+				int64_t pos[CH];
+				double val[CH], old[CH];
+#pragma unroll
+				for (int r = 0; r < CH; r++) {
+					const int p = base + tid + r * NT;
+					pos[r] = -1;
+					val[r] = 0.0;
+					if (p < EB * NL2) {
+						const int e = p / NL2, pp = p % NL2;
+						const int m = s_m[e];
+						if (pp < m * m) {
+							const double *Eb = E0 + e * S::E_SIZE;
+							const int *ei = reinterpret_cast<const int *>(Eb + S::E_I);
+							const int64_t *cs = reinterpret_cast<const int64_t *>(Eb + S::E_CS);
+							const int b = pp / m, a = pp % m;
+							const int sa = ei[NL + a], sb = ei[NL + b];
+							const double *A = Eb + S::E_A;
+							val[r] = Eb[S::E_C + a] * Eb[S::E_C + b] * (A[sa * NL + sb] + A[sb * NL + sa]);
+							const int64_t t = cs[b] + args.el_off[(k0 + e) * NL2 + b * NL + a];
+							if (t < cs[NL + b]) pos[r] = t;
+							else atomicOr(args.status, kErrBounds);
+						}
+					}
+				}
+#pragma unroll
+				for (int r = 0; r < CH; r++) old[r] = pos[r] >= 0 ? Ax[pos[r]] : 0.0;
+#pragma unroll
+				for (int r = 0; r < CH; r++)
+					if (pos[r] >= 0) Ax[pos[r]] = old[r] + val[r];
 			}
 		}
-		if (args.rhs && args.lf) {
-			for (int a = tid; a < mcnt; a += NT) {
-				const int sa = es[a];
+		if (do_rhs) {
+			for (int i = tid; i < EB * NL; i += NT) {
+				const int e = i / NL, a = i % NL;
+				if (a >= s_m[e]) continue;
+				const double *Eb = E0 + e * S::E_SIZE;
+				const int *ei = reinterpret_cast<const int *>(Eb + S::E_I);
+				const double *A = Eb + S::E_A;
+				const int sa = ei[NL + a];
+				const double ca = Eb[S::E_C + a];
 				double lr = 0.0;
-				for (int j = mcnt; j < mcnt + lcnt; j++) {
-					const int sj = es[j];
-					lr -= ec[a] * ec[j] * (A[sa * NL + sj] + A[sj * NL + sa]);
+				for (int j = s_m[e]; j < s_m[e] + s_l[e]; j++) {
+					const int sj = ei[NL + j];
+					lr -= ca * Eb[S::E_C + j] * (A[sa * NL + sj] + A[sj * NL + sa]);
 				}
-				lr += F[sa] * ec[a];
-				args.rhs[edof[a]] += lr;
+				lr += Eb[S::E_F + sa] * ca;
+				args.rhs[ei[a]] += lr;
 			}
 		}
 		__syncthreads();

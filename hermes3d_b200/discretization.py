@@ -251,6 +251,11 @@ class Discretization:
         capi.call("h3dg_disc_kernel_times", self.handle, buf, cap, C.byref(n))
         return [buf[i] for i in range(n.value)]
 
+    def tuning(self):
+        t, e, ms = C.c_int32(), C.c_int32(), C.c_float()
+        capi.call("h3dg_disc_get_tuning", self.handle, C.byref(t), C.byref(e), C.byref(ms))
+        return {"threads": t.value, "elems_per_cta": e.value, "ms": ms.value}
+
     def last_launch_count(self):
         n = C.c_int32()
         capi.call("h3dg_disc_last_launch_count", self.handle, C.byref(n))

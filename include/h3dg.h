@@ -136,6 +136,12 @@ h3dg_status h3dg_disc_update_coefficients(h3dg_disc *disc, const double *elem_co
 /* number of kernels launched by the last assemble call */
 h3dg_status h3dg_disc_last_launch_count(const h3dg_disc *disc, int32_t *count);
 
+/* the kernel variant the autotuner picked on the first assembly of the
+ * current plan: threads per CTA, elements per CTA pass, and the time of one
+ * assembly with it in milliseconds (all -1 / 0 before the first assembly).
+ * No reference counterpart. */
+h3dg_status h3dg_disc_get_tuning(const h3dg_disc *disc, int32_t *threads, int32_t *elems_per_cta, float *ms);
+
 /* Kernel-only timing (no reference counterpart; a measurement hook): when
  * enabled with capacity n, each assemble call records a CUDA event pair on its
  * launch stream around its kernel launches (after the output zeroing), up to
