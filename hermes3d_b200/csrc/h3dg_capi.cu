@@ -3,6 +3,7 @@
 #include "host/h3dg_host.h"
 #include "host/lobatto.h"
 #include "kernels/asm_fp64.cuh"
+#include "kernels/asm_fp64_seq.cuh"
 #include "kernels/geom.cuh"
 
 #include <cuda_runtime.h>
@@ -401,18 +402,24 @@ KernelSpec spec() {
 	                    h3dg::SfShape<P, P, P, NQ, NQ, NQ, EB>::SMEM_BYTES, false };
 }
 
+template <int P, int NQ, int NT, int EB>
+KernelSpec spec_seq() {
+	return KernelSpec { P, NQ, &h3dg::k_assemble_fp64_seq<P, P, P, NQ, NQ, NQ, NT, EB>, NT, EB,
+	                    h3dg::SfShapeSeq<P, P, P, NQ, NQ, NQ, EB>::SMEM_BYTES, false };
+}
+
 // FP64 kernel variants per (order, points); the autotuner times each on the
 // actual plan at the first assembly and keeps the fastest.
 std::vector<KernelSpec> &kernel_table() {
 	static std::vector<KernelSpec> t = {
-		spec<1, 2, 128, 8>(), spec<1, 3, 128, 8>(),
-		spec<2, 3, 128, 2>(), spec<2, 3, 256, 4>(),
-		spec<2, 4, 128, 1>(), spec<2, 4, 128, 2>(), spec<2, 4, 256, 4>(), spec<2, 4, 256, 8>(),
-		spec<2, 5, 128, 2>(), spec<2, 5, 256, 4>(),
-		spec<3, 4, 256, 1>(), spec<3, 4, 256, 2>(),
-		spec<3, 5, 256, 1>(), spec<3, 5, 256, 2>(), spec<3, 5, 512, 2>(),
-		spec<3, 6, 256, 1>(), spec<3, 6, 256, 2>(),
-		spec<4, 5, 512, 1>(), spec<4, 6, 512, 1>(),
+		spec<1, 2, 128, 4>(), spec<1, 3, 128, 4>(),
+		spec<2, 3, 128, 1>(), spec<2, 3, 128, 2>(),
+		spec<2, 4, 128, 1>(), spec<2, 4, 128, 2>(), spec<2, 4, 256, 2>(), spec<2, 4, 256, 3>(),
+		spec<2, 5, 128, 1>(), spec<2, 5, 256, 2>(),
+		spec<3, 4, 256, 1>(), spec<3, 4, 512, 1>(),
+		spec<3, 5, 256, 1>(), spec<3, 5, 512, 1>(), spec_seq<3, 5, 256, 1>(),
+		spec<3, 6, 256, 1>(), spec<3, 6, 512, 1>(),
+		spec_seq<4, 5, 512, 1>(), spec_seq<4, 6, 512, 1>(),
 	};
 	return t;
 }

@@ -12,12 +12,16 @@
 // It is formed as K = A + A^T with
 //     A = sum_r (G_rr/2) B_r^T B_r + sum_{r<s} G_rs B_r^T B_s  (+ (M/2) V^T V)
 // and every one of the 7 terms is contracted by sum factorisation over the
-// three quadrature directions (q3, then q2, then q1), because each factor
-// d_r phi_i(q) is a product of 1D table entries.  Work per element is
-// O(nq p^6) instead of the O(nq^3 p^6) of the dense per-pair loops.
-//
-// A CTA works on EB elements at once: every stage is one flat loop over
-// (element, item), so each block barrier is paid once per batch.
+// three quadrature directions, because each factor d_r phi_i(q) is a
+// product of 1D table entries:
+//   stage 1  T1_t[q1][q2][c][c'] = sum_q3 G_t[q1][q2][q3] Wz_t[c][c'][q3]
+//   stage 2  T2_t[q1][b][b'][cc'] = sum_q2 Wy_t[b][b'][q2] T1_t[q1][q2][cc']
+//   stage 3  A[(a,b,c)][(a',b',c')] = sum_t sum_q1 Wx_t[a][a'][q1] T2_t[q1][bb'cc']
+// Work per element is O(nq p^6) instead of the O(nq^3 p^6) of the dense
+// per-pair loops.  Stages 1 and 2 run for all terms at once (3 block
+// barriers per batch); in stage 3 each thread owns one (b,b',c,c') column
+// and keeps the (a,a') rows in registers, so the W tables are read as
+// broadcasts and each T2 value is loaded once per term.
 //
 // Scatter.  Entry (a, b) of the element's assembly list goes to
 // Ax[Ap[dof_b] + off[b][a]] (CSC: column = trial DOF).  Elements of one
@@ -38,6 +42,7 @@ struct SfShape {
 	static constexpr int NX = PX + 1, NY = PY + 1, NZ = PZ + 1;
 	static constexpr int NL = NX * NY * NZ;
 	static constexpr int NQ = NQX * NQY * NQZ;
+	static constexpr int NT_TERMS = 7;
 	// 1D tables blob: Vx Dx Vy Dy Vz Dz (k-major, q fastest) then q/w per direction
 	static constexpr int OVX = 0, ODX = OVX + NX * NQX, OVY = ODX + NX * NQX, ODY = OVY + NY * NQY;
 	static constexpr int OVZ = ODY + NY * NQY, ODZ = OVZ + NZ * NQZ;
@@ -47,12 +52,18 @@ struct SfShape {
 	static constexpr int TABP = (TAB + 1) & ~1;
 	// products W^f[k][k'][q] = E^(f>>1)[k][q] E^(f&1)[k'][q], E^0 = V, E^1 = D
 	static constexpr int WX = 4 * NX * NX * NQX, WY = 4 * NY * NY * NQY, WZ = 4 * NZ * NZ * NQZ;
-	static constexpr int T1N = NQX * NQY * NZ * NZ;
-	static constexpr int T2N = NQX * NY * NY * NZ * NZ;
-	// per-element work area: [G (8 NQ) | T1 | T2] during the terms, reused for A (NL^2) after
-	static constexpr int WORK = (8 * NQ + T1N + T2N) > NL * NL ? (8 * NQ + T1N + T2N) : NL * NL;
-	static constexpr int E_G = 0, E_T1 = 8 * NQ, E_T2 = E_T1 + T1N, E_A = 0;
-	static constexpr int E_F = WORK;            // NL
+	static constexpr int T1N = NQX * NQY * NZ * NZ;           // per term
+	static constexpr int T2N = NQX * NY * NY * NZ * NZ;       // per term
+	static constexpr int COLS = NY * NY * NZ * NZ;            // stage-3 columns (b,b',c,c')
+	// per-element area: [G (8 NQ) | T1 (7 terms)] then T2 (7 terms).  A (NL^2)
+	// is written at offset 0 by stage 3, which reads only T2: T2 starts past
+	// both, so A never overwrites data still being read.
+	static constexpr int E_G = 0;
+	static constexpr int E_T1 = 8 * NQ;
+	static constexpr int E_A = 0;
+	static constexpr int T1_END = E_T1 + NT_TERMS * T1N;
+	static constexpr int E_T2 = T1_END > NL * NL ? T1_END : NL * NL;
+	static constexpr int E_F = E_T2 + NT_TERMS * T2N;   // NL
 	static constexpr int E_X = E_F + NL;        // 24
 	static constexpr int E_C = E_X + 24;        // NL coefficients
 	static constexpr int E_CS = E_C + NL;       // NL column starts (int64)
@@ -79,8 +90,8 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 	using S = SfShape<PX, PY, PZ, NQX, NQY, NQZ, EB>;
 	constexpr int NX = S::NX, NY = S::NY, NZ = S::NZ, NL = S::NL, NQ = S::NQ;
 	constexpr int NL2 = NL * NL;
-	constexpr int NACC = (EB * NL2 + NT - 1) / NT;
-	constexpr int CH = 8;   // scatter chunk: loads in flight per thread
+	constexpr int COLS = S::COLS;
+	constexpr int CH = 4;   // scatter chunk: loads in flight per thread
 	extern __shared__ __align__(128) double sm[];
 	__shared__ uint64_t bar;
 	__shared__ int s_m[EB], s_l[EB];
@@ -178,7 +189,7 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 		}
 		__syncthreads();
 
-		// element load vectors F_i = sum_q (w det f)(q) phi_i(q)
+		// ---- element load vectors F_i = sum_q (w det f)(q) phi_i(q)
 		if (do_rhs) {
 			for (int i = tid; i < EB * NL; i += NT) {
 				const int e = i / NL, j = i % NL;
@@ -200,66 +211,76 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 			}
 		}
 
-		double acc[NACC];
+		// ---- stage 1, all terms: item (e, t, q1, q2) produces T1_t[q1][q2][*][*]
+		for (int i = tid; i < EB * nterms * NQX * NQY; i += NT) {
+			const int e = i / (nterms * NQX * NQY), r = i % (nterms * NQX * NQY);
+			const int t = r / (NQX * NQY), q12 = r % (NQX * NQY);
+			double *Eb = E0 + e * S::E_SIZE;
+			const double *gp = Eb + S::E_G + t * NQ + q12 * NQZ;
+			const double *wz = Wz + kTermFlags[t][2] * NZ * NZ * NQZ;
+			double g[NQZ];
 #pragma unroll
-		for (int r = 0; r < NACC; r++) acc[r] = 0.0;
-
-		for (int t = 0; t < nterms; t++) {
-			const int fx = kTermFlags[t][0], fy = kTermFlags[t][1], fz = kTermFlags[t][2];
-			const double *wx = Wx + fx * NX * NX * NQX;
-			const double *wy = Wy + fy * NY * NY * NQY;
-			const double *wz = Wz + fz * NZ * NZ * NQZ;
-			// stage 1: T1[q1][q2][c][c'] = sum_q3 G[q1][q2][q3] Wz[c][c'][q3]
-			for (int i = tid; i < EB * S::T1N; i += NT) {
-				const int e = i / S::T1N, ii = i % S::T1N;
-				double *Eb = E0 + e * S::E_SIZE;
-				const int cc = ii % (NZ * NZ), q12 = ii / (NZ * NZ);
-				const double *gp = Eb + S::E_G + t * NQ + q12 * NQZ, *wp = wz + cc * NQZ;
+			for (int q3 = 0; q3 < NQZ; q3++) g[q3] = gp[q3];
+			double *out = Eb + S::E_T1 + t * S::T1N + q12 * NZ * NZ;
+#pragma unroll
+			for (int cc = 0; cc < NZ * NZ; cc++) {
 				double s = 0.0;
 #pragma unroll
-				for (int q3 = 0; q3 < NQZ; q3++) s += gp[q3] * wp[q3];
-				Eb[S::E_T1 + ii] = s;
+				for (int q3 = 0; q3 < NQZ; q3++) s += g[q3] * wz[cc * NQZ + q3];
+				out[cc] = s;
 			}
-			__syncthreads();
-			// stage 2: T2[q1][b][b'][c][c'] = sum_q2 Wy[b][b'][q2] T1[q1][q2][c][c']
-			for (int i = tid; i < EB * S::T2N; i += NT) {
-				const int e = i / S::T2N, ii = i % S::T2N;
-				double *Eb = E0 + e * S::E_SIZE;
-				const int cc = ii % (NZ * NZ), bb = (ii / (NZ * NZ)) % (NY * NY), q1 = ii / (NZ * NZ * NY * NY);
-				const double *wp = wy + bb * NQY, *tp = Eb + S::E_T1 + q1 * NQY * NZ * NZ + cc;
+		}
+		__syncthreads();
+		// ---- stage 2, all terms: item (e, t, q1, cc) produces T2_t[q1][*][*][cc]
+		for (int i = tid; i < EB * nterms * NQX * NZ * NZ; i += NT) {
+			const int e = i / (nterms * NQX * NZ * NZ), r = i % (nterms * NQX * NZ * NZ);
+			const int t = r / (NQX * NZ * NZ), r2 = r % (NQX * NZ * NZ);
+			const int q1 = r2 / (NZ * NZ), cc = r2 % (NZ * NZ);
+			double *Eb = E0 + e * S::E_SIZE;
+			const double *tp = Eb + S::E_T1 + t * S::T1N + q1 * NQY * NZ * NZ + cc;
+			const double *wy = Wy + kTermFlags[t][1] * NY * NY * NQY;
+			double v[NQY];
+#pragma unroll
+			for (int q2 = 0; q2 < NQY; q2++) v[q2] = tp[q2 * NZ * NZ];
+			double *out = Eb + S::E_T2 + t * S::T2N + q1 * NY * NY * NZ * NZ + cc;
+#pragma unroll
+			for (int bb = 0; bb < NY * NY; bb++) {
 				double s = 0.0;
 #pragma unroll
-				for (int q2 = 0; q2 < NQY; q2++) s += wp[q2] * tp[q2 * NZ * NZ];
-				Eb[S::E_T2 + ii] = s;
+				for (int q2 = 0; q2 < NQY; q2++) s += wy[bb * NQY + q2] * v[q2];
+				out[bb * NZ * NZ] = s;
 			}
-			__syncthreads();
-			// stage 3: A[(a,b,c)][(a',b',c')] += sum_q1 Wx[a][a'][q1] T2[q1][b][b'][c][c']
+		}
+		__syncthreads();
+		// ---- stage 3: thread owns column (e, b, b', c, c'), rows (a, a') in registers
+		for (int i = tid; i < EB * COLS; i += NT) {
+			const int e = i / COLS, col = i % COLS;
+			double *Eb = E0 + e * S::E_SIZE;
+			double acc[NX * NX];
 #pragma unroll
-			for (int r = 0; r < NACC; r++) {
-				const int idx = tid + r * NT;
-				if ((EB * NL2) % NT == 0 || idx < EB * NL2) {
-					const int e = idx / NL2, ij = idx % NL2;
-					const int i = ij / NL, j = ij % NL;
-					const int a = i / (NY * NZ), b = (i / NZ) % NY, c = i % NZ;
-					const int a2 = j / (NY * NZ), b2 = (j / NZ) % NY, c2 = j % NZ;
-					const double *wp = wx + (a * NX + a2) * NQX;
-					const double *tp = E0 + e * S::E_SIZE + S::E_T2 + ((b * NY + b2) * NZ + c) * NZ + c2;
+			for (int r = 0; r < NX * NX; r++) acc[r] = 0.0;
+			for (int t = 0; t < nterms; t++) {
+				const double *tp = Eb + S::E_T2 + t * S::T2N + col;
+				const double *wx = Wx + kTermFlags[t][0] * NX * NX * NQX;
+				double v[NQX];
+#pragma unroll
+				for (int q1 = 0; q1 < NQX; q1++) v[q1] = tp[q1 * COLS];
+#pragma unroll
+				for (int r = 0; r < NX * NX; r++) {
 					double s = acc[r];
 #pragma unroll
-					for (int q1 = 0; q1 < NQX; q1++) s += wp[q1] * tp[q1 * NY * NY * NZ * NZ];
+					for (int q1 = 0; q1 < NQX; q1++) s += wx[r * NQX + q1] * v[q1];
 					acc[r] = s;
 				}
 			}
-			__syncthreads();
-		}
-		// A overwrites the G/T1/T2 work area (F already computed)
+			const int bb = col / (NZ * NZ), cc = col % (NZ * NZ);
+			const int b = bb / NY, b2 = bb % NY, c = cc / NZ, c2 = cc % NZ;
+			double *A = Eb + S::E_A;
 #pragma unroll
-		for (int r = 0; r < NACC; r++) {
-			const int idx = tid + r * NT;
-			if ((EB * NL2) % NT == 0 || idx < EB * NL2) {
-				const int e = idx / NL2, ij = idx % NL2;
-				E0[e * S::E_SIZE + S::E_A + ij] = acc[r];
-			}
+			for (int a = 0; a < NX; a++)
+#pragma unroll
+				for (int a2 = 0; a2 < NX; a2++)
+					A[((a * NY + b) * NZ + c) * NL + (a2 * NY + b2) * NZ + c2] = acc[a * NX + a2];
 		}
 		__syncthreads();
 
