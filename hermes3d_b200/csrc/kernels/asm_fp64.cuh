@@ -27,8 +27,9 @@
 // Ax[Ap[dof_b] + off[b][a]] (CSC: column = trial DOF).  Elements of one
 // colour share no DOF, so the read-modify-write needs no atomics and the
 // summation order of every entry (colour order) is fixed: bitwise
-// reproducible.  Each thread issues the loads of a chunk of targets before
-// any store.  Dirichlet lifting follows src/discretization.cc:316-317, the
+// reproducible.  The add is a posted reduction (red.global.add.f64): no
+// two elements of a launch target the same entry, so it changes nothing in
+// the arithmetic and lets the thread move on without waiting for the line.  Dirichlet lifting follows src/discretization.cc:316-317, the
 // RHS :329-338 (lifting only enters the RHS when a linear form is set, as
 // in the reference).
 #pragma once
@@ -91,7 +92,7 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 	constexpr int NX = S::NX, NY = S::NY, NZ = S::NZ, NL = S::NL, NQ = S::NQ;
 	constexpr int NL2 = NL * NL;
 	constexpr int COLS = S::COLS;
-	constexpr int CH = 4;   // scatter chunk: loads in flight per thread
+	constexpr int CH = 4;   // scatter chunk per thread
 	extern __shared__ __align__(128) double sm[];
 	__shared__ uint64_t bar;
 	__shared__ int s_m[EB], s_l[EB];
@@ -289,7 +290,7 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 			double *__restrict__ Ax = args.Ax;
 			for (int base = 0; base < EB * NL2; base += NT * CH) {
 				int64_t pos[CH];
-				double val[CH], old[CH];
+				double val[CH];
 #pragma unroll
 				for (int r = 0; r < CH; r++) {
 					const int p = base + tid + r * NT;
@@ -313,10 +314,8 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 					}
 				}
 #pragma unroll
-				for (int r = 0; r < CH; r++) old[r] = pos[r] >= 0 ? Ax[pos[r]] : 0.0;
-#pragma unroll
 				for (int r = 0; r < CH; r++)
-					if (pos[r] >= 0) Ax[pos[r]] = old[r] + val[r];
+					if (pos[r] >= 0) posted_add(Ax + pos[r], val[r]);
 			}
 		}
 		if (do_rhs) {
@@ -334,7 +333,7 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 					lr -= ca * Eb[S::E_C + j] * (A[sa * NL + sj] + A[sj * NL + sa]);
 				}
 				lr += Eb[S::E_F + sa] * ca;
-				args.rhs[ei[a]] += lr;
+				posted_add(args.rhs + ei[a], lr);
 			}
 		}
 		__syncthreads();

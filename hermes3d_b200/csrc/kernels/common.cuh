@@ -141,6 +141,15 @@ __device__ __forceinline__ void refmap_point(const double *X, const double vx[2]
 	irm[2][2] = (m[0][0] * m[1][1] - m[0][1] * m[1][0]) * ij;
 }
 
+// Posted add to global memory (no value returned, so the issuing thread does
+// not wait for it).  Used for the colour-exclusive scatter: within one
+// launch every target address receives at most one add, and launches are
+// ordered on the stream, so the summation order of each entry is the colour
+// order whatever the scheduling -- the result is bitwise reproducible.
+__device__ __forceinline__ void posted_add(double *addr, double v) {
+	asm volatile("red.global.add.f64 [%0], %1;" ::"l"(addr), "d"(v) : "memory");
+}
+
 __device__ __forceinline__ double source_value(int lf, double value, const double xp[3]) {
 	if (lf == 1) return value;
 	if (lf == 2) {
