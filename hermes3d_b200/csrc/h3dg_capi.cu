@@ -412,14 +412,12 @@ KernelSpec spec_seq() {
 // actual plan at the first assembly and keeps the fastest.
 std::vector<KernelSpec> &kernel_table() {
 	static std::vector<KernelSpec> t = {
-		spec<1, 2, 128, 4>(), spec<1, 3, 128, 4>(),
-		spec<2, 3, 128, 1>(), spec<2, 3, 128, 2>(),
-		spec<2, 4, 128, 1>(), spec<2, 4, 128, 2>(), spec<2, 4, 256, 2>(), spec<2, 4, 256, 3>(),
-		spec<2, 5, 128, 1>(), spec<2, 5, 256, 2>(),
-		spec<3, 4, 256, 1>(), spec<3, 4, 512, 1>(),
-		spec<3, 5, 256, 1>(), spec<3, 5, 512, 1>(), spec_seq<3, 5, 256, 1>(),
-		spec<3, 6, 256, 1>(), spec<3, 6, 512, 1>(),
-		spec_seq<4, 5, 512, 1>(), spec_seq<4, 6, 512, 1>(),
+		spec<1, 2, 64, 4>(), spec<1, 3, 64, 4>(), spec<1, 2, 128, 8>(), spec<1, 3, 128, 8>(),
+		spec<2, 3, 96, 1>(), spec<2, 3, 192, 2>(),
+		spec<2, 4, 96, 1>(), spec<2, 4, 128, 1>(), spec<2, 4, 192, 2>(), spec<2, 4, 256, 3>(),
+		spec<2, 5, 96, 1>(), spec<2, 5, 192, 2>(),
+		spec<3, 4, 256, 1>(), spec<3, 5, 256, 1>(), spec<3, 5, 512, 2>(), spec<3, 6, 256, 1>(),
+		spec<4, 5, 640, 1>(), spec<4, 6, 640, 1>(), spec_seq<4, 6, 512, 1>(),
 	};
 	return t;
 }

@@ -18,10 +18,10 @@
 //   stage 2  T2_t[q1][b][b'][cc'] = sum_q2 Wy_t[b][b'][q2] T1_t[q1][q2][cc']
 //   stage 3  A[(a,b,c)][(a',b',c')] = sum_t sum_q1 Wx_t[a][a'][q1] T2_t[q1][bb'cc']
 // Work per element is O(nq p^6) instead of the O(nq^3 p^6) of the dense
-// per-pair loops.  Stages 1 and 2 run for all terms at once (3 block
-// barriers per batch); in stage 3 each thread owns one (b,b',c,c') column
-// and keeps the (a,a') rows in registers, so the W tables are read as
-// broadcasts and each T2 value is loaded once per term.
+// per-pair loops.  Stage 1 runs for all terms at once into shared memory;
+// in stages 2+3 each thread owns one (b,b',c,c') column, forms its T2 values
+// in registers (no T2 buffer, same FMA count) and keeps the (a,a') rows of
+// A in registers, so the Wx table is read as broadcasts.
 //
 // Scatter.  Entry (a, b) of the element's assembly list goes to
 // Ax[Ap[dof_b] + off[b][a]] (CSC: column = trial DOF).  Elements of one
@@ -56,15 +56,13 @@ struct SfShape {
 	static constexpr int T1N = NQX * NQY * NZ * NZ;           // per term
 	static constexpr int T2N = NQX * NY * NY * NZ * NZ;       // per term
 	static constexpr int COLS = NY * NY * NZ * NZ;            // stage-3 columns (b,b',c,c')
-	// per-element area: [G (8 NQ) | T1 (7 terms)] then T2 (7 terms).  A (NL^2)
-	// is written at offset 0 by stage 3, which reads only T2: T2 starts past
-	// both, so A never overwrites data still being read.
+	// per-element area: [G (8 NQ) | T1 (7 terms)]; A (NL^2) overwrites it once
+	// every thread has finished reading T1 (block barrier in between).
 	static constexpr int E_G = 0;
 	static constexpr int E_T1 = 8 * NQ;
 	static constexpr int E_A = 0;
 	static constexpr int T1_END = E_T1 + NT_TERMS * T1N;
-	static constexpr int E_T2 = T1_END > NL * NL ? T1_END : NL * NL;
-	static constexpr int E_F = E_T2 + NT_TERMS * T2N;   // NL
+	static constexpr int E_F = T1_END > NL * NL ? T1_END : NL * NL;   // NL
 	static constexpr int E_X = E_F + NL;        // 24
 	static constexpr int E_C = E_X + 24;        // NL coefficients
 	static constexpr int E_CS = E_C + NL;       // NL column starts (int64)
@@ -232,56 +230,53 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 			}
 		}
 		__syncthreads();
-		// ---- stage 2, all terms: item (e, t, q1, cc) produces T2_t[q1][*][*][cc]
-		for (int i = tid; i < EB * nterms * NQX * NZ * NZ; i += NT) {
-			const int e = i / (nterms * NQX * NZ * NZ), r = i % (nterms * NQX * NZ * NZ);
-			const int t = r / (NQX * NZ * NZ), r2 = r % (NQX * NZ * NZ);
-			const int q1 = r2 / (NZ * NZ), cc = r2 % (NZ * NZ);
-			double *Eb = E0 + e * S::E_SIZE;
-			const double *tp = Eb + S::E_T1 + t * S::T1N + q1 * NQY * NZ * NZ + cc;
-			const double *wy = Wy + kTermFlags[t][1] * NY * NY * NQY;
-			double v[NQY];
-#pragma unroll
-			for (int q2 = 0; q2 < NQY; q2++) v[q2] = tp[q2 * NZ * NZ];
-			double *out = Eb + S::E_T2 + t * S::T2N + q1 * NY * NY * NZ * NZ + cc;
-#pragma unroll
-			for (int bb = 0; bb < NY * NY; bb++) {
-				double s = 0.0;
-#pragma unroll
-				for (int q2 = 0; q2 < NQY; q2++) s += wy[bb * NQY + q2] * v[q2];
-				out[bb * NZ * NZ] = s;
-			}
-		}
-		__syncthreads();
-		// ---- stage 3: thread owns column (e, b, b', c, c'), rows (a, a') in registers
-		for (int i = tid; i < EB * COLS; i += NT) {
-			const int e = i / COLS, col = i % COLS;
-			double *Eb = E0 + e * S::E_SIZE;
+		// ---- stages 2+3: thread owns column (e, b, b', c, c'); per term it forms
+		// T2_t[q1][col] = sum_q2 Wy_t[b][b'][q2] T1_t[q1][q2][c][c'] in registers
+		// and accumulates A[(a,b,c)][(a',b',c')] for all (a, a') in registers.
+		{
+			static_assert(EB * COLS <= NT, "one stage-3 column per thread");
+			const int e = tid / COLS, col = tid % COLS;
+			const bool active = tid < EB * COLS;
 			double acc[NX * NX];
 #pragma unroll
 			for (int r = 0; r < NX * NX; r++) acc[r] = 0.0;
-			for (int t = 0; t < nterms; t++) {
-				const double *tp = Eb + S::E_T2 + t * S::T2N + col;
-				const double *wx = Wx + kTermFlags[t][0] * NX * NX * NQX;
-				double v[NQX];
+			const int bb = col / (NZ * NZ), cc = col % (NZ * NZ);
+			if (active) {
+				const double *Eb = E0 + e * S::E_SIZE;
+				for (int t = 0; t < nterms; t++) {
+					const double *wy = Wy + kTermFlags[t][1] * NY * NY * NQY + bb * NQY;
+					const double *wx = Wx + kTermFlags[t][0] * NX * NX * NQX;
+					const double *t1 = Eb + S::E_T1 + t * S::T1N + cc;
+					double wyr[NQY];
 #pragma unroll
-				for (int q1 = 0; q1 < NQX; q1++) v[q1] = tp[q1 * COLS];
+					for (int q2 = 0; q2 < NQY; q2++) wyr[q2] = wy[q2];
+					double v[NQX];
 #pragma unroll
-				for (int r = 0; r < NX * NX; r++) {
-					double s = acc[r];
+					for (int q1 = 0; q1 < NQX; q1++) {
+						double s2 = 0.0;
 #pragma unroll
-					for (int q1 = 0; q1 < NQX; q1++) s += wx[r * NQX + q1] * v[q1];
-					acc[r] = s;
+						for (int q2 = 0; q2 < NQY; q2++) s2 += wyr[q2] * t1[(q1 * NQY + q2) * NZ * NZ];
+						v[q1] = s2;
+					}
+#pragma unroll
+					for (int r = 0; r < NX * NX; r++) {
+						double s3 = acc[r];
+#pragma unroll
+						for (int q1 = 0; q1 < NQX; q1++) s3 += wx[r * NQX + q1] * v[q1];
+						acc[r] = s3;
+					}
 				}
 			}
-			const int bb = col / (NZ * NZ), cc = col % (NZ * NZ);
-			const int b = bb / NY, b2 = bb % NY, c = cc / NZ, c2 = cc % NZ;
-			double *A = Eb + S::E_A;
+			__syncthreads();   // T1 fully consumed: A may overwrite it
+			if (active) {
+				const int b = bb / NY, b2 = bb % NY, c = cc / NZ, c2 = cc % NZ;
+				double *A = E0 + e * S::E_SIZE + S::E_A;
 #pragma unroll
-			for (int a = 0; a < NX; a++)
+				for (int a = 0; a < NX; a++)
 #pragma unroll
-				for (int a2 = 0; a2 < NX; a2++)
-					A[((a * NY + b) * NZ + c) * NL + (a2 * NY + b2) * NZ + c2] = acc[a * NX + a2];
+					for (int a2 = 0; a2 < NX; a2++)
+						A[((a * NY + b) * NZ + c) * NL + (a2 * NY + b2) * NZ + c2] = acc[a * NX + a2];
+			}
 		}
 		__syncthreads();
 
