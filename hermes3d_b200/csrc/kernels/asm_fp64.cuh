@@ -18,10 +18,13 @@
 //   stage 2  T2_t[q1][b][b'][cc'] = sum_q2 Wy_t[b][b'][q2] T1_t[q1][q2][cc']
 //   stage 3  A[(a,b,c)][(a',b',c')] = sum_t sum_q1 Wx_t[a][a'][q1] T2_t[q1][bb'cc']
 // Work per element is O(nq p^6) instead of the O(nq^3 p^6) of the dense
-// per-pair loops.  Stage 1 runs for all terms at once into shared memory;
-// in stages 2+3 each thread owns one (b,b',c,c') column, forms its T2 values
-// in registers (no T2 buffer, same FMA count) and keeps the (a,a') rows of
-// A in registers, so the Wx table is read as broadcasts.
+// per-pair loops.  The 7 terms use only 3 distinct x tables (value/value,
+// derivative/value, derivative/derivative) and share y and z tables, so the
+// contraction is evaluated as a tree: stage 1 forms 6 products T1_k (zz and
+// mass share one), stage 2 accumulates them into 3 x-classes, stage 3
+// applies the 3 x tables.  Stage 1 runs into shared memory; in stages 2+3
+// each thread owns one (b,b',c,c') column, keeps its stage-2 values and the
+// (a,a') rows of A in registers, and reads the x tables as broadcasts.
 //
 // Scatter.  Entry (a, b) of the element's assembly list goes to
 // Ax[Ap[dof_b] + off[b][a]] (CSC: column = trial DOF).  Elements of one
@@ -43,7 +46,7 @@ struct SfShape {
 	static constexpr int NX = PX + 1, NY = PY + 1, NZ = PZ + 1;
 	static constexpr int NL = NX * NY * NZ;
 	static constexpr int NQ = NQX * NQY * NQZ;
-	static constexpr int NT_TERMS = 7;
+	static constexpr int NT_TERMS = 6;   // stage-1 products (zz and mass share one)
 	// 1D tables blob: Vx Dx Vy Dy Vz Dz (k-major, q fastest) then q/w per direction
 	static constexpr int OVX = 0, ODX = OVX + NX * NQX, OVY = ODX + NX * NQX, ODY = OVY + NY * NQY;
 	static constexpr int OVZ = ODY + NY * NQY, ODZ = OVZ + NZ * NQZ;
@@ -82,6 +85,12 @@ __device__ __constant__ int kTermFlags[7][3] = {
 	{ 3, 0, 0 }, { 0, 3, 0 }, { 0, 0, 3 },   // xx yy zz
 	{ 2, 1, 0 }, { 2, 0, 1 }, { 0, 2, 1 },   // xy xz yz
 	{ 0, 0, 0 }                               // mass
+};
+
+// stage-1 products k = xx, yy, zz(+mass), xy, xz, yz: (x, y, z) table flags
+// and the x-class each feeds (0: Wx^0, 1: Wx^2, 2: Wx^3)
+__device__ __constant__ int kT1Flags[6][3] = {
+	{ 3, 0, 0 }, { 0, 3, 0 }, { 0, 0, 3 }, { 2, 1, 0 }, { 2, 0, 1 }, { 0, 2, 1 }
 };
 
 template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ, int NT, int EB>
@@ -123,7 +132,6 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 	}
 	__syncthreads();
 
-	const int nterms = args.mass ? 7 : 6;
 	const bool do_rhs = args.rhs && args.lf;
 	const int64_t nbatch = (kend - kbeg + EB - 1) / EB;
 	for (int64_t bt = blockIdx.x; bt < nbatch; bt += gridDim.x) {
@@ -210,61 +218,87 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 			}
 		}
 
-		// ---- stage 1, all terms: item (e, t, q1, q2) produces T1_t[q1][q2][*][*]
-		for (int i = tid; i < EB * nterms * NQX * NQY; i += NT) {
-			const int e = i / (nterms * NQX * NQY), r = i % (nterms * NQX * NQY);
-			const int t = r / (NQX * NQY), q12 = r % (NQX * NQY);
+		// ---- stage 1: item (e, k, q1, q2) produces T1_k[q1][q2][*][*]
+		//   k: 0 xx, 1 yy, 2 zz (+ mass), 3 xy, 4 xz, 5 yz
+		for (int i = tid; i < EB * 6 * NQX * NQY; i += NT) {
+			const int e = i / (6 * NQX * NQY), r = i % (6 * NQX * NQY);
+			const int kk = r / (NQX * NQY), q12 = r % (NQX * NQY);
 			double *Eb = E0 + e * S::E_SIZE;
-			const double *gp = Eb + S::E_G + t * NQ + q12 * NQZ;
-			const double *wz = Wz + kTermFlags[t][2] * NZ * NZ * NQZ;
+			const double *gp = Eb + S::E_G + kk * NQ + q12 * NQZ;
+			const double *wz = Wz + kT1Flags[kk][2] * NZ * NZ * NQZ;
 			double g[NQZ];
 #pragma unroll
 			for (int q3 = 0; q3 < NQZ; q3++) g[q3] = gp[q3];
-			double *out = Eb + S::E_T1 + t * S::T1N + q12 * NZ * NZ;
+			double *out = Eb + S::E_T1 + kk * S::T1N + q12 * NZ * NZ;
+			if (kk == 2 && args.mass) {
+				const double *gm = Eb + S::E_G + 6 * NQ + q12 * NQZ;
+				const double *wz0 = Wz;
+				double h[NQZ];
 #pragma unroll
-			for (int cc = 0; cc < NZ * NZ; cc++) {
-				double s = 0.0;
+				for (int q3 = 0; q3 < NQZ; q3++) h[q3] = gm[q3];
 #pragma unroll
-				for (int q3 = 0; q3 < NQZ; q3++) s += g[q3] * wz[cc * NQZ + q3];
-				out[cc] = s;
+				for (int cc = 0; cc < NZ * NZ; cc++) {
+					double s = 0.0;
+#pragma unroll
+					for (int q3 = 0; q3 < NQZ; q3++) s += g[q3] * wz[cc * NQZ + q3] + h[q3] * wz0[cc * NQZ + q3];
+					out[cc] = s;
+				}
+			}
+			else {
+#pragma unroll
+				for (int cc = 0; cc < NZ * NZ; cc++) {
+					double s = 0.0;
+#pragma unroll
+					for (int q3 = 0; q3 < NQZ; q3++) s += g[q3] * wz[cc * NQZ + q3];
+					out[cc] = s;
+				}
 			}
 		}
 		__syncthreads();
-		// ---- stages 2+3: thread owns column (e, b, b', c, c'); per term it forms
-		// T2_t[q1][col] = sum_q2 Wy_t[b][b'][q2] T1_t[q1][q2][c][c'] in registers
-		// and accumulates A[(a,b,c)][(a',b',c')] for all (a, a') in registers.
+		// ---- stages 2+3: thread owns column (e, b, b', c, c'); it accumulates
+		// the stage-2 values of the 3 x-classes in registers,
+		//   V_f[q1] = sum_k(class f) sum_q2 Wy_k[b][b'][q2] T1_k[q1][q2][c][c'],
+		// then A[(a,b,c)][(a',b',c')] = sum_f sum_q1 Wx_f[a][a'][q1] V_f[q1].
 		{
 			static_assert(EB * COLS <= NT, "one stage-3 column per thread");
 			const int e = tid / COLS, col = tid % COLS;
 			const bool active = tid < EB * COLS;
 			double acc[NX * NX];
-#pragma unroll
-			for (int r = 0; r < NX * NX; r++) acc[r] = 0.0;
 			const int bb = col / (NZ * NZ), cc = col % (NZ * NZ);
 			if (active) {
 				const double *Eb = E0 + e * S::E_SIZE;
-				for (int t = 0; t < nterms; t++) {
-					const double *wy = Wy + kTermFlags[t][1] * NY * NY * NQY + bb * NQY;
-					const double *wx = Wx + kTermFlags[t][0] * NX * NX * NQX;
-					const double *t1 = Eb + S::E_T1 + t * S::T1N + cc;
+				double V[3][NQX];
+#pragma unroll
+				for (int f = 0; f < 3; f++)
+#pragma unroll
+					for (int q1 = 0; q1 < NQX; q1++) V[f][q1] = 0.0;
+#pragma unroll
+				for (int kk = 0; kk < 6; kk++) {
+					// compile-time after unrolling, so V stays in registers
+					constexpr int kFy[6] = { 0, 3, 0, 1, 0, 2 };
+					constexpr int kCls[6] = { 2, 0, 0, 1, 1, 0 };
+					const double *wy = Wy + kFy[kk] * NY * NY * NQY + bb * NQY;
+					const double *t1 = Eb + S::E_T1 + kk * S::T1N + cc;
+					const int f = kCls[kk];
 					double wyr[NQY];
 #pragma unroll
 					for (int q2 = 0; q2 < NQY; q2++) wyr[q2] = wy[q2];
-					double v[NQX];
 #pragma unroll
 					for (int q1 = 0; q1 < NQX; q1++) {
-						double s2 = 0.0;
+						double s2 = V[f][q1];
 #pragma unroll
 						for (int q2 = 0; q2 < NQY; q2++) s2 += wyr[q2] * t1[(q1 * NQY + q2) * NZ * NZ];
-						v[q1] = s2;
+						V[f][q1] = s2;
 					}
+				}
+				const double *wx0 = Wx, *wx2 = Wx + 2 * NX * NX * NQX, *wx3 = Wx + 3 * NX * NX * NQX;
 #pragma unroll
-					for (int r = 0; r < NX * NX; r++) {
-						double s3 = acc[r];
+				for (int r = 0; r < NX * NX; r++) {
+					double s3 = 0.0;
 #pragma unroll
-						for (int q1 = 0; q1 < NQX; q1++) s3 += wx[r * NQX + q1] * v[q1];
-						acc[r] = s3;
-					}
+					for (int q1 = 0; q1 < NQX; q1++)
+						s3 += wx0[r * NQX + q1] * V[0][q1] + wx2[r * NQX + q1] * V[1][q1] + wx3[r * NQX + q1] * V[2][q1];
+					acc[r] = s3;
 				}
 			}
 			__syncthreads();   // T1 fully consumed: A may overwrite it
