@@ -67,7 +67,8 @@ struct SfShape {
 	static constexpr int T1_END = E_T1 + NT_TERMS * T1N;
 	static constexpr int E_F = T1_END > NL * NL ? T1_END : NL * NL;   // NL
 	static constexpr int E_X = E_F + NL;        // 24
-	static constexpr int E_C = E_X + 24;        // NL coefficients
+	static constexpr int E_M = E_X + 24;        // 24 trilinear monomial coefficients
+	static constexpr int E_C = E_M + 24;        // NL coefficients
 	static constexpr int E_CS = E_C + NL;       // NL column starts (int64)
 	static constexpr int E_CE = E_CS + NL;      // NL column ends (int64)
 	static constexpr int E_I = E_CE + NL;       // ints: dof NL, s NL (NL doubles)
@@ -93,8 +94,8 @@ __device__ __constant__ int kT1Flags[6][3] = {
 	{ 3, 0, 0 }, { 0, 3, 0 }, { 0, 0, 3 }, { 2, 1, 0 }, { 2, 0, 1 }, { 0, 2, 1 }
 };
 
-template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ, int NT, int EB>
-__global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, int64_t kend) {
+template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ, int NT, int EB, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_assemble_fp64(KArgs args, int64_t kbeg, int64_t kend) {
 	using S = SfShape<PX, PY, PZ, NQX, NQY, NQZ, EB>;
 	constexpr int NX = S::NX, NY = S::NY, NZ = S::NZ, NL = S::NL, NQ = S::NQ;
 	constexpr int NL2 = NL * NL;
@@ -164,33 +165,70 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64(KArgs args, int64_t kbeg, 
 		}
 		__syncthreads();
 
-		// ---- geometry at the quadrature points -> term weights
+		// ---- trilinear map as monomials: x_r = sum_m c_m[r] mono_m(xi, eta, zeta),
+		// mono = 1, xi, eta, zeta, xi eta, xi zeta, eta zeta, xi eta zeta;
+		// c_m = (1/8) sum_v X_v prod_{d in m} s_d(v), s_d(v) = +-1 the vertex's
+		// reference coordinate (src/refdomain.cc:96-105)
+		for (int i = tid; i < EB * 24; i += NT) {
+			const int e = i / 24, mr = i % 24, mo = mr / 3, r = mr % 3;
+			double *Eb = E0 + e * S::E_SIZE;
+			const int usex = mo == 1 || mo == 4 || mo == 5 || mo == 7;
+			const int usey = mo == 2 || mo == 4 || mo == 6 || mo == 7;
+			const int usez = mo == 3 || mo == 5 || mo == 6 || mo == 7;
+			double c = 0.0;
+#pragma unroll
+			for (int v = 0; v < 8; v++) {
+				const int bx = ((v + 1) >> 1) & 1, by = (v >> 1) & 1, bz = v >> 2;
+				const int neg = (usex && !bx) ^ (usey && !by) ^ (usez && !bz);
+				const double xv = Eb[S::E_X + 3 * v + r];
+				c += neg ? -xv : xv;
+			}
+			Eb[S::E_M + mr] = 0.125 * c;
+		}
+		__syncthreads();
+
+		// ---- geometry at the quadrature points -> term weights.  Jacobian,
+		// signed determinant and inverse as in RefMap::calc_inv_ref_map
+		// (src/refmap.cc:177-231); G = w det J^-1 J^-T = (w / det) adj(J) adj(J)^T.
 		for (int i = tid; i < EB * NQ; i += NT) {
 			const int e = i / NQ, q = i % NQ;
 			double *Eb = E0 + e * S::E_SIZE;
 			double *G = Eb + S::E_G;
+			const double *cm = Eb + S::E_M;
 			const int q1 = q / (NQY * NQZ), q2 = (q / NQZ) % NQY, q3 = q % NQZ;
-			const double vx[2] = { tab[S::OVX + q1], tab[S::OVX + NQX + q1] };
-			const double dx[2] = { tab[S::ODX + q1], tab[S::ODX + NQX + q1] };
-			const double vy[2] = { tab[S::OVY + q2], tab[S::OVY + NQY + q2] };
-			const double dy[2] = { tab[S::ODY + q2], tab[S::ODY + NQY + q2] };
-			const double vz[2] = { tab[S::OVZ + q3], tab[S::OVZ + NQZ + q3] };
-			const double dz[2] = { tab[S::ODZ + q3], tab[S::ODZ + NQZ + q3] };
-			double m[3][3], det, irm[3][3], xp[3];
-			refmap_point(Eb + S::E_X, vx, dx, vy, dy, vz, dz, m, det, irm, xp);
-			const double wd = tab[S::OWX + q1] * tab[S::OWY + q2] * tab[S::OWZ + q3] * det;
-			double g[3][3];
+			const double x = tab[S::OQX + q1], y = tab[S::OQY + q2], z = tab[S::OQZ + q3];
+			const double xy = x * y, xz = x * z, yz = y * z, xyz = xy * z;
+			double m[3][3], xp[3];
 #pragma unroll
-			for (int c = 0; c < 3; c++)
-#pragma unroll
-				for (int d = c; d < 3; d++) g[c][d] = irm[0][c] * irm[0][d] + irm[1][c] * irm[1][d] + irm[2][c] * irm[2][d];
-			const double s = wd * s_cg[e];
-			G[0 * NQ + q] = 0.5 * s * g[0][0];
-			G[1 * NQ + q] = 0.5 * s * g[1][1];
-			G[2 * NQ + q] = 0.5 * s * g[2][2];
-			G[3 * NQ + q] = s * g[0][1];
-			G[4 * NQ + q] = s * g[0][2];
-			G[5 * NQ + q] = s * g[1][2];
+			for (int r = 0; r < 3; r++) {
+				const double c0 = cm[r], c1 = cm[3 + r], c2 = cm[6 + r], c3 = cm[9 + r];
+				const double c4 = cm[12 + r], c5 = cm[15 + r], c6 = cm[18 + r], c7 = cm[21 + r];
+				m[r][0] = c1 + c4 * y + c5 * z + c7 * yz;
+				m[r][1] = c2 + c4 * x + c6 * z + c7 * xz;
+				m[r][2] = c3 + c5 * x + c6 * y + c7 * xy;
+				xp[r] = c0 + c1 * x + c2 * y + c3 * z + c4 * xy + c5 * xz + c6 * yz + c7 * xyz;
+			}
+			// cofactors: adj(J)[c][k] = C[k][c]; J^-1 = adj(J) / det
+			const double C00 = m[1][1] * m[2][2] - m[1][2] * m[2][1];
+			const double C01 = m[1][2] * m[2][0] - m[1][0] * m[2][2];
+			const double C02 = m[1][0] * m[2][1] - m[1][1] * m[2][0];
+			const double C10 = m[0][2] * m[2][1] - m[0][1] * m[2][2];
+			const double C11 = m[0][0] * m[2][2] - m[0][2] * m[2][0];
+			const double C12 = m[0][1] * m[2][0] - m[0][0] * m[2][1];
+			const double C20 = m[0][1] * m[1][2] - m[0][2] * m[1][1];
+			const double C21 = m[0][2] * m[1][0] - m[0][0] * m[1][2];
+			const double C22 = m[0][0] * m[1][1] - m[0][1] * m[1][0];
+			const double det = m[0][0] * C00 + m[0][1] * C01 + m[0][2] * C02;
+			const double w = tab[S::OWX + q1] * tab[S::OWY + q2] * tab[S::OWZ + q3];
+			const double wd = w * det;
+			const double s = w * s_cg[e] / det;
+			// (J^-1)[c][k] = C[k][c] / det  =>  G[c][d] = sum_k C[k][c] C[k][d] / det^2
+			G[0 * NQ + q] = 0.5 * s * (C00 * C00 + C10 * C10 + C20 * C20);
+			G[1 * NQ + q] = 0.5 * s * (C01 * C01 + C11 * C11 + C21 * C21);
+			G[2 * NQ + q] = 0.5 * s * (C02 * C02 + C12 * C12 + C22 * C22);
+			G[3 * NQ + q] = s * (C00 * C01 + C10 * C11 + C20 * C21);
+			G[4 * NQ + q] = s * (C00 * C02 + C10 * C12 + C20 * C22);
+			G[5 * NQ + q] = s * (C01 * C02 + C11 * C12 + C21 * C22);
 			G[6 * NQ + q] = 0.5 * wd;
 			G[7 * NQ + q] = wd * source_value(args.lf, args.lf_value, xp);
 		}

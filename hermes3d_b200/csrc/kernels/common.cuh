@@ -152,10 +152,7 @@ __device__ __forceinline__ void posted_add(double *addr, double v) {
 
 __device__ __forceinline__ double source_value(int lf, double value, const double xp[3]) {
 	if (lf == 1) return value;
-	if (lf == 2) {
-		const double pi = 3.141592653589793238462643383279502884;
-		return sin(pi * xp[0]) * sin(pi * xp[1]) * sin(pi * xp[2]);
-	}
+	if (lf == 2) return sinpi(xp[0]) * sinpi(xp[1]) * sinpi(xp[2]);   // sin(pi x) sin(pi y) sin(pi z)
 	return 0.0;
 }
 
