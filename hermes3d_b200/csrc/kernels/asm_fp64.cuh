@@ -234,25 +234,35 @@ __global__ void __launch_bounds__(NT, MINB) k_assemble_fp64(KArgs args, int64_t 
 		}
 		__syncthreads();
 
-		// ---- element load vectors F_i = sum_q (w det f)(q) phi_i(q)
+		// ---- element load vectors F_i = sum_q (w det f)(q) phi_i(q), by sum
+		// factorisation: thread (e, a, b) contracts q3, then q2, then q1 for all c
 		if (do_rhs) {
-			for (int i = tid; i < EB * NL; i += NT) {
-				const int e = i / NL, j = i % NL;
+			for (int i = tid; i < EB * NX * NY; i += NT) {
+				const int e = i / (NX * NY), ab = i % (NX * NY), a = ab / NY, b = ab % NY;
 				double *Eb = E0 + e * S::E_SIZE;
 				const double *src = Eb + S::E_G + 7 * NQ;
-				const int a = j / (NY * NZ), b = (j / NZ) % NY, c = j % NZ;
-				double s = 0.0;
-				for (int q1 = 0; q1 < NQX; q1++) {
-					double s1 = 0.0;
-					for (int q2 = 0; q2 < NQY; q2++) {
-						double s2 = 0.0;
+				double fc[NZ];
 #pragma unroll
-						for (int q3 = 0; q3 < NQZ; q3++) s2 += src[(q1 * NQY + q2) * NQZ + q3] * tab[S::OVZ + c * NQZ + q3];
-						s1 += s2 * tab[S::OVY + b * NQY + q2];
+				for (int c = 0; c < NZ; c++) fc[c] = 0.0;
+				for (int q1 = 0; q1 < NQX; q1++) {
+					double s1[NZ];
+#pragma unroll
+					for (int c = 0; c < NZ; c++) s1[c] = 0.0;
+					for (int q2 = 0; q2 < NQY; q2++) {
+						const double vy = tab[S::OVY + b * NQY + q2];
+#pragma unroll
+						for (int q3 = 0; q3 < NQZ; q3++) {
+							const double w = src[(q1 * NQY + q2) * NQZ + q3] * vy;
+#pragma unroll
+							for (int c = 0; c < NZ; c++) s1[c] += w * tab[S::OVZ + c * NQZ + q3];
+						}
 					}
-					s += s1 * tab[S::OVX + a * NQX + q1];
+					const double vx = tab[S::OVX + a * NQX + q1];
+#pragma unroll
+					for (int c = 0; c < NZ; c++) fc[c] += vx * s1[c];
 				}
-				Eb[S::E_F + j] = s;
+#pragma unroll
+				for (int c = 0; c < NZ; c++) Eb[S::E_F + ab * NZ + c] = fc[c];
 			}
 		}
 
@@ -366,11 +376,11 @@ __global__ void __launch_bounds__(NT, MINB) k_assemble_fp64(KArgs args, int64_t 
 					if (p < EB * NL2) {
 						const int e = p / NL2, pp = p % NL2;
 						const int m = s_m[e];
-						if (pp < m * m) {
+						const int b = pp / NL, a = pp % NL;
+						if (a < m && b < m) {
 							const double *Eb = E0 + e * S::E_SIZE;
 							const int *ei = reinterpret_cast<const int *>(Eb + S::E_I);
 							const int64_t *cs = reinterpret_cast<const int64_t *>(Eb + S::E_CS);
-							const int b = pp / m, a = pp % m;
 							const int sa = ei[NL + a], sb = ei[NL + b];
 							const double *A = Eb + S::E_A;
 							val[r] = Eb[S::E_C + a] * Eb[S::E_C + b] * (A[sa * NL + sb] + A[sb * NL + sa]);
