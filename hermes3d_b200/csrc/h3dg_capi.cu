@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -494,6 +496,11 @@ h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, dou
 	};
 	// autotune once per plan: time one colour sweep of every variant (results are
 	// bitwise identical across variants; the outputs are re-zeroed afterwards)
+	// H3DG_FP64_VARIANT=i pins candidate i (profiling runs) and skips the timing pass
+	if (disc->variant < 0 && !cands.empty() && std::getenv("H3DG_FP64_VARIANT")) {
+		int v = std::atoi(std::getenv("H3DG_FP64_VARIANT"));
+		disc->variant = cands[(size_t) std::max(0, std::min(v, (int) cands.size() - 1))];
+	}
 	if (disc->variant < 0 && cands.size() > 1) {
 		cudaEvent_t e0, e1;
 		H3DG_CUDA_TRY(cudaEventCreate(&e0));
