@@ -4,6 +4,7 @@
 #include "host/lobatto.h"
 #include "kernels/asm_fp64.cuh"
 #include "kernels/asm_fp64_seq.cuh"
+#include "kernels/asm_fp64_ho.cuh"
 #include "kernels/geom.cuh"
 
 #include <cuda_runtime.h>
@@ -84,7 +85,9 @@ struct h3dg_disc {
 	DBuf<double> xyz, coef, tables, qx, qy, qz, Ax, rhs;
 	DBuf<int64_t> Ap;
 	DBuf<int32_t> Ai, el_vtx, el_cnt, el_dof, el_id;
-	DBuf<uint16_t> el_s, el_off;
+	DBuf<uint16_t> el_s, el_off, el_offc;
+	DBuf<int32_t> el_cdof;
+	DBuf<double> el_ccoef;
 	DBuf<double> el_coef;
 	DBuf<int> status;
 	int table_bytes = 0;
@@ -335,7 +338,15 @@ h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nn
 	int nq[3];
 	for (int d = 0; d < 3; d++) nq[d] = disc->qmode == H3DG_QUAD_FIXED ? disc->qn : sp.order[d] + disc->qn;
 	std::string err;
-	if (h3dg::build_plan(sp, nq[0], nq[1], nq[2], disc->plan, err) != 0) return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
+	// orders >= 5: the element matrix does not fit in shared memory; the
+	// high-order kernel works on canonical tables
+	int pmax = 0;
+	for (size_t i = 0; i < sp.order.size(); i++) pmax = std::max(pmax, sp.order[i]);
+	// H3DG_FORCE_HIGH_ORDER=1 routes every order through the high-order kernel
+	// (used by the parity tests to check that kernel on the low-order fixtures)
+	const char *force = std::getenv("H3DG_FORCE_HIGH_ORDER");
+	const bool canon = pmax >= 5 || (force && force[0] == '1');
+	if (h3dg::build_plan(sp, nq[0], nq[1], nq[2], disc->plan, err, canon) != 0) return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
 	const h3dg::Plan &P = disc->plan;
 	disc->on_device = false;
 	disc->have_plan = true;
@@ -357,11 +368,18 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 	H3DG_CUDA_TRY(disc->Ai.upload(P.Ai));
 	H3DG_CUDA_TRY(disc->el_vtx.upload(P.el_vtx));
 	H3DG_CUDA_TRY(disc->el_cnt.upload(P.el_cnt));
-	H3DG_CUDA_TRY(disc->el_s.upload(P.el_s));
-	H3DG_CUDA_TRY(disc->el_dof.upload(P.el_dof));
-	H3DG_CUDA_TRY(disc->el_coef.upload(P.el_coef));
-	H3DG_CUDA_TRY(disc->el_off.upload(P.el_off));
 	H3DG_CUDA_TRY(disc->el_id.upload(P.el_id));
+	if (P.canon) {
+		H3DG_CUDA_TRY(disc->el_cdof.upload(P.el_cdof));
+		H3DG_CUDA_TRY(disc->el_ccoef.upload(P.el_ccoef));
+		H3DG_CUDA_TRY(disc->el_offc.upload(P.el_offc));
+	}
+	else {
+		H3DG_CUDA_TRY(disc->el_s.upload(P.el_s));
+		H3DG_CUDA_TRY(disc->el_dof.upload(P.el_dof));
+		H3DG_CUDA_TRY(disc->el_coef.upload(P.el_coef));
+		H3DG_CUDA_TRY(disc->el_off.upload(P.el_off));
+	}
 	std::vector<double> blob;
 	build_table_blob(P, blob);
 	disc->table_bytes = (int) (blob.size() * sizeof(double));
@@ -426,9 +444,89 @@ std::vector<KernelSpec> &kernel_table() {
 	return t;
 }
 
+using HoFn = void (*)(h3dg::KArgsHO, int64_t, int64_t);
+
+struct HoSpec {
+	int p, nq;
+	HoFn fn;
+	int threads;
+	size_t smem;
+	bool configured;
+};
+
+template <int P, int NQ, int NT>
+HoSpec ho_spec() {
+	return HoSpec { P, NQ, &h3dg::k_assemble_fp64_ho<P, P, P, NQ, NQ, NQ, NT>, NT,
+	                h3dg::HoShape<P, P, P, NQ, NQ, NQ>::SMEM_BYTES, false };
+}
+
+std::vector<HoSpec> &ho_table() {
+	static std::vector<HoSpec> t = {
+		ho_spec<2, 4, 128>(), ho_spec<3, 5, 256>(),
+		ho_spec<5, 6, 256>(), ho_spec<5, 7, 256>(), ho_spec<6, 7, 256>(), ho_spec<6, 8, 256>(),
+		ho_spec<7, 8, 256>(), ho_spec<7, 9, 256>(), ho_spec<8, 9, 256>(), ho_spec<8, 10, 256>(),
+		ho_spec<8, 10, 384>(),
+	};
+	return t;
+}
+
 } // namespace
 
 extern "C" {
+
+static h3dg_status assemble_ho(h3dg_disc *disc, double *d_Ax, double *d_rhs, cudaStream_t st) {
+	const h3dg::Plan &P = disc->plan;
+	std::vector<int> cands;
+	for (size_t i = 0; i < ho_table().size(); i++)
+		if (ho_table()[i].p == P.px && ho_table()[i].nq == P.nqx) cands.push_back((int) i);
+	if (cands.empty()) return fail(H3DG_ERR_INVALID_ARG, "assemble: no high-order kernel instantiated for this order / rule");
+	h3dg::KArgsHO a;
+	a.xyz = disc->xyz.p;
+	a.el_vtx = disc->el_vtx.p;
+	a.el_id = disc->el_id.p;
+	a.ecoef = disc->coef.p;
+	a.cdof = disc->el_cdof.p;
+	a.ccoef = disc->el_ccoef.p;
+	a.offc = disc->el_offc.p;
+	a.Ap = disc->Ap.p;
+	a.tables = disc->tables.p;
+	a.table_bytes = disc->table_bytes;
+	a.mass = disc->bf == H3DG_BF_GRAD_GRAD_MASS;
+	a.lf = disc->lf;
+	a.lf_value = disc->lf_value;
+	a.Ax = d_Ax;
+	a.rhs = disc->lf ? d_rhs : nullptr;
+	a.status = disc->status.p;
+	if (d_Ax) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
+	if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
+	int nsm = 148;
+	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
+	HoSpec &k = ho_table()[cands.back()];
+	if (!k.configured) {
+		H3DG_CUDA_TRY(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) k.smem));
+		k.configured = true;
+	}
+	int per_sm = 1;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, k.smem);
+	if (per_sm < 1) per_sm = 1;
+	const bool rec = disc->tn < disc->tcap;
+	if (rec) H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn], st));
+	int32_t launches = 0;
+	for (int c = 0; c < P.ncolors; c++) {
+		int64_t kb = P.color_ptr[c], ke = P.color_ptr[c + 1];
+		if (ke <= kb) continue;
+		int64_t grid = std::min<int64_t>(ke - kb, (int64_t) nsm * per_sm);
+		k.fn<<<(unsigned) grid, k.threads, k.smem, st>>>(a, kb, ke);
+		launches++;
+	}
+	H3DG_CUDA_TRY(cudaGetLastError());
+	if (rec) {
+		H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn + 1], st));
+		disc->tn++;
+	}
+	disc->last_launches = launches;
+	return H3DG_OK;
+}
 
 h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream) {
 	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "assemble: create_pattern() first");
@@ -436,6 +534,12 @@ h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, dou
 	const h3dg::Plan &P = disc->plan;
 	if (P.px != P.py || P.px != P.pz || P.nqx != P.nqy || P.nqx != P.nqz)
 		return fail(H3DG_ERR_INVALID_ARG, "assemble: anisotropic orders need the batched path");
+	if (P.canon) {
+		h3dg_status s0 = ensure_device(disc);
+		if (s0 != H3DG_OK) return s0;
+		H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+		return assemble_ho(disc, d_Ax, d_rhs, (cudaStream_t) stream);
+	}
 	std::vector<int> cands;
 	for (size_t i = 0; i < kernel_table().size(); i++)
 		if (kernel_table()[i].p == P.px && kernel_table()[i].nq == P.nqx) cands.push_back((int) i);
@@ -445,7 +549,7 @@ h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, dou
 		h3dg_status s0 = ensure_device(disc);
 		if (s0 != H3DG_OK) return s0;
 	}
-	if (!disc->xyz.p || !disc->el_vtx.p || !disc->el_off.p || !disc->Ap.p || !disc->tables.p || !disc->status.p)
+	if (!disc->xyz.p || !disc->el_vtx.p || !disc->el_off.p || !disc->Ap.p || !disc->tables.p || !disc->status.p || !disc->el_s.p)
 		return fail(H3DG_ERR_STATE, "assemble: device plan missing");
 	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
 	cudaStream_t st = (cudaStream_t) stream;

@@ -542,7 +542,7 @@ static void parallel_for(int64_t n, F f) {
 // holds both.  Built here column by column from the DOF -> element adjacency
 // instead of page lists.  Also produces the per-element tables, the
 // row-position map used by the scatter and an element colouring.
-int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string &err) {
+int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string &err, bool canon) {
 	if (!sp.assigned) { err = "assign_dofs() has not been called"; return -1; }
 	const Mesh &m = *sp.mesh;
 	int64_t ne = m.ne();
@@ -675,6 +675,50 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 		P.color_ptr = cc;
 		std::vector<int64_t> fill(cc.begin(), cc.end() - 1);
 		for (int64_t e = 0; e < ne; e++) order_[fill[color[e]]++] = e;
+	}
+
+	P.canon = canon;
+	if (canon) {
+		// canonical tables: every canonical index must occur at most once per element
+		for (int64_t e = 0; e < ne; e++) {
+			std::vector<char> seen(nl, 0);
+			for (int k = 0; k < cnt[2 * e] + cnt[2 * e + 1]; k++) {
+				int sidx = ss[(size_t) e * nl + k];
+				if (seen[sidx]) { err = "a canonical function repeats in one assembly list"; return -1; }
+				seen[sidx] = 1;
+			}
+		}
+		P.el_vtx.resize(8 * ne);
+		P.el_id.resize(ne);
+		P.el_cdof.assign((size_t) ne * nl, -1);
+		P.el_ccoef.assign((size_t) ne * nl, 0.0);
+		P.el_offc.assign((size_t) ne * nl * nl, 0);
+		P.el_cnt.resize(2 * ne);
+		parallel_for(ne, [&](int64_t lo, int64_t hi) {
+			for (int64_t k = lo; k < hi; k++) {
+				int64_t e = order_[k];
+				P.el_id[k] = (int32_t) e;
+				for (int v = 0; v < 8; v++) P.el_vtx[8 * k + v] = (int32_t) m.hex[8 * e + v];
+				P.el_cnt[2 * k] = cnt[2 * e];
+				P.el_cnt[2 * k + 1] = cnt[2 * e + 1];
+				for (int t = 0; t < cnt[2 * e] + cnt[2 * e + 1]; t++) {
+					int sidx = ss[(size_t) e * nl + t];
+					P.el_cdof[(size_t) k * nl + sidx] = dofs[(size_t) e * nl + t];
+					P.el_ccoef[(size_t) k * nl + sidx] = cf[(size_t) e * nl + t];
+				}
+				int mc = cnt[2 * e];
+				for (int b = 0; b < mc; b++) {
+					int col = dofs[(size_t) e * nl + b], sj = ss[(size_t) e * nl + b];
+					const int32_t *c0 = &P.Ai[P.Ap[col]], *c1 = &P.Ai[P.Ap[col + 1]];
+					for (int a = 0; a < mc; a++) {
+						int row = dofs[(size_t) e * nl + a], si = ss[(size_t) e * nl + a];
+						const int32_t *pos = std::lower_bound(c0, c1, row);
+						P.el_offc[((size_t) k * nl + si) * nl + sj] = (uint16_t) (pos - c0);
+					}
+				}
+			}
+		});
+		return 0;
 	}
 
 	// tables in assembly (colour-major) order

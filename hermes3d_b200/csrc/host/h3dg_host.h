@@ -128,6 +128,13 @@ struct Plan {
 	std::vector<uint16_t> el_off;            // ne x nl x nl: row position of dof_a in column dof_b
 	std::vector<int32_t> el_id;              // reference element id - 1 of each assembly slot
 
+	// canonical form (high orders): indexed by the canonical function, not the
+	// AsmList entry; requires each canonical function to occur at most once
+	bool canon = false;
+	std::vector<int32_t> el_cdof;            // ne x nl: DOF or -1
+	std::vector<double> el_ccoef;            // ne x nl: sign x coefficient (lifting value when DOF = -1), 0 absent
+	std::vector<uint16_t> el_offc;           // ne x nl x nl: [i][j] row position of cdof_i in column cdof_j
+
 	// element colouring: no two elements of a colour share a DOF
 	int ncolors = 0;
 	std::vector<int64_t> color_ptr;          // ncolors + 1 (ranges in assembly order)
@@ -136,6 +143,6 @@ struct Plan {
 	std::vector<double> qx, wx, qy, wy, qz, wz;
 };
 
-int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &plan, std::string &err);
+int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &plan, std::string &err, bool canon = false);
 
 } // namespace h3dg

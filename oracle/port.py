@@ -34,6 +34,7 @@ def lib():
         L.h3d_port_assemble.argtypes = [C.c_int64, pd, C.c_int64, pi64, pi32, pi64, pi64, pi32, pd, C.c_int, pd, C.c_int,
                                         C.c_double, C.c_int64, pi64, pi32, pd, pd]
         L.h3d_port_element_matrix.argtypes = [pd, C.c_int, C.c_int, C.c_int, C.c_int, pi64, C.c_int, C.c_double, pd]
+        L.h3d_port_element_rows.argtypes = [pd, C.c_int, C.c_int, C.c_int, C.c_int, pi64, C.c_int, pi32, C.c_int, C.c_double, pd]
         _lib = L
     return _lib
 
@@ -113,3 +114,15 @@ def element_matrix(X, nq, idx, mass=False, gradcoef=1.0):
     lib().h3d_port_element_matrix(_p(X, C.c_double), nqx, nqy, nqz, n, _p(idx, C.c_int64), int(mass), float(gradcoef),
                                   _p(K, C.c_double))
     return K
+
+
+def element_rows(X, nq, idx, rows, mass=False, gradcoef=1.0):
+    """Rows (test indices into idx) of the element matrix, all columns."""
+    X = np.ascontiguousarray(X, np.float64).reshape(8, 3)
+    idx = np.ascontiguousarray(idx, np.int64)
+    rows = np.ascontiguousarray(rows, np.int32)
+    out = np.zeros((len(rows), len(idx)), np.float64)
+    nqx, nqy, nqz = (nq, nq, nq) if np.isscalar(nq) else nq
+    lib().h3d_port_element_rows(_p(X, C.c_double), nqx, nqy, nqz, len(idx), _p(idx, C.c_int64), len(rows),
+                                _p(rows, C.c_int32), int(mass), float(gradcoef), _p(out, C.c_double))
+    return out

@@ -351,3 +351,13 @@ int h3d_port_element_matrix(const double *X, int nqx, int nqy, int nqz, int cnt,
 	elem_free(&c);
 	return 0;
 }
+
+int h3d_port_element_rows(const double *X, int nqx, int nqy, int nqz, int cnt, const int64_t *idx, int nrows,
+                          const int32_t *rows, int mass, double gradcoef, double *out) {
+	ElemCache c;
+	if (elem_cache(X, nqx, nqy, nqz, cnt, idx, &c) != 0) return -1;
+	for (int r = 0; r < nrows; r++)
+		for (int j = 0; j < cnt; j++) out[(size_t) r * cnt + j] = biform(&c, j, rows[r], mass, gradcoef);
+	elem_free(&c);
+	return 0;
+}

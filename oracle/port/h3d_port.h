@@ -38,6 +38,11 @@ int h3d_port_assemble(int64_t nv, const double *xyz, int64_t ne, const int64_t *
 int h3d_port_element_matrix(const double *X /* 8 x 3 */, int nqx, int nqy, int nqz, int cnt, const int64_t *idx,
                             int mass, double gradcoef, double *K);
 
+/* Selected rows of the element matrix: K[r][j] for r in rows (test indices
+ * into idx), all j; out is nrows x cnt. */
+int h3d_port_element_rows(const double *X, int nqx, int nqy, int nqz, int cnt, const int64_t *idx, int nrows,
+                          const int32_t *rows, int mass, double gradcoef, double *out);
+
 #ifdef __cplusplus
 }
 #endif
