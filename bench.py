@@ -33,6 +33,20 @@ N_POINTS = 4
 METRIC = "hp assembly elements/s (FP64, C2: 64^3 jittered, p=2, 4^3 pts, grad+mass, sin source, full CSC+RHS)"
 CPU_SAMPLE_SIDE = 16
 
+# the other configurations (parity cases; reported with --workload, never the headline)
+WORKLOADS = {
+    "c2": dict(side=64, jitter=0.2, p=2, nq=4, mass=True, lf="sin", coef=None,
+               desc="C2: 64^3=262144 jittered (+-0.2h) hexahedra, p=2, 4^3 Gauss points, grad.grad+mass, "
+                    "f=sin(pi x)sin(pi y)sin(pi z), full CSC+RHS"),
+    "c1": dict(side=8, jitter=0.0, p=3, nq=5, mass=False, lf=1.0, coef=None,
+               desc="C1: 8^3 unit cube, p=3, 5^3 Gauss points, homogeneous Dirichlet, grad.grad, f=1"),
+    "c4": dict(side=16, jitter=0.2, p=8, nq=10, mass=False, lf=None, coef=(0.5, 2.0),
+               desc="C4: 16^3 jittered hexahedra, p=8, 10^3 Gauss points, a_e grad.grad, a_e ~ U[0.5,2]"),
+    "c5": dict(side=32, jitter=0.2, p=3, nq=5, mass=False, lf=1.0, coef="lognormal",
+               desc="C5 forward: 32^3 jittered hexahedra, p=3, 5^3 points, a_e grad.grad with a_e = exp(g_e), "
+                    "g_e ~ N(0, 0.5^2), f=1"),
+}
+
 
 def peaks():
     try:
@@ -91,17 +105,25 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def build_problem(h, seed, device, side=N_ELEM_SIDE):
-    mesh = h.unit_cube(side, 0.2, seed)
+def build_problem(h, seed, device, side=N_ELEM_SIDE, workload="c2"):
+    import numpy as np
+    w = WORKLOADS[workload]
+    side = side if workload == "c2" else w["side"]
+    mesh = h.unit_cube(side, w["jitter"], seed)
     mesh.ugh()
     sp = h.H1Space(mesh)
-    sp.set_uniform_order(P_ORDER)
+    sp.set_uniform_order(w["p"])
     sp.assign_dofs()
     d = h.Discretization(device)
     d.set_spaces(sp)
-    d.set_bilinear_form(h.int_grad_u_grad_v_plus_u_v)
-    d.set_linear_form(h.int_F_v("sin"))
-    d.set_quadrature(points=N_POINTS)
+    coef = None
+    if w["coef"] == "lognormal":
+        coef = np.exp(np.random.default_rng(seed).normal(0.0, 0.5, mesh.num_elements))
+    elif w["coef"] is not None:
+        coef = np.random.default_rng(seed).uniform(w["coef"][0], w["coef"][1], mesh.num_elements)
+    d.set_bilinear_form(h.int_grad_u_grad_v_plus_u_v if w["mass"] else h.int_grad_u_grad_v, coef)
+    d.set_linear_form(None if w["lf"] is None else h.int_F_v(w["lf"]))
+    d.set_quadrature(points=w["nq"])
     d.create()
     return mesh, sp, d
 
@@ -111,10 +133,11 @@ def algorithmic_bytes(nnz, ndof, nv, ne):
     return 8 * nnz + 8 * ndof + 24 * nv + 32 * ne
 
 
-def dense_flops_per_element():
-    nl = (P_ORDER + 1) ** 3
-    nq = N_POINTS ** 3
-    return 2 * nl * nl * 3 * nq + 2 * nl * nl * nq + 2 * nl * nq
+def dense_flops_per_element(workload="c2"):
+    w = WORKLOADS[workload]
+    nl = (w["p"] + 1) ** 3
+    nq = w["nq"] ** 3
+    return 2 * nl * nl * 3 * nq + (2 * nl * nl * nq if w["mass"] else 0) + (2 * nl * nq if w["lf"] is not None else 0)
 
 
 def cpu_baseline(repeat=3):
@@ -188,6 +211,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--side", type=int, default=N_ELEM_SIDE, help="elements per cube side (profiling runs only)")
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -211,7 +235,7 @@ def main():
             dist.barrier()
 
     t_setup = time.time()
-    mesh, sp, d = build_problem(h, seed=rank, device=local, side=args.side)
+    mesh, sp, d = build_problem(h, seed=rank, device=local, side=args.side, workload=args.workload)
     t_setup = time.time() - t_setup
     ne, ndof, nnz, nv = mesh.num_elements, d.ndof, d.nnz, mesh.num_vertices
     stream = torch.cuda.current_stream()
@@ -281,13 +305,16 @@ def main():
             except Exception:
                 traffic = None
         out = {
-            "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
+            "metric": METRIC if args.workload == "c2" else METRIC.replace("C2: 64^3 jittered, p=2, 4^3 pts, grad+mass, sin source",
+                                                                             WORKLOADS[args.workload]["desc"]),
+            "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded jittered unit-cube mesh)",
-            "config": {"workload": "C2: 64^3=262144 jittered (+-0.2h) hexahedra, p=2, 4^3 Gauss points, "
-                                   "grad.grad+mass, f=sin(pi x)sin(pi y)sin(pi z), full CSC+RHS",
-                       "ndof": ndof, "nnz": nnz, "elements_per_gpu": ne, "l2": "inputs larger than L2 (Ax alone 1.0 GB)",
-                       "parallelism": "replicas: one 64^3 subdomain per GPU" if world > 1 else "single GPU",
+            "config": {"workload": WORKLOADS[args.workload]["desc"] if args.side == N_ELEM_SIDE or args.workload != "c2"
+                       else "C2 forms on %d^3 elements (profiling size)" % args.side,
+                       "ndof": ndof, "nnz": nnz, "elements_per_gpu": ne,
+                       "l2": "inputs larger than L2 (Ax alone %.2f GB)" % (8e-9 * nnz),
+                       "parallelism": "replicas: one subdomain per GPU" if world > 1 else "single GPU",
                        "setup_s": round(t_setup, 2)},
             "nnz_per_s": world * nnz / (ms_per_step * 1e-3),
             "kernel_ms_per_step": kernel_ms,
@@ -296,13 +323,13 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind,
                          "algorithmic_bytes_per_step": B,
-                         "fp64_dense_equiv_tflops": ne * dense_flops_per_element() / (kms * 1e-3) / 1e12},
+                         "fp64_dense_equiv_tflops": ne * dense_flops_per_element(args.workload) / (kms * 1e-3) / 1e12},
             "e2e": {"value": e2e_value, "unit": "elements/s", "h2d_bytes_per_step": 24 * nv,
                     "d2h_bytes_per_step": 8 * nnz + 8 * ndof, "ms_per_step": 1e3 * float(te.item())},
             "clocks": clk.summary(),
             "finite": ok,
         }
-        if not args.no_cpu_baseline and world == 1:
+        if not args.no_cpu_baseline and world == 1 and args.workload == "c2":
             try:
                 out["cpu_baseline"] = cpu_baseline()
             except Exception as ex:  # report, do not fail the GPU number
