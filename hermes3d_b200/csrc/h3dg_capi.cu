@@ -5,6 +5,7 @@
 #include "kernels/asm_fp64.cuh"
 #include "kernels/asm_fp64_seq.cuh"
 #include "kernels/asm_fp64_ho.cuh"
+#include "kernels/adjoint.cuh"
 #include "kernels/geom.cuh"
 
 #include <cuda_runtime.h>
@@ -470,6 +471,29 @@ std::vector<HoSpec> &ho_table() {
 	return t;
 }
 
+using AdjFn = void (*)(h3dg::AdjArgs);
+
+struct AdjSpec {
+	int p, nq;
+	AdjFn fn;
+	size_t smem;
+	bool configured;
+};
+
+template <int P, int NQ>
+AdjSpec adj_spec() {
+	return AdjSpec { P, NQ, &h3dg::k_adjoint<P, P, P, NQ, NQ, NQ, 128>, h3dg::AdjShape<P, P, P, NQ, NQ, NQ>::SMEM_BYTES, false };
+}
+
+std::vector<AdjSpec> &adj_table() {
+	static std::vector<AdjSpec> t = {
+		adj_spec<1, 2>(), adj_spec<1, 3>(), adj_spec<2, 3>(), adj_spec<2, 4>(), adj_spec<3, 4>(), adj_spec<3, 5>(),
+		adj_spec<4, 5>(), adj_spec<4, 6>(), adj_spec<5, 6>(), adj_spec<5, 7>(), adj_spec<6, 7>(), adj_spec<6, 8>(),
+		adj_spec<8, 10>(),
+	};
+	return t;
+}
+
 } // namespace
 
 extern "C" {
@@ -645,6 +669,59 @@ h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, dou
 		disc->tn++;
 	}
 	disc->last_launches = launches;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_adjoint(h3dg_disc *disc, int nfields, const double *d_logcoef, const double *d_u,
+                              const double *d_lambda, double *d_S, double *d_grad, void *stream) {
+	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "adjoint: create_pattern() first");
+	if (nfields < 1 || !d_u || !d_lambda) return fail(H3DG_ERR_INVALID_ARG, "adjoint: bad arguments");
+	const h3dg::Plan &P = disc->plan;
+	if (P.px != P.py || P.px != P.pz || P.nqx != P.nqy || P.nqx != P.nqz)
+		return fail(H3DG_ERR_INVALID_ARG, "adjoint: anisotropic orders need the batched path");
+	AdjSpec *k = nullptr;
+	for (auto &a : adj_table())
+		if (a.p == P.px && a.nq == P.nqx) k = &a;
+	if (!k) return fail(H3DG_ERR_INVALID_ARG, "adjoint: no kernel instantiated for this order / rule");
+	{
+		h3dg_status s0 = ensure_device(disc);
+		if (s0 != H3DG_OK) return s0;
+	}
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	h3dg::AdjArgs a;
+	a.xyz = disc->xyz.p;
+	a.el_vtx = disc->el_vtx.p;
+	a.el_id = disc->el_id.p;
+	a.el_cnt = disc->el_cnt.p;
+	a.el_s = P.canon ? nullptr : disc->el_s.p;
+	a.el_dof = P.canon ? nullptr : disc->el_dof.p;
+	a.el_coef = P.canon ? nullptr : disc->el_coef.p;
+	a.cdof = P.canon ? disc->el_cdof.p : nullptr;
+	a.ccoef = P.canon ? disc->el_ccoef.p : nullptr;
+	a.tables = disc->tables.p;
+	a.table_bytes = disc->table_bytes;
+	a.nfields = nfields;
+	a.lift = disc->lf != H3DG_LF_NONE;
+	a.ne = P.ne;
+	a.ndof = P.ndof;
+	a.logcoef = d_logcoef;
+	a.u = d_u;
+	a.lam = d_lambda;
+	a.S = d_S;
+	a.grad = d_grad;
+	a.status = disc->status.p;
+	if (!k->configured) {
+		H3DG_CUDA_TRY(cudaFuncSetAttribute(k->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) k->smem));
+		k->configured = true;
+	}
+	int nsm = 148, per_sm = 1;
+	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k->fn, 128, k->smem);
+	if (per_sm < 1) per_sm = 1;
+	int64_t grid = std::min<int64_t>(P.ne, (int64_t) nsm * per_sm);
+	k->fn<<<(unsigned) grid, 128, k->smem, (cudaStream_t) stream>>>(a);
+	H3DG_CUDA_TRY(cudaGetLastError());
+	disc->last_launches = 1;
 	return H3DG_OK;
 }
 

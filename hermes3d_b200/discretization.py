@@ -234,6 +234,31 @@ class Discretization:
                   *[C.c_void_p(x.data_ptr()) if x is not None else None for x in (jac, irm, xyz)],
                   C.c_void_p(stream.cuda_stream))
 
+    def adjoint(self, logcoef, u, lam, S=None, grad=None, stream=None):
+        """Element sensitivities of L_k = lam_k^T K(exp(g_k)) u_k - lam_k^T f(exp(g_k)).
+
+        logcoef (nf x ne, element-id order, or None), u and lam (nf x ndof) are
+        torch CUDA float64 tensors; returns (S, grad), both nf x ne, with
+        grad = exp(logcoef) * S = dL/dg."""
+        import torch
+        u = u.reshape(-1, self.ndof)
+        lam = lam.reshape(-1, self.ndof)
+        nf = u.shape[0]
+        ne = self.space.mesh.num_elements
+        dev = u.device
+        if S is None:
+            S = torch.empty(nf, ne, dtype=torch.float64, device=dev)
+        if grad is None:
+            grad = torch.empty(nf, ne, dtype=torch.float64, device=dev)
+        if stream is None:
+            stream = torch.cuda.current_stream(dev)
+        lg = None if logcoef is None else logcoef.reshape(nf, ne).contiguous()
+        u, lam = u.contiguous(), lam.contiguous()
+        capi.call("h3dg_disc_adjoint", self.handle, nf, None if lg is None else C.c_void_p(lg.data_ptr()),
+                  C.c_void_p(u.data_ptr()), C.c_void_p(lam.data_ptr()), C.c_void_p(S.data_ptr()),
+                  C.c_void_p(grad.data_ptr()), C.c_void_p(stream.cuda_stream))
+        return S, grad
+
     def update_vertices(self, xyz):
         a = np.ascontiguousarray(xyz, dtype=np.float64)
         capi.call("h3dg_disc_update_vertices", self.handle, capi.ptr(a, C.c_double), len(a.reshape(-1, 3)))

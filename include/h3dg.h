@@ -150,6 +150,19 @@ h3dg_status h3dg_disc_get_tuning(const h3dg_disc *disc, int32_t *threads, int32_
 h3dg_status h3dg_disc_enable_kernel_timing(h3dg_disc *disc, int32_t n);
 h3dg_status h3dg_disc_kernel_times(h3dg_disc *disc, float *ms, int32_t cap, int32_t *n);
 
+/* Adjoint of the coefficient-weighted assembly (no reference counterpart: the
+ * reference has no adjoint).  For nfields fields k with per-element
+ * log-coefficients g_k (a = exp(g) multiplies the grad-grad term, as the
+ * coefficient of h3dg_disc_set_bilinear_form does) and vectors u_k, lambda_k:
+ *   L_k = lambda_k^T K(a_k) u_k - lambda_k^T f(a_k),
+ *   d_S[k][e]    = lambda_e^T K_e^(1) (u_e + d_e)   (unit coefficient; d_e Dirichlet lifting
+ *                  when a linear form is set)
+ *   d_grad[k][e] = dL_k / dg_{k,e} = exp(g_{k,e}) d_S[k][e].
+ * Device arrays: d_logcoef nfields x ne (element-id order, or NULL for a = 1),
+ * d_u and d_lambda nfields x ndof, d_S and d_grad nfields x ne (either may be NULL). */
+h3dg_status h3dg_disc_adjoint(h3dg_disc *disc, int nfields, const double *d_logcoef, const double *d_u,
+	const double *d_lambda, double *d_S, double *d_grad, void *stream);
+
 /* RefMap (src/refmap.cc:177-231, 265-316): per element (id order) and per point of the
  * disc's volume rule, the signed Jacobian determinant (get_jacobian without the
  * weight), the transposed inverse Jacobian irm[r][c] = (J^-1)[c][r] (get_inv_ref_map)
