@@ -6,6 +6,8 @@
 #include "kernels/asm_fp64_seq.cuh"
 #include "kernels/asm_fp64_ho.cuh"
 #include "kernels/adjoint.cuh"
+#include "kernels/tc_selftest.cuh"
+#include <cuda_bf16.h>
 #include "kernels/geom.cuh"
 
 #include <cuda_runtime.h>
@@ -722,6 +724,23 @@ h3dg_status h3dg_disc_adjoint(h3dg_disc *disc, int nfields, const double *d_logc
 	k->fn<<<(unsigned) grid, 128, k->smem, (cudaStream_t) stream>>>(a);
 	H3DG_CUDA_TRY(cudaGetLastError());
 	disc->last_launches = 1;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_tc_selftest(int kind, const float *d_A, const float *d_B, float *d_C, int device) {
+	if (kind != 1 && kind != 2) return fail(H3DG_ERR_INVALID_ARG, "tc_selftest: kind must be 1 (bf16) or 2 (tf32)");
+	H3DG_CUDA_TRY(cudaSetDevice(device));
+	int *st = nullptr;
+	H3DG_CUDA_TRY(cudaMalloc(&st, sizeof(int)));
+	H3DG_CUDA_TRY(cudaMemset(st, 0, sizeof(int)));
+	if (kind == 2) h3dg::k_tc_selftest<h3dg::tc::kTF32><<<1, 128>>>(d_A, d_B, d_C, st);
+	else h3dg::k_tc_selftest<h3dg::tc::kBF16><<<1, 128>>>(d_A, d_B, d_C, st);
+	cudaError_t e = cudaDeviceSynchronize();
+	int hs = 0;
+	if (e == cudaSuccess) e = cudaMemcpy(&hs, st, sizeof(int), cudaMemcpyDeviceToHost);
+	cudaFree(st);
+	if (e != cudaSuccess) return fail(H3DG_ERR_CUDA, std::string("tc_selftest: ") + cudaGetErrorString(e));
+	if (hs) return fail(H3DG_ERR_TIMEOUT, "tc_selftest: MMA completion wait gave up");
 	return H3DG_OK;
 }
 
