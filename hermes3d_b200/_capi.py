@@ -22,6 +22,7 @@ BF_GRAD_GRAD, BF_GRAD_GRAD_MASS = 1, 2
 LF_NONE, LF_CONST, LF_SIN = 0, 1, 2
 QUAD_FIXED, QUAD_P_PLUS = 0, 1
 PREC_FP64 = 0
+PREC_TF32X3 = 1
 
 BC_TYPE_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.c_void_p)
 BC_VALUE_FN = C.CFUNCTYPE(C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, C.c_void_p)

@@ -2,12 +2,8 @@
 #include "../../include/h3dg.h"
 #include "host/h3dg_host.h"
 #include "host/lobatto.h"
-#include "kernels/asm_fp64.cuh"
-#include "kernels/asm_fp64_seq.cuh"
-#include "kernels/asm_fp64_ho.cuh"
-#include "kernels/adjoint.cuh"
+#include "kernel_tables.h"
 #include "kernels/tc_selftest.cuh"
-#include <cuda_bf16.h>
 #include "kernels/geom.cuh"
 
 #include <cuda_runtime.h>
@@ -407,105 +403,17 @@ h3dg_status h3dg_disc_get_pattern(const h3dg_disc *disc, int64_t *Ap, int32_t *A
 
 } // extern "C"
 
-namespace {
-
-using KernelFn = void (*)(h3dg::KArgs, int64_t, int64_t);
-
-struct KernelSpec {
-	int p, nq;
-	KernelFn fn;
-	int threads, eb;
-	size_t smem;
-	bool configured;
-};
-
-template <int P, int NQ, int NT, int EB, int MINB = 1>
-KernelSpec spec() {
-	return KernelSpec { P, NQ, &h3dg::k_assemble_fp64<P, P, P, NQ, NQ, NQ, NT, EB, MINB>, NT, EB,
-	                    h3dg::SfShape<P, P, P, NQ, NQ, NQ, EB>::SMEM_BYTES, false };
-}
-
-template <int P, int NQ, int NT, int EB>
-KernelSpec spec_seq() {
-	return KernelSpec { P, NQ, &h3dg::k_assemble_fp64_seq<P, P, P, NQ, NQ, NQ, NT, EB>, NT, EB,
-	                    h3dg::SfShapeSeq<P, P, P, NQ, NQ, NQ, EB>::SMEM_BYTES, false };
-}
-
-// FP64 kernel variants per (order, points); the autotuner times each on the
-// actual plan at the first assembly and keeps the fastest.
-std::vector<KernelSpec> &kernel_table() {
-	static std::vector<KernelSpec> t = {
-		spec<1, 2, 64, 4, 8>(), spec<1, 3, 64, 4, 8>(), spec<1, 2, 128, 8, 4>(), spec<1, 3, 128, 8, 4>(),
-		spec<2, 3, 96, 1, 8>(), spec<2, 3, 192, 2, 4>(),
-		spec<2, 4, 96, 1>(), spec<2, 4, 96, 1, 8>(), spec<2, 4, 96, 1, 10>(), spec<2, 4, 128, 1, 8>(),
-		spec<2, 4, 192, 2, 4>(), spec<2, 4, 192, 2, 5>(), spec<2, 4, 256, 3, 3>(),
-		spec<2, 5, 96, 1, 8>(), spec<2, 5, 192, 2, 4>(),
-		spec<3, 4, 256, 1, 3>(), spec<3, 5, 256, 1>(), spec<3, 5, 256, 1, 3>(), spec<3, 5, 512, 2>(),
-		spec<3, 6, 256, 1, 2>(),
-		spec<4, 5, 640, 1>(), spec<4, 6, 640, 1>(), spec_seq<4, 6, 512, 1>(),
-	};
-	return t;
-}
-
-using HoFn = void (*)(h3dg::KArgsHO, int64_t, int64_t);
-
-struct HoSpec {
-	int p, nq;
-	HoFn fn;
-	int threads;
-	size_t smem;
-	bool configured;
-};
-
-template <int P, int NQ, int NT>
-HoSpec ho_spec() {
-	return HoSpec { P, NQ, &h3dg::k_assemble_fp64_ho<P, P, P, NQ, NQ, NQ, NT>, NT,
-	                h3dg::HoShape<P, P, P, NQ, NQ, NQ>::SMEM_BYTES, false };
-}
-
-std::vector<HoSpec> &ho_table() {
-	static std::vector<HoSpec> t = {
-		ho_spec<2, 4, 128>(), ho_spec<3, 5, 256>(),
-		ho_spec<5, 6, 256>(), ho_spec<5, 7, 256>(), ho_spec<6, 7, 256>(), ho_spec<6, 8, 256>(),
-		ho_spec<7, 8, 256>(), ho_spec<7, 9, 256>(), ho_spec<8, 9, 256>(), ho_spec<8, 10, 256>(),
-		ho_spec<8, 10, 384>(),
-	};
-	return t;
-}
-
-using AdjFn = void (*)(h3dg::AdjArgs);
-
-struct AdjSpec {
-	int p, nq;
-	AdjFn fn;
-	size_t smem;
-	bool configured;
-};
-
-template <int P, int NQ>
-AdjSpec adj_spec() {
-	return AdjSpec { P, NQ, &h3dg::k_adjoint<P, P, P, NQ, NQ, NQ, 128>, h3dg::AdjShape<P, P, P, NQ, NQ, NQ>::SMEM_BYTES, false };
-}
-
-std::vector<AdjSpec> &adj_table() {
-	static std::vector<AdjSpec> t = {
-		adj_spec<1, 2>(), adj_spec<1, 3>(), adj_spec<2, 3>(), adj_spec<2, 4>(), adj_spec<3, 4>(), adj_spec<3, 5>(),
-		adj_spec<4, 5>(), adj_spec<4, 6>(), adj_spec<5, 6>(), adj_spec<5, 7>(), adj_spec<6, 7>(), adj_spec<6, 8>(),
-		adj_spec<8, 10>(),
-	};
-	return t;
-}
-
-} // namespace
+using namespace h3dg_tables;
 
 extern "C" {
 
-static h3dg_status assemble_ho(h3dg_disc *disc, double *d_Ax, double *d_rhs, cudaStream_t st) {
+static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, cudaStream_t st) {
 	const h3dg::Plan &P = disc->plan;
+	std::vector<HoSpec> &table = precision == H3DG_PREC_TF32X3 ? ho_tc_table() : ho_table();
 	std::vector<int> cands;
-	for (size_t i = 0; i < ho_table().size(); i++)
-		if (ho_table()[i].p == P.px && ho_table()[i].nq == P.nqx) cands.push_back((int) i);
-	if (cands.empty()) return fail(H3DG_ERR_INVALID_ARG, "assemble: no high-order kernel instantiated for this order / rule");
+	for (size_t i = 0; i < table.size(); i++)
+		if (table[i].p == P.px && table[i].nq == P.nqx) cands.push_back((int) i);
+	if (cands.empty()) return fail(H3DG_ERR_INVALID_ARG, "assemble: no high-order kernel instantiated for this order / rule / precision");
 	h3dg::KArgsHO a;
 	a.xyz = disc->xyz.p;
 	a.el_vtx = disc->el_vtx.p;
@@ -527,7 +435,7 @@ static h3dg_status assemble_ho(h3dg_disc *disc, double *d_Ax, double *d_rhs, cud
 	if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
 	int nsm = 148;
 	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
-	HoSpec &k = ho_table()[cands.back()];
+	HoSpec &k = table[cands.back()];
 	if (!k.configured) {
 		H3DG_CUDA_TRY(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) k.smem));
 		k.configured = true;
@@ -556,7 +464,7 @@ static h3dg_status assemble_ho(h3dg_disc *disc, double *d_Ax, double *d_rhs, cud
 
 h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream) {
 	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "assemble: create_pattern() first");
-	if (precision != H3DG_PREC_FP64) return fail(H3DG_ERR_INVALID_ARG, "assemble: unknown precision");
+	if (precision != H3DG_PREC_FP64 && precision != H3DG_PREC_TF32X3) return fail(H3DG_ERR_INVALID_ARG, "assemble: unknown precision");
 	const h3dg::Plan &P = disc->plan;
 	if (P.px != P.py || P.px != P.pz || P.nqx != P.nqy || P.nqx != P.nqz)
 		return fail(H3DG_ERR_INVALID_ARG, "assemble: anisotropic orders need the batched path");
@@ -564,7 +472,7 @@ h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, dou
 		h3dg_status s0 = ensure_device(disc);
 		if (s0 != H3DG_OK) return s0;
 		H3DG_CUDA_TRY(cudaSetDevice(disc->device));
-		return assemble_ho(disc, d_Ax, d_rhs, (cudaStream_t) stream);
+		return assemble_ho(disc, precision, d_Ax, d_rhs, (cudaStream_t) stream);
 	}
 	std::vector<int> cands;
 	for (size_t i = 0; i < kernel_table().size(); i++)

@@ -1,0 +1,57 @@
+// Kernel variant tables.  Each table lives in its own translation unit so
+// the template instantiations compile in parallel; the dispatcher in
+// h3dg_capi.cu only sees function pointers, launch shapes and shared-memory
+// sizes.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "kernels/common.cuh"
+#include "kernels/asm_fp64_ho.cuh"
+#include "kernels/adjoint.cuh"
+
+namespace h3dg_tables {
+
+using KernelFn = void (*)(h3dg::KArgs, int64_t, int64_t);
+
+struct KernelSpec {
+	int p, nq;
+	KernelFn fn;
+	int threads, eb;
+	size_t smem;
+	bool configured;
+};
+
+using HoFn = void (*)(h3dg::KArgsHO, int64_t, int64_t);
+
+struct HoSpec {
+	int p, nq;
+	HoFn fn;
+	int threads;
+	size_t smem;
+	bool configured;
+};
+
+using AdjFn = void (*)(h3dg::AdjArgs);
+
+struct AdjSpec {
+	int p, nq;
+	AdjFn fn;
+	size_t smem;
+	bool configured;
+};
+
+// FP64 low-order kernels (register / shared-memory element matrix); the
+// autotuner times each candidate for an (order, points) pair on the actual
+// plan at the first assembly and keeps the fastest.
+std::vector<KernelSpec> &kernel_table();
+// FP64 high-order kernels (element matrix never materialised)
+std::vector<HoSpec> &ho_table();
+// split-precision high-order kernels (tcgen05 3xTF32 stage 3)
+std::vector<HoSpec> &ho_tc_table();
+// adjoint (element sensitivity) kernels
+std::vector<AdjSpec> &adj_table();
+
+} // namespace h3dg_tables

@@ -82,7 +82,7 @@ struct SfShape {
 
 // flags of the 7 terms: per direction, f = 2*alpha + beta (alpha: test side
 // differentiated, beta: trial side differentiated)
-__device__ __constant__ int kTermFlags[7][3] = {
+static __device__ __constant__ int kTermFlags[7][3] = {
 	{ 3, 0, 0 }, { 0, 3, 0 }, { 0, 0, 3 },   // xx yy zz
 	{ 2, 1, 0 }, { 2, 0, 1 }, { 0, 2, 1 },   // xy xz yz
 	{ 0, 0, 0 }                               // mass
@@ -90,7 +90,7 @@ __device__ __constant__ int kTermFlags[7][3] = {
 
 // stage-1 products k = xx, yy, zz(+mass), xy, xz, yz: (x, y, z) table flags
 // and the x-class each feeds (0: Wx^0, 1: Wx^2, 2: Wx^3)
-__device__ __constant__ int kT1Flags[6][3] = {
+static __device__ __constant__ int kT1Flags[6][3] = {
 	{ 3, 0, 0 }, { 0, 3, 0 }, { 0, 0, 3 }, { 2, 1, 0 }, { 2, 0, 1 }, { 0, 2, 1 }
 };
 

@@ -208,20 +208,24 @@ class Discretization:
         if rhs is not None:
             rhs.v = np.zeros(self.ndof, np.float64)
 
-    def assemble(self, matrix: Optional[UMFPackMatrix] = None, rhs: Optional[UMFPackVector] = None):
-        """Discretization::assemble into the host sinks (copies inside)."""
+    def assemble(self, matrix: Optional[UMFPackMatrix] = None, rhs: Optional[UMFPackVector] = None,
+                 precision: int = capi.PREC_FP64):
+        """Discretization::assemble into the host sinks (copies inside).
+        ``precision``: PREC_FP64 (default, the reference's arithmetic) or
+        PREC_TF32X3 (tensor-core split precision for the high-order path,
+        normwise relative error below 1e-6)."""
         ax = None if matrix is None else matrix.Ax
         rv = None if rhs is None else rhs.v
-        capi.call("h3dg_disc_assemble_host", self.handle, capi.PREC_FP64, capi.ptr(ax, C.c_double), capi.ptr(rv, C.c_double))
+        capi.call("h3dg_disc_assemble_host", self.handle, precision, capi.ptr(ax, C.c_double), capi.ptr(rv, C.c_double))
 
-    def assemble_device(self, Ax, rhs=None, stream=None):
+    def assemble_device(self, Ax, rhs=None, stream=None, precision: int = capi.PREC_FP64):
         """Assemble into device tensors (torch CUDA float64) on ``stream``
         (default: torch's current stream)."""
         import torch
         if stream is None:
             stream = torch.cuda.current_stream(Ax.device if Ax is not None else rhs.device)
         sp = C.c_void_p(stream.cuda_stream)
-        capi.call("h3dg_disc_assemble", self.handle, capi.PREC_FP64,
+        capi.call("h3dg_disc_assemble", self.handle, precision,
                   C.c_void_p(Ax.data_ptr()) if Ax is not None else None,
                   C.c_void_p(rhs.data_ptr()) if rhs is not None else None, sp)
 

@@ -58,6 +58,13 @@ typedef int h3dg_status;
 
 /* arithmetic of the element-matrix contraction */
 #define H3DG_PREC_FP64    0
+/* Split precision: geometry, load vector, lifting and coefficient products
+ * in FP64; the z / y sum-factorisation stages in FP32; the x stage on the
+ * tensor cores as three TF32 products (hi*hi + hi*lo + lo*hi) with FP32
+ * accumulation.  Normwise relative error of the matrix below 1e-6.  Used by
+ * the high-order path; where the FP64 kernels are the faster choice (low
+ * orders) the matrix is assembled in FP64. */
+#define H3DG_PREC_TF32X3  1
 
 typedef struct h3dg_mesh h3dg_mesh;
 typedef struct h3dg_space h3dg_space;

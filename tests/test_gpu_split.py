@@ -1,0 +1,114 @@
+"""Split precision (PREC_TF32X3: FP64 geometry / load vector / lifting,
+FP32 z and y stages, 3xTF32 x stage on tcgen05) against the FP64 kernel,
+the reference fixtures and the restatement oracle.
+
+Tolerance: 1e-6 of the largest matrix entry, entrywise (max |dA| / max |A|),
+and 1e-6 normwise (||dA||_2 / ||A||_2).  The load vector is FP64 throughout,
+so it keeps the FP64 tolerance."""
+import os
+
+import numpy as np
+import pytest
+
+import hermes3d_b200 as h
+from helpers import FP64_RTOL, disc_of, load, rel_err, space_of
+from oracle import port
+
+pytestmark = pytest.mark.gpu
+
+SPLIT_RTOL = 1e-6
+
+
+def _norm_err(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture
+def force_high_order():
+    os.environ["H3DG_FORCE_HIGH_ORDER"] = "1"
+    yield
+    del os.environ["H3DG_FORCE_HIGH_ORDER"]
+
+
+@pytest.mark.parametrize("name", ["c1_small", "perm_p3_mass_sin", "perm_p2_lifting", "coef_p3"])
+def test_split_on_reference_fixtures(gpu, force_high_order, name):
+    g = load(name)
+    sp = space_of(g)
+    d = disc_of(g, sp)
+    M, V = h.UMFPackMatrix(), h.UMFPackVector()
+    d.create(M, V)
+    d.assemble(M, V, precision=h.PREC_TF32X3)
+    e_max, e_norm = rel_err(M.Ax, g["Ax"]), _norm_err(M.Ax, g["Ax"])
+    print("%s: split error max %.2e norm %.2e" % (name, e_max, e_norm))
+    assert e_max < SPLIT_RTOL and e_norm < SPLIT_RTOL
+    assert rel_err(V.v, g["rhs"]) < FP64_RTOL
+
+
+@pytest.mark.parametrize("p,bc,n", [(5, "lifting", 2), (6, "dirichlet0", 2), (8, "natural", 1)])
+def test_split_matches_restatement(gpu, p, bc, n):
+    mesh = h.permute_vertices(h.unit_cube(n, 0.15, 3), seed=p)
+    mesh.ugh()
+    sp = h.H1Space(mesh)
+    if bc == "natural":
+        sp.set_bc_types(lambda m: h.BC_NATURAL)
+    if bc == "lifting":
+        sp.set_bc_values(lambda m, x, y, z: x * x + y * y + z * z)
+    sp.set_uniform_order(p)
+    sp.assign_dofs()
+    d = h.Discretization()
+    d.set_spaces(sp)
+    coef = np.random.default_rng(p).uniform(0.5, 2.0, mesh.num_elements)
+    d.set_bilinear_form(h.int_grad_u_grad_v_plus_u_v if bc != "dirichlet0" else h.int_grad_u_grad_v, coef)
+    d.set_linear_form(h.int_F_v(-6.0 if bc == "lifting" else "sin"))
+    d.set_quadrature(p_plus=2)
+    M, V = h.UMFPackMatrix(), h.UMFPackVector()
+    d.create(M, V)
+    d.assemble(M, V, precision=h.PREC_TF32X3)
+    al = port.asmlists_from_space(sp, mesh.num_elements)
+    Ax, rhs = port.assemble(mesh.xyz, mesh.hexes - 1, p + 2, al, sp.ndof, M.Ap, M.Ai, mass=(bc != "dirichlet0"),
+                            gradcoef=coef, lf=1 if bc == "lifting" else 2, lf_value=-6.0)
+    e_max, e_norm = rel_err(M.Ax, Ax), _norm_err(M.Ax, Ax)
+    print("p=%d %s: split error max %.2e norm %.2e" % (p, bc, e_max, e_norm))
+    assert e_max < SPLIT_RTOL and e_norm < SPLIT_RTOL
+    assert rel_err(V.v, rhs) < FP64_RTOL
+
+
+def test_split_is_deterministic_and_close_to_fp64(gpu):
+    import torch
+    mesh = h.unit_cube(3, 0.2, 11)
+    mesh.ugh()
+    sp = h.H1Space(mesh)
+    sp.set_uniform_order(6)
+    sp.assign_dofs()
+    d = h.Discretization()
+    d.set_spaces(sp)
+    d.set_bilinear_form(h.int_grad_u_grad_v, np.random.default_rng(1).uniform(0.5, 2.0, mesh.num_elements))
+    d.set_linear_form(None)
+    d.set_quadrature(points=8)
+    d.create()
+    A64 = torch.empty(d.nnz, dtype=torch.float64, device="cuda")
+    A1, A2 = torch.empty_like(A64), torch.empty_like(A64)
+    d.assemble_device(A64)
+    d.assemble_device(A1, precision=h.PREC_TF32X3)
+    d.assemble_device(A2, precision=h.PREC_TF32X3)
+    torch.cuda.synchronize()
+    assert torch.equal(A1, A2)
+    a, b = A1.cpu().numpy(), A64.cpu().numpy()
+    assert rel_err(a, b) < SPLIT_RTOL and _norm_err(a, b) < SPLIT_RTOL
+    # the split result is not the FP64 one (the tensor path really ran)
+    assert not np.array_equal(a, b)
+
+
+def test_split_low_order_uses_fp64(gpu):
+    """Below the high-order threshold the FP64 kernels are the faster choice;
+    PREC_TF32X3 then returns the FP64 matrix."""
+    g = load("p2_c2_forms")
+    sp = space_of(g)
+    d = disc_of(g, sp)
+    M, V = h.UMFPackMatrix(), h.UMFPackVector()
+    d.create(M, V)
+    d.assemble(M, V, precision=h.PREC_TF32X3)
+    M2, V2 = h.UMFPackMatrix(), h.UMFPackVector()
+    d.create(M2, V2)
+    d.assemble(M2, V2)
+    assert np.array_equal(M.Ax, M2.Ax)
