@@ -85,6 +85,7 @@ struct h3dg_disc {
 	DBuf<int64_t> Ap;
 	DBuf<int32_t> Ai, el_vtx, el_cnt, el_dof, el_id;
 	DBuf<uint16_t> el_s, el_off, el_offc;
+	DBuf<uint16_t> el_offt;    // tensor-core scatter stream (built at the first split-precision assembly)
 	DBuf<int32_t> el_cdof;
 	DBuf<double> el_ccoef;
 	DBuf<double> el_coef;
@@ -372,6 +373,7 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 		H3DG_CUDA_TRY(disc->el_cdof.upload(P.el_cdof));
 		H3DG_CUDA_TRY(disc->el_ccoef.upload(P.el_ccoef));
 		H3DG_CUDA_TRY(disc->el_offc.upload(P.el_offc));
+		disc->el_offt.release();
 	}
 	else {
 		H3DG_CUDA_TRY(disc->el_s.upload(P.el_s));
@@ -422,6 +424,23 @@ static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, dou
 	a.cdof = disc->el_cdof.p;
 	a.ccoef = disc->el_ccoef.p;
 	a.offc = disc->el_offc.p;
+	if (precision == H3DG_PREC_TF32X3 && d_Ax && !disc->el_offt.p && P.ne > 0) {
+		// built once per plan; the build validates every position against its
+		// column, so the split kernel posts without a per-entry bounds test
+		size_t cnt = 0;
+		H3DG_CUDA_TRY(build_offt(disc->el_offc.p, disc->el_cdof.p, disc->Ap.p, P.ne, P.px, P.nqx, &disc->el_offt.p, &cnt,
+		                         disc->status.p, st));
+		disc->el_offt.n = cnt;
+		int hs = 0;
+		H3DG_CUDA_TRY(cudaMemcpyAsync(&hs, disc->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+		H3DG_CUDA_TRY(cudaStreamSynchronize(st));
+		if (hs & h3dg::kErrBounds) {
+			disc->el_offt.release();
+			cudaMemsetAsync(disc->status.p, 0, sizeof(int), st);
+			return fail(H3DG_ERR_STATE, "assemble: a scatter position falls outside its column (plan corrupt)");
+		}
+	}
+	a.offt = disc->el_offt.p;
 	a.Ap = disc->Ap.p;
 	a.tables = disc->tables.p;
 	a.table_bytes = disc->table_bytes;

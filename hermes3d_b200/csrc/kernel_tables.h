@@ -8,6 +8,8 @@
 #include <cstdint>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "kernels/common.cuh"
 #include "kernels/asm_fp64_ho.cuh"
 #include "kernels/adjoint.cuh"
@@ -51,6 +53,9 @@ std::vector<KernelSpec> &kernel_table();
 std::vector<HoSpec> &ho_table();
 // split-precision high-order kernels (tcgen05 3xTF32 stage 3)
 std::vector<HoSpec> &ho_tc_table();
+// tensor-core scatter stream from the canonical position map (async on st)
+cudaError_t build_offt(const uint16_t *offc, const int32_t *cdof, const int64_t *Ap, int64_t ne, int px, int nq,
+                       uint16_t **offt, size_t *count, int *status, cudaStream_t st);
 // adjoint (element sensitivity) kernels
 std::vector<AdjSpec> &adj_table();
 

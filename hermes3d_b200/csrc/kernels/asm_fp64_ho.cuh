@@ -35,6 +35,7 @@ struct KArgsHO {
 	const int32_t *cdof;       // ne x nl: DOF of canonical function i, -1 if not a matrix entry
 	const double *ccoef;       // ne x nl: sign x AsmList coefficient (lifting value when cdof = -1), 0 if absent
 	const uint16_t *offc;      // ne x nl x nl: [i][j] row position of cdof_i in column cdof_j
+	const uint16_t *offt;      // tensor-core scatter stream (k_build_offt), or nullptr
 	const int64_t *Ap;
 	const double *tables;
 	int table_bytes;

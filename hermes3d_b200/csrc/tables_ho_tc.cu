@@ -18,4 +18,16 @@ std::vector<HoSpec> &ho_tc_table() {
 	return t;
 }
 
+cudaError_t build_offt(const uint16_t *offc, const int32_t *cdof, const int64_t *Ap, int64_t ne, int px, int nq,
+                       uint16_t **offt, size_t *count, int *status, cudaStream_t st) {
+	(void) nq;
+	const int nx = px + 1, nb = (nx * nx + 15) / 16 * 16;
+	const size_t n = (size_t) ne * nx * (size_t) (nx * nx * nx) * nb;
+	cudaError_t e = cudaMalloc((void **) offt, sizeof(uint16_t) * n);
+	if (e != cudaSuccess) return e;
+	*count = n;
+	h3dg::k_build_offt<<<148 * 8, 256, 0, st>>>(offc, cdof, Ap, ne, nx, nx, nx, nb, *offt, status);
+	return cudaGetLastError();
+}
+
 } // namespace h3dg_tables
