@@ -12,6 +12,8 @@ import os
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libh3dg.so")
 
 H3DG_OK = 0
+H3DG_ERR_STATE = 6
+H3DG_ERR_TOO_LARGE = 8
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "unsupported form",
     5: "mesh error", 6: "call out of order", 7: "device wait timed out", 8: "size limit exceeded",
@@ -23,6 +25,7 @@ LF_NONE, LF_CONST, LF_SIN = 0, 1, 2
 QUAD_FIXED, QUAD_P_PLUS = 0, 1
 PREC_FP64 = 0
 PREC_TF32X3 = 1
+NOALLOC_SCRATCH_DOUBLES = 2 << 20
 
 BC_TYPE_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.c_void_p)
 BC_VALUE_FN = C.CFUNCTYPE(C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, C.c_void_p)
@@ -70,6 +73,7 @@ SIGNATURES = {
     "h3dg_disc_geometry": [_p, _p, _p, _p, _p],
     "h3dg_disc_adjoint": [_p, C.c_int, _p, _p, _p, _p, _p, _p],
     "h3dg_tc_selftest": [C.c_int, _p, _p, _p, C.c_int],
+    "h3dg_disc_assemble_host_noalloc": [_p, C.c_int, _p, _p],
     "h3dg_disc_enable_kernel_timing": [_p, _i32],
     "h3dg_disc_get_tuning": [_p, _pi32, _pi32, C.POINTER(C.c_float)],
     "h3dg_disc_kernel_times": [_p, C.POINTER(C.c_float), _i32, _pi32],

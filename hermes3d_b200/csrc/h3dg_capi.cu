@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -720,6 +721,78 @@ h3dg_status h3dg_disc_assemble_host(h3dg_disc *disc, int precision, double *Ax, 
 		cudaMemset(disc->status.p, 0, sizeof(int));
 		if (st & h3dg::kErrBounds) return fail(H3DG_ERR_STATE, "assemble_host: a scatter target fell outside its column (plan corrupt)");
 		return fail(H3DG_ERR_TIMEOUT, "assemble_host: a device wait gave up");
+	}
+	return H3DG_OK;
+}
+
+} // extern "C"
+
+// Staging array of h3dg_disc_assemble_host_noalloc (16 MiB per device,
+// reserved when the module loads; no allocation at call time).
+static __device__ __align__(256) double g_noalloc_scratch[H3DG_NOALLOC_SCRATCH_DOUBLES];
+
+static h3dg_status noalloc_scratch(int device, double **out) {
+	constexpr int kMaxDevices = 64;
+	static std::mutex mu;
+	static double *ptrs[kMaxDevices] = {};
+	if (device < 0 || device >= kMaxDevices) return fail(H3DG_ERR_INVALID_ARG, "assemble_host_noalloc: device index out of range");
+	std::lock_guard<std::mutex> lock(mu);
+	if (!ptrs[device]) {
+		// set-up once per device, with that device current
+		double *p = nullptr;
+		cudaError_t e = cudaGetSymbolAddress((void **) &p, g_noalloc_scratch);
+		if (e != cudaSuccess || !p)
+			return fail(H3DG_ERR_CUDA, std::string("assemble_host_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+		ptrs[device] = p;
+	}
+	*out = ptrs[device];
+	return H3DG_OK;
+}
+
+extern "C" {
+
+h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, double *Ax, double *rhs) {
+	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "assemble_host_noalloc: create_pattern() first");
+	if (precision != H3DG_PREC_FP64 && precision != H3DG_PREC_TF32X3)
+		return fail(H3DG_ERR_INVALID_ARG, "assemble_host_noalloc: unknown precision");
+	const h3dg::Plan &P = disc->plan;
+	const size_t rhs_off = ((size_t) P.nnz + 31) / 32 * 32;          // 256-byte boundary
+	const size_t need = (rhs ? rhs_off + (size_t) P.ndof : (size_t) P.nnz);
+	if (need > (size_t) H3DG_NOALLOC_SCRATCH_DOUBLES)
+		return fail(H3DG_ERR_TOO_LARGE, "assemble_host_noalloc: nnz + ndof = " + std::to_string(need) +
+		                                    " doubles exceed the fixed staging array of " +
+		                                    std::to_string((size_t) H3DG_NOALLOC_SCRATCH_DOUBLES) +
+		                                    " (16 MiB); use h3dg_disc_assemble_host");
+	// everything h3dg_disc_assemble would allocate lazily must already exist
+	if (!disc->on_device || !disc->status.p)
+		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: device plan not uploaded; make one allocating assembly call first");
+	if (P.canon && precision == H3DG_PREC_TF32X3 && Ax && !disc->el_offt.p && P.ne > 0)
+		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: split-precision scatter stream not built; make one allocating "
+		                            "split-precision assembly call first");
+	if (!P.canon && disc->variant < 0) {
+		int ncand = 0;
+		for (size_t i = 0; i < kernel_table().size(); i++)
+			if (kernel_table()[i].p == P.px && kernel_table()[i].nq == P.nqx) ncand++;
+		if (ncand > 1)
+			return fail(H3DG_ERR_STATE, "assemble_host_noalloc: kernel variant not tuned yet; make one allocating assembly "
+			                            "call first");
+	}
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	double *scratch = nullptr;
+	h3dg_status s0 = noalloc_scratch(disc->device, &scratch);
+	if (s0 != H3DG_OK) return s0;
+	double *d_Ax = Ax ? scratch : nullptr;
+	double *d_rhs = rhs ? scratch + rhs_off : nullptr;
+	h3dg_status s = h3dg_disc_assemble(disc, precision, d_Ax, d_rhs, nullptr);   // zeroes its outputs first
+	if (s != H3DG_OK) return s;
+	if (Ax) H3DG_CUDA_TRY(cudaMemcpy(Ax, d_Ax, sizeof(double) * P.nnz, cudaMemcpyDeviceToHost));
+	if (rhs) H3DG_CUDA_TRY(cudaMemcpy(rhs, d_rhs, sizeof(double) * P.ndof, cudaMemcpyDeviceToHost));
+	int st = 0;
+	H3DG_CUDA_TRY(cudaMemcpy(&st, disc->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+	if (st) {
+		cudaMemset(disc->status.p, 0, sizeof(int));
+		if (st & h3dg::kErrBounds) return fail(H3DG_ERR_STATE, "assemble_host_noalloc: a scatter target fell outside its column (plan corrupt)");
+		return fail(H3DG_ERR_TIMEOUT, "assemble_host_noalloc: a device wait gave up");
 	}
 	return H3DG_OK;
 }

@@ -218,6 +218,20 @@ class Discretization:
         rv = None if rhs is None else rhs.v
         capi.call("h3dg_disc_assemble_host", self.handle, precision, capi.ptr(ax, C.c_double), capi.ptr(rv, C.c_double))
 
+    def assemble_noalloc(self, matrix: Optional[UMFPackMatrix] = None, rhs: Optional[UMFPackVector] = None,
+                         precision: int = capi.PREC_FP64):
+        """``assemble`` without any device allocation (no reference
+        counterpart): stages Ax and rhs in the library's fixed 16 MiB device
+        array, so it serves callers that cannot allocate device memory (a
+        pool holds it all, or cudaFree's device-wide synchronisation is not
+        acceptable).  Raises H3dgError TOO_LARGE above that size and STATE
+        unless one ``assemble`` with the same precision came first.
+        Overlapping calls on one device race on the array."""
+        ax = None if matrix is None else matrix.Ax
+        rv = None if rhs is None else rhs.v
+        capi.call("h3dg_disc_assemble_host_noalloc", self.handle, precision, capi.ptr(ax, C.c_double),
+                  capi.ptr(rv, C.c_double))
+
     def assemble_device(self, Ax, rhs=None, stream=None, precision: int = capi.PREC_FP64):
         """Assemble into device tensors (torch CUDA float64) on ``stream``
         (default: torch's current stream)."""

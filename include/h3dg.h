@@ -136,6 +136,24 @@ h3dg_status h3dg_disc_get_pattern(const h3dg_disc *disc, int64_t *Ap, int32_t *A
 h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream);
 /* the same into host arrays (UMFPackMatrix::Ax / UMFPackVector::v); copies inside */
 h3dg_status h3dg_disc_assemble_host(h3dg_disc *disc, int precision, double *Ax, double *rhs);
+/* No reference counterpart.  h3dg_disc_assemble_host without any device
+ * allocation, for callers that must not allocate: an application whose
+ * device memory is fully reserved by its own pool (cudaMalloc would fail),
+ * or one that cannot afford the implicit device-wide synchronisation of
+ * cudaFree while other streams run.  Ax and rhs are staged in a fixed
+ * 16 MiB device array of the library (H3DG_NOALLOC_SCRATCH_DOUBLES doubles,
+ * shared by Ax and rhs, the rhs part starting on a 256-byte boundary);
+ * larger problems are rejected with H3DG_ERR_TOO_LARGE.  Preconditions
+ * (H3DG_ERR_STATE otherwise): one allocating device call on this disc with
+ * the same precision came first (h3dg_disc_assemble or
+ * h3dg_disc_assemble_host), so the device plan, the autotuned variant and
+ * the split-precision scatter stream exist.  The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress) with that device
+ * current; make it outside any stream capture.  The array is zeroed by the
+ * assembly itself.  Calls that overlap in time on one device share the
+ * array and race: serialise them. */
+#define H3DG_NOALLOC_SCRATCH_DOUBLES (2u << 20)
+h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, double *Ax, double *rhs);
 /* replace the vertex coordinates (same topology) from host memory, nv x 3 */
 h3dg_status h3dg_disc_update_vertices(h3dg_disc *disc, const double *xyz, int64_t nv);
 /* replace the per-element coefficient (ne values, element-id order) from host memory */
