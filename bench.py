@@ -192,7 +192,7 @@ def run_reference_arm(args):
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "vs_baseline": None, "dtype": "f64" if prec == h.PREC_FP64 else "tf32x3 (x stage) + f32 (z, y stages) + f64", "data": "synthetic", "impl": "reference",
         "config": {"workload": "C2 sample: %d^3 jittered hexahedra per process, p=2, 4^3 Gauss points, grad+mass, "
                                "sin source" % n, "processes": ncores},
         "cpu_baseline": {"value": value, "unit": "elements/s", "cores": ncores, "kind": "reference",
@@ -212,6 +212,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--side", type=int, default=N_ELEM_SIDE, help="elements per cube side (profiling runs only)")
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3"],
+                    help="tf32x3: split precision (tcgen05 3xTF32 x stage; high-order path)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -238,12 +240,13 @@ def main():
     mesh, sp, d = build_problem(h, seed=rank, device=local, side=args.side, workload=args.workload)
     t_setup = time.time() - t_setup
     ne, ndof, nnz, nv = mesh.num_elements, d.ndof, d.nnz, mesh.num_vertices
+    prec = h.PREC_TF32X3 if args.precision == "tf32x3" else h.PREC_FP64
     stream = torch.cuda.current_stream()
     Ax = torch.empty(nnz, dtype=torch.float64, device="cuda")
     rhs = torch.empty(ndof, dtype=torch.float64, device="cuda")
 
     for _ in range(max(3, args.warmup)):
-        d.assemble_device(Ax, rhs, stream)
+        d.assemble_device(Ax, rhs, stream, precision=prec)
     torch.cuda.synchronize()
     launches_per_step = d.last_launch_count()
 
@@ -255,7 +258,7 @@ def main():
     with ClockSampler(local) as clk:
         e0.record(stream)
         for _ in range(args.steps):
-            d.assemble_device(Ax, rhs, stream)
+            d.assemble_device(Ax, rhs, stream, precision=prec)
         e1.record(stream)
         torch.cuda.synchronize()
     barrier()
@@ -279,13 +282,13 @@ def main():
         M, V = h.UMFPackMatrix(), h.UMFPackVector()
         M.Ax, V.v = Ax_np, rhs_np
         d.update_vertices(xyz_np)
-        d.assemble(M, V)
+        d.assemble(M, V, precision=prec)
         barrier()
         torch.cuda.synchronize()
         c0 = time.perf_counter()
         for _ in range(args.e2e_steps):
             d.update_vertices(xyz_np)
-            d.assemble(M, V)
+            d.assemble(M, V, precision=prec)
         torch.cuda.synchronize()
         e2e_s = (time.perf_counter() - c0) / args.e2e_steps
         te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
@@ -296,6 +299,20 @@ def main():
         ok = bool(np.all(np.isfinite(Ax_np))) and bool(np.all(np.isfinite(rhs_np)))
     else:
         ok = bool(torch.isfinite(Ax).all().item())
+
+    # ---- split precision: error of the timed result against the FP64 kernel
+    split_error = None
+    if prec != h.PREC_FP64:
+        d.assemble_device(Ax, rhs, stream, precision=prec)
+        A64 = torch.empty_like(Ax)
+        d.assemble_device(A64, None, stream)
+        torch.cuda.synchronize()
+        diff = (Ax - A64)
+        split_error = {
+            "max_abs_over_max": float(diff.abs().max() / A64.abs().max()),
+            "frobenius_rel": float(torch.linalg.vector_norm(diff) / torch.linalg.vector_norm(A64)),
+            "tolerance": 1e-6, "against": "FP64 kernel on the same plan (itself oracle-checked at 1e-12)"}
+        del diff, A64
 
     if rank == 0:
         hbm, peak_kind = peaks()
@@ -309,12 +326,15 @@ def main():
                 traffic = json.load(open(tf)).get("bytes_per_step")
             except Exception:
                 traffic = None
+        metric = METRIC if args.workload == "c2" else METRIC.replace("C2: 64^3 jittered, p=2, 4^3 pts, grad+mass, sin source",
+                                                                        WORKLOADS[args.workload]["desc"])
+        if prec != h.PREC_FP64:
+            metric = metric.replace("(FP64, ", "(split precision 3xTF32 on tcgen05, FP64 geometry/scatter, ")
         out = {
-            "metric": METRIC if args.workload == "c2" else METRIC.replace("C2: 64^3 jittered, p=2, 4^3 pts, grad+mass, sin source",
-                                                                             WORKLOADS[args.workload]["desc"]),
+            "metric": metric,
             "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded jittered unit-cube mesh)",
+            "vs_baseline": None, "dtype": "f64" if prec == h.PREC_FP64 else "tf32x3 (x stage) + f32 (z, y stages) + f64", "data": "synthetic (seeded jittered unit-cube mesh)",
             "config": {"workload": WORKLOADS[args.workload]["desc"] if args.side == N_ELEM_SIDE or args.workload != "c2"
                        else "C2 forms on %d^3 elements (profiling size)" % args.side,
                        "ndof": ndof, "nnz": nnz, "elements_per_gpu": ne,
@@ -335,6 +355,8 @@ def main():
             "clocks": clk.summary(),
             "finite": ok,
         }
+        if split_error is not None:
+            out["split_error"] = split_error
         if not args.no_cpu_baseline and world == 1 and args.workload == "c2":
             try:
                 out["cpu_baseline"] = cpu_baseline()
