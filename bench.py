@@ -40,6 +40,10 @@ WORKLOADS = {
                     "f=sin(pi x)sin(pi y)sin(pi z), full CSC+RHS"),
     "c1": dict(side=8, jitter=0.0, p=3, nq=5, mass=False, lf=1.0, coef=None,
                desc="C1: 8^3 unit cube, p=3, 5^3 Gauss points, homogeneous Dirichlet, grad.grad, f=1"),
+    "c3": dict(side=32, jitter=0.0, p=(1, 6), nq=None, qplus=2, mass=False, lf=1.0, coef=None,
+               desc="C3 (unrefined): 32^3 hexahedra, anisotropic orders p_d ~ U{1..6} per element and direction "
+                    "(seeded), p_d+2 Gauss points per direction, grad.grad, f=1, homogeneous Dirichlet; "
+                    "mixed-order batched path (kernel classes, persistent CTAs, CUDA graph)"),
     "c4": dict(side=16, jitter=0.2, p=8, nq=10, mass=False, lf=None, coef=(0.5, 2.0),
                desc="C4: 16^3 jittered hexahedra, p=8, 10^3 Gauss points, a_e grad.grad, a_e ~ U[0.5,2]"),
     "c5": dict(side=32, jitter=0.2, p=3, nq=5, mass=False, lf=1.0, coef="lognormal",
@@ -112,7 +116,11 @@ def build_problem(h, seed, device, side=N_ELEM_SIDE, workload="c2"):
     mesh = h.unit_cube(side, w["jitter"], seed)
     mesh.ugh()
     sp = h.H1Space(mesh)
-    sp.set_uniform_order(w["p"])
+    if isinstance(w["p"], tuple):
+        lo, hi = w["p"]
+        sp.set_element_orders(np.random.default_rng(1000 + seed).integers(lo, hi + 1, size=(mesh.num_elements, 3)))
+    else:
+        sp.set_uniform_order(w["p"])
     sp.assign_dofs()
     d = h.Discretization(device)
     d.set_spaces(sp)
@@ -123,7 +131,10 @@ def build_problem(h, seed, device, side=N_ELEM_SIDE, workload="c2"):
         coef = np.random.default_rng(seed).uniform(w["coef"][0], w["coef"][1], mesh.num_elements)
     d.set_bilinear_form(h.int_grad_u_grad_v_plus_u_v if w["mass"] else h.int_grad_u_grad_v, coef)
     d.set_linear_form(None if w["lf"] is None else h.int_F_v(w["lf"]))
-    d.set_quadrature(points=w["nq"])
+    if w.get("qplus") is not None:
+        d.set_quadrature(p_plus=w["qplus"])
+    else:
+        d.set_quadrature(points=w["nq"])
     d.create()
     return mesh, sp, d
 
@@ -135,6 +146,11 @@ def algorithmic_bytes(nnz, ndof, nv, ne):
 
 def dense_flops_per_element(workload="c2"):
     w = WORKLOADS[workload]
+    if isinstance(w["p"], tuple):     # mixed orders: mean over the order distribution (independent directions)
+        ps = range(w["p"][0], w["p"][1] + 1)
+        m_nl2nq = (sum((p + 1) ** 2 * (p + w["qplus"]) for p in ps) / len(ps)) ** 3
+        m_nlnq = (sum((p + 1) * (p + w["qplus"]) for p in ps) / len(ps)) ** 3
+        return 2 * m_nl2nq * 3 + (2 * m_nl2nq if w["mass"] else 0) + (2 * m_nlnq if w["lf"] is not None else 0)
     nl = (w["p"] + 1) ** 3
     nq = w["nq"] ** 3
     return 2 * nl * nl * 3 * nq + (2 * nl * nl * nq if w["mass"] else 0) + (2 * nl * nq if w["lf"] is not None else 0)

@@ -95,8 +95,32 @@ struct h3dg_disc {
 	// kernel-only timing records
 	std::vector<cudaEvent_t> tev;
 	int tcap = 0, tn = 0;
+	// mixed-order path: plan tables, work counters, tuned variants, and the
+	// CUDA graph of one whole assembly (memsets + every launch), cached for
+	// the output pointers it was captured with
+	DBuf<int32_t> el_desc;
+	DBuf<int64_t> el_base, el_obase;
+	DBuf<uint16_t> el_offm;
+	DBuf<unsigned> mx_counters;
+	int mx_variant[h3dg::Plan::kClasses] = { -1, -1, -1 };
+	cudaGraphExec_t mx_exec = nullptr;
+	double *mx_ax = nullptr, *mx_rhs = nullptr;
+	int32_t mx_launches = 0;
+	cudaStream_t mx_s[2] = { nullptr, nullptr };
+	cudaEvent_t mx_ev[3] = { nullptr, nullptr, nullptr };
+	void reset_mixed() {
+		if (mx_exec) cudaGraphExecDestroy(mx_exec);
+		mx_exec = nullptr;
+		mx_ax = mx_rhs = nullptr;
+		for (int c = 0; c < h3dg::Plan::kClasses; c++) mx_variant[c] = -1;
+	}
 	~h3dg_disc() {
 		for (auto e : tev) cudaEventDestroy(e);
+		reset_mixed();
+		for (auto s : mx_s)
+			if (s) cudaStreamDestroy(s);
+		for (auto e : mx_ev)
+			if (e) cudaEventDestroy(e);
 	}
 };
 
@@ -347,7 +371,21 @@ h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nn
 	// (used by the parity tests to check that kernel on the low-order fixtures)
 	const char *force = std::getenv("H3DG_FORCE_HIGH_ORDER");
 	const bool canon = pmax >= 5 || (force && force[0] == '1');
-	if (h3dg::build_plan(sp, nq[0], nq[1], nq[2], disc->plan, err, canon) != 0) return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
+	// elements of different order triples: the mixed-order (batched) path;
+	// H3DG_FORCE_MIXED=1 routes uniform spaces there too (parity tests)
+	bool mixed = false;
+	for (int64_t e = 1; e < (int64_t) sp.order.size() / 3 && !mixed; e++)
+		for (int d = 0; d < 3; d++)
+			if (sp.order[3 * e + d] != sp.order[d]) mixed = true;
+	const char *force_mixed = std::getenv("H3DG_FORCE_MIXED");
+	if (force_mixed && force_mixed[0] == '1') mixed = true;
+	disc->reset_mixed();
+	if (mixed) {
+		if (h3dg::build_plan_mixed(sp, disc->qmode == H3DG_QUAD_P_PLUS, disc->qn, disc->plan, err) != 0)
+			return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
+	}
+	else if (h3dg::build_plan(sp, nq[0], nq[1], nq[2], disc->plan, err, canon) != 0)
+		return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
 	const h3dg::Plan &P = disc->plan;
 	disc->on_device = false;
 	disc->have_plan = true;
@@ -370,7 +408,18 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 	H3DG_CUDA_TRY(disc->el_vtx.upload(P.el_vtx));
 	H3DG_CUDA_TRY(disc->el_cnt.upload(P.el_cnt));
 	H3DG_CUDA_TRY(disc->el_id.upload(P.el_id));
-	if (P.canon) {
+	if (P.mixed) {
+		H3DG_CUDA_TRY(disc->el_desc.upload(P.el_desc));
+		H3DG_CUDA_TRY(disc->el_base.upload(P.el_base));
+		H3DG_CUDA_TRY(disc->el_obase.upload(P.el_obase));
+		H3DG_CUDA_TRY(disc->el_cdof.upload(P.el_cdof));
+		H3DG_CUDA_TRY(disc->el_ccoef.upload(P.el_ccoef));
+		H3DG_CUDA_TRY(disc->el_offm.upload(P.el_offm));
+		H3DG_CUDA_TRY(disc->mx_counters.alloc((size_t) P.ncolors * h3dg::Plan::kClasses));
+		disc->el_offc.release();
+		disc->el_offt.release();
+	}
+	else if (P.canon) {
 		H3DG_CUDA_TRY(disc->el_cdof.upload(P.el_cdof));
 		H3DG_CUDA_TRY(disc->el_ccoef.upload(P.el_ccoef));
 		H3DG_CUDA_TRY(disc->el_offc.upload(P.el_offc));
@@ -383,7 +432,8 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 		H3DG_CUDA_TRY(disc->el_off.upload(P.el_off));
 	}
 	std::vector<double> blob;
-	build_table_blob(P, blob);
+	if (P.mixed) blob = P.mixed_tables;
+	else build_table_blob(P, blob);
 	disc->table_bytes = (int) (blob.size() * sizeof(double));
 	H3DG_CUDA_TRY(disc->tables.upload(blob));
 	H3DG_CUDA_TRY(disc->qx.upload(P.qx));
@@ -482,10 +532,179 @@ static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, dou
 	return H3DG_OK;
 }
 
+// set while h3dg_disc_assemble_host_noalloc runs: the mixed path then
+// launches directly instead of instantiating a graph
+static thread_local bool t_mixed_direct = false;
+
+// Mixed orders: per colour, one launch per kernel class; the classes of a
+// colour touch disjoint entries and run as parallel branches, colours are
+// joined in order.  The whole assembly is captured once into a CUDA graph
+// (per output pointers) and replayed.
+static h3dg_status assemble_mixed(h3dg_disc *disc, double *d_Ax, double *d_rhs, cudaStream_t st) {
+	const h3dg::Plan &P = disc->plan;
+	constexpr int NC = h3dg::Plan::kClasses;
+	h3dg::KArgsMixed a;
+	a.xyz = disc->xyz.p;
+	a.el_vtx = disc->el_vtx.p;
+	a.el_id = disc->el_id.p;
+	a.ecoef = disc->coef.p;
+	a.el_desc = disc->el_desc.p;
+	a.el_base = disc->el_base.p;
+	a.el_obase = disc->el_obase.p;
+	a.cdof = disc->el_cdof.p;
+	a.ccoef = disc->el_ccoef.p;
+	a.offm = disc->el_offm.p;
+	a.Ap = disc->Ap.p;
+	a.tables = disc->tables.p;
+	a.table_bytes = disc->table_bytes;
+	a.mass = disc->bf == H3DG_BF_GRAD_GRAD_MASS;
+	a.lf = disc->lf;
+	a.lf_value = disc->lf_value;
+	a.Ax = d_Ax;
+	a.rhs = disc->lf ? d_rhs : nullptr;
+	a.status = disc->status.p;
+	a.counters = disc->mx_counters.p;
+	int nsm = 148;
+	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
+	auto prepare = [&](MixSpec &k, int &per_sm) -> h3dg_status {
+		const size_t smem = k.smem(disc->table_bytes);
+		if (!k.configured || k.configured_smem < smem) {
+			H3DG_CUDA_TRY(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+			k.configured = true;
+			k.configured_smem = smem;
+		}
+		per_sm = 1;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, smem);
+		if (per_sm < 1) per_sm = 1;
+		return H3DG_OK;
+	};
+	auto launch = [&](MixSpec &k, int per_sm, int c, int cls, cudaStream_t s) -> bool {
+		const int li = c * NC + cls;
+		const int64_t kb = P.launch_ptr[li], ke = P.launch_ptr[li + 1];
+		if (ke <= kb) return false;
+		const int64_t grid = std::min<int64_t>(ke - kb, (int64_t) nsm * per_sm);
+		k.fn<<<(unsigned) grid, k.threads, k.smem(disc->table_bytes), s>>>(a, kb, ke, li);
+		return true;
+	};
+	const size_t ncnt = sizeof(unsigned) * (size_t) P.ncolors * NC;
+	// variants: time each class's launches once per plan, keep the fastest
+	if (disc->mx_variant[0] < 0) {
+		cudaEvent_t e0, e1;
+		H3DG_CUDA_TRY(cudaEventCreate(&e0));
+		H3DG_CUDA_TRY(cudaEventCreate(&e1));
+		for (int cls = 0; cls < NC; cls++) {
+			float best = 1e30f;
+			int besti = -1;
+			for (size_t vi = 0; vi < mix_table().size(); vi++) {
+				MixSpec &k = mix_table()[vi];
+				if (k.cls != cls) continue;
+				int per_sm;
+				if (prepare(k, per_sm) != H3DG_OK) return H3DG_ERR_CUDA;
+				if (besti < 0) besti = (int) vi;
+				float tot = 0.0f;
+				for (int rep = 0; rep < 2; rep++) {
+					H3DG_CUDA_TRY(cudaMemsetAsync(disc->mx_counters.p, 0, ncnt, st));
+					H3DG_CUDA_TRY(cudaEventRecord(e0, st));
+					for (int c = 0; c < P.ncolors; c++) launch(k, per_sm, c, cls, st);
+					H3DG_CUDA_TRY(cudaEventRecord(e1, st));
+					H3DG_CUDA_TRY(cudaEventSynchronize(e1));
+					float ms = 0.0f;
+					H3DG_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+					if (rep) tot += ms;
+				}
+				if (tot < best) { best = tot; besti = (int) vi; }
+			}
+			disc->mx_variant[cls] = besti;
+		}
+		cudaEventDestroy(e0);
+		cudaEventDestroy(e1);
+		H3DG_CUDA_TRY(cudaGetLastError());
+	}
+	int per_sm[NC];
+	for (int cls = 0; cls < NC; cls++)
+		if (prepare(mix_table()[disc->mx_variant[cls]], per_sm[cls]) != H3DG_OK) return H3DG_ERR_CUDA;
+	// the whole assembly, on s0 with the classes 1, 2 of each colour forked to s1, s2
+	auto enqueue = [&](cudaStream_t s0, cudaStream_t s1, cudaStream_t s2, bool fork) -> h3dg_status {
+		int32_t n = 0;
+		if (d_Ax) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, s0));
+		if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, s0));
+		H3DG_CUDA_TRY(cudaMemsetAsync(disc->mx_counters.p, 0, ncnt, s0));
+		for (int c = 0; c < P.ncolors; c++) {
+			if (fork) {
+				H3DG_CUDA_TRY(cudaEventRecord(disc->mx_ev[0], s0));
+				H3DG_CUDA_TRY(cudaStreamWaitEvent(s1, disc->mx_ev[0], 0));
+				H3DG_CUDA_TRY(cudaStreamWaitEvent(s2, disc->mx_ev[0], 0));
+			}
+			cudaStream_t ss[NC] = { s0, s1, s2 };
+			for (int cls = 0; cls < NC; cls++)
+				if (launch(mix_table()[disc->mx_variant[cls]], per_sm[cls], c, cls, ss[cls])) n++;
+			if (fork) {
+				H3DG_CUDA_TRY(cudaEventRecord(disc->mx_ev[1], s1));
+				H3DG_CUDA_TRY(cudaEventRecord(disc->mx_ev[2], s2));
+				H3DG_CUDA_TRY(cudaStreamWaitEvent(s0, disc->mx_ev[1], 0));
+				H3DG_CUDA_TRY(cudaStreamWaitEvent(s0, disc->mx_ev[2], 0));
+			}
+		}
+		H3DG_CUDA_TRY(cudaGetLastError());
+		disc->mx_launches = n;
+		return H3DG_OK;
+	};
+	const bool rec = disc->tn < disc->tcap;
+	if (t_mixed_direct) {
+		if (rec) H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn], st));
+		h3dg_status s = enqueue(st, st, st, false);
+		if (s != H3DG_OK) return s;
+	}
+	else {
+		if (!disc->mx_exec || disc->mx_ax != d_Ax || disc->mx_rhs != d_rhs) {
+			if (disc->mx_exec) cudaGraphExecDestroy(disc->mx_exec);
+			disc->mx_exec = nullptr;
+			for (auto &s : disc->mx_s)
+				if (!s) H3DG_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+			for (auto &e : disc->mx_ev)
+				if (!e) H3DG_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+			cudaStream_t cap;
+			H3DG_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+			cudaGraph_t g = nullptr;
+			H3DG_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+			h3dg_status s = enqueue(cap, disc->mx_s[0], disc->mx_s[1], true);
+			cudaError_t e = cudaStreamEndCapture(cap, &g);
+			cudaStreamDestroy(cap);
+			if (s != H3DG_OK) {
+				if (g) cudaGraphDestroy(g);
+				return s;
+			}
+			if (e != cudaSuccess) return fail(H3DG_ERR_CUDA, std::string("assemble: graph capture: ") + cudaGetErrorString(e));
+			e = cudaGraphInstantiate(&disc->mx_exec, g, 0);
+			cudaGraphDestroy(g);
+			if (e != cudaSuccess) {
+				disc->mx_exec = nullptr;
+				return fail(H3DG_ERR_CUDA, std::string("assemble: graph instantiate: ") + cudaGetErrorString(e));
+			}
+			disc->mx_ax = d_Ax;
+			disc->mx_rhs = d_rhs;
+		}
+		if (rec) H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn], st));
+		H3DG_CUDA_TRY(cudaGraphLaunch(disc->mx_exec, st));
+	}
+	if (rec) {
+		H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn + 1], st));
+		disc->tn++;
+	}
+	disc->last_launches = disc->mx_launches;
+	return H3DG_OK;
+}
+
 h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream) {
 	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "assemble: create_pattern() first");
 	if (precision != H3DG_PREC_FP64 && precision != H3DG_PREC_TF32X3) return fail(H3DG_ERR_INVALID_ARG, "assemble: unknown precision");
 	const h3dg::Plan &P = disc->plan;
+	if (P.mixed) {
+		h3dg_status s0 = ensure_device(disc);
+		if (s0 != H3DG_OK) return s0;
+		H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+		return assemble_mixed(disc, d_Ax, d_rhs, (cudaStream_t) stream);
+	}
 	if (P.px != P.py || P.px != P.pz || P.nqx != P.nqy || P.nqx != P.nqz)
 		return fail(H3DG_ERR_INVALID_ARG, "assemble: anisotropic orders need the batched path");
 	if (P.canon) {
@@ -607,6 +826,7 @@ h3dg_status h3dg_disc_adjoint(h3dg_disc *disc, int nfields, const double *d_logc
 	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "adjoint: create_pattern() first");
 	if (nfields < 1 || !d_u || !d_lambda) return fail(H3DG_ERR_INVALID_ARG, "adjoint: bad arguments");
 	const h3dg::Plan &P = disc->plan;
+	if (P.mixed) return fail(H3DG_ERR_INVALID_ARG, "adjoint: not available for mixed-order plans");
 	if (P.px != P.py || P.px != P.pz || P.nqx != P.nqy || P.nqx != P.nqz)
 		return fail(H3DG_ERR_INVALID_ARG, "adjoint: anisotropic orders need the batched path");
 	AdjSpec *k = nullptr;
@@ -769,6 +989,9 @@ h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, doub
 	if (P.canon && precision == H3DG_PREC_TF32X3 && Ax && !disc->el_offt.p && P.ne > 0)
 		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: split-precision scatter stream not built; make one allocating "
 		                            "split-precision assembly call first");
+	if (P.mixed && disc->mx_variant[0] < 0)
+		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: kernel variants not tuned yet; make one allocating assembly "
+		                            "call first");
 	if (!P.canon && disc->variant < 0) {
 		int ncand = 0;
 		for (size_t i = 0; i < kernel_table().size(); i++)
@@ -783,7 +1006,9 @@ h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, doub
 	if (s0 != H3DG_OK) return s0;
 	double *d_Ax = Ax ? scratch : nullptr;
 	double *d_rhs = rhs ? scratch + rhs_off : nullptr;
+	t_mixed_direct = true;
 	h3dg_status s = h3dg_disc_assemble(disc, precision, d_Ax, d_rhs, nullptr);   // zeroes its outputs first
+	t_mixed_direct = false;
 	if (s != H3DG_OK) return s;
 	if (Ax) H3DG_CUDA_TRY(cudaMemcpy(Ax, d_Ax, sizeof(double) * P.nnz, cudaMemcpyDeviceToHost));
 	if (rhs) H3DG_CUDA_TRY(cudaMemcpy(rhs, d_rhs, sizeof(double) * P.ndof, cudaMemcpyDeviceToHost));
@@ -826,6 +1051,7 @@ h3dg_status h3dg_disc_last_launch_count(const h3dg_disc *disc, int32_t *count) {
 h3dg_status h3dg_disc_geometry(h3dg_disc *disc, double *d_jac, double *d_irm, double *d_xyz, void *stream) {
 	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "geometry: create_pattern() first");
 	const h3dg::Plan &P = disc->plan;
+	if (P.mixed) return fail(H3DG_ERR_INVALID_ARG, "geometry: one rule per plan needed (mixed-order plan)");
 	{ h3dg_status s0 = ensure_device(disc); if (s0 != H3DG_OK) return s0; }
 	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
 	h3dg::GeomArgs g;

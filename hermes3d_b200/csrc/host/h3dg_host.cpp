@@ -754,4 +754,230 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 	return 0;
 }
 
+// Mixed orders.  Same pattern rule as build_plan (the CSC pattern does not
+// depend on how the elements are grouped); the per-element tables are
+// variable-length, indexed by prefix bases.
+int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string &err) {
+	if (!sp.assigned) { err = "assign_dofs() has not been called"; return -1; }
+	const Mesh &m = *sp.mesh;
+	const int64_t ne = m.ne();
+	P = Plan();
+	P.ne = ne;
+	P.ndof = sp.ndof();
+	P.mixed = true;
+	P.canon = true;
+	P.px = P.py = P.pz = -1;
+	P.nqx = P.nqy = P.nqz = -1;
+
+	// orders, rules, table sets, kernel class
+	std::vector<int64_t> eb(ne + 1, 0);
+	std::vector<std::array<int, 11>> desc(ne);
+	std::vector<std::pair<int, int>> set_key;
+	std::vector<int> set_off;
+	auto table_set = [&](int p, int nq) -> int {
+		for (size_t t = 0; t < set_key.size(); t++)
+			if (set_key[t].first == p && set_key[t].second == nq) return set_off[t];
+		int off = (int) P.mixed_tables.size();
+		std::vector<double> q, w;
+		gauss_legendre(nq, q, w);
+		for (int k = 0; k <= p; k++)
+			for (int i = 0; i < nq; i++) P.mixed_tables.push_back(lobatto_value(k, q[i]));
+		for (int k = 0; k <= p; k++)
+			for (int i = 0; i < nq; i++) P.mixed_tables.push_back(lobatto_deriv(k, q[i]));
+		P.mixed_tables.insert(P.mixed_tables.end(), q.begin(), q.end());
+		P.mixed_tables.insert(P.mixed_tables.end(), w.begin(), w.end());
+		if (P.mixed_tables.size() % 2) P.mixed_tables.push_back(0.0);
+		set_key.push_back({ p, nq });
+		set_off.push_back(off);
+		return off;
+	};
+	for (int64_t e = 0; e < ne; e++) {
+		auto &d = desc[e];
+		int nl = 1, pmax = 0, qmax = 0;
+		for (int r = 0; r < 3; r++) {
+			const int p = sp.order[3 * e + r];
+			const int nq = p_plus ? p + qn : qn;
+			if (p < 1 || p > 10) { err = "element order out of range"; return -1; }
+			if (nq < 1 || nq > kMaxQuadPoints) { err = "Gauss points per direction must be in 1..13"; return -1; }
+			d[r] = p;
+			d[3 + r] = nq;
+			d[6 + r] = table_set(p, nq);
+			nl *= p + 1;
+			pmax = std::max(pmax, p);
+			qmax = std::max(qmax, nq);
+		}
+		d[9] = nl;
+		int cls = -1;
+		for (int c = 0; c < Plan::kClasses && cls < 0; c++)
+			if (pmax <= Plan::kClassP[c] && qmax <= Plan::kClassQ[c]) cls = c;
+		if (cls < 0) { err = "mixed-order kernels cover orders <= 6 and <= 8 points per direction"; return -1; }
+		d[10] = cls;
+		eb[e + 1] = eb[e] + nl;
+		P.max_nl = std::max(P.max_nl, nl);
+	}
+
+	// assembly lists
+	std::vector<int32_t> cnt(2 * ne), dofs(eb[ne], -1);
+	std::vector<uint16_t> ss(eb[ne], 0);
+	std::vector<double> cf(eb[ne], 0.0);
+	std::vector<int> bad(ne, 0);
+	parallel_for(ne, [&](int64_t lo, int64_t hi) {
+		std::vector<AsmEntry> al;
+		std::vector<char> seen;
+		for (int64_t e = lo; e < hi; e++) {
+			const int nl = desc[e][9], py = desc[e][1], pz = desc[e][2];
+			sp.element_assembly_list(e, al);
+			int mcount = 0, lcount = 0;
+			for (auto &a : al) (a.dof >= 0 ? mcount : lcount)++;
+			if (mcount + lcount > nl) { bad[e] = 1; continue; }
+			int im = 0, il = mcount;
+			seen.assign(nl, 0);
+			for (auto &a : al) {
+				Canon c = decode_index(a.idx);
+				int sidx = (c.a * (py + 1) + c.b) * (pz + 1) + c.c;
+				if (sidx < 0 || sidx >= nl || seen[sidx]) { bad[e] = 3; break; }
+				seen[sidx] = 1;
+				int k = a.dof >= 0 ? im++ : il++;
+				ss[eb[e] + k] = (uint16_t) sidx;
+				dofs[eb[e] + k] = a.dof >= 0 ? a.dof : DIRICHLET_DOF;
+				cf[eb[e] + k] = c.sign * a.coef;
+			}
+			cnt[2 * e] = mcount;
+			cnt[2 * e + 1] = lcount;
+		}
+	});
+	for (int64_t e = 0; e < ne; e++)
+		if (bad[e]) {
+			err = bad[e] == 1 ? "assembly list longer than the element basis" : "a canonical function repeats in one assembly list (constrained space)";
+			return -1;
+		}
+
+	// DOF -> elements adjacency, CSC pattern (as build_plan)
+	const int64_t nd = P.ndof;
+	std::vector<int64_t> dptr(nd + 1, 0);
+	for (int64_t e = 0; e < ne; e++)
+		for (int k = 0; k < cnt[2 * e]; k++) dptr[dofs[eb[e] + k] + 1]++;
+	for (int64_t d = 0; d < nd; d++) dptr[d + 1] += dptr[d];
+	std::vector<int32_t> dadj(dptr[nd]);
+	{
+		std::vector<int64_t> fill(dptr.begin(), dptr.end() - 1);
+		for (int64_t e = 0; e < ne; e++)
+			for (int k = 0; k < cnt[2 * e]; k++) dadj[fill[dofs[eb[e] + k]]++] = (int32_t) e;
+	}
+	std::vector<int64_t> collen(nd, 0);
+	auto column = [&](int64_t d, std::vector<int32_t> &buf) {
+		buf.clear();
+		for (int64_t k = dptr[d]; k < dptr[d + 1]; k++) {
+			int64_t e = dadj[k];
+			for (int j = 0; j < cnt[2 * e]; j++) buf.push_back(dofs[eb[e] + j]);
+		}
+		std::sort(buf.begin(), buf.end());
+		buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+	};
+	parallel_for(nd, [&](int64_t lo, int64_t hi) {
+		std::vector<int32_t> buf;
+		for (int64_t d = lo; d < hi; d++) { column(d, buf); collen[d] = (int64_t) buf.size(); }
+	});
+	P.Ap.assign(nd + 1, 0);
+	for (int64_t d = 0; d < nd; d++) P.Ap[d + 1] = P.Ap[d] + collen[d];
+	P.nnz = P.Ap[nd];
+	P.Ai.resize(P.nnz);
+	int64_t maxcol = 0;
+	for (int64_t d = 0; d < nd; d++) maxcol = std::max(maxcol, collen[d]);
+	if (maxcol > 65535) { err = "a column holds more than 65535 rows"; return -1; }
+	parallel_for(nd, [&](int64_t lo, int64_t hi) {
+		std::vector<int32_t> buf;
+		for (int64_t d = lo; d < hi; d++) {
+			column(d, buf);
+			std::copy(buf.begin(), buf.end(), P.Ai.begin() + P.Ap[d]);
+		}
+	});
+
+	// greedy colouring in element order
+	std::vector<int> color(ne, -1);
+	int ncol = 0;
+	{
+		std::vector<int64_t> stamp(64, -1);
+		for (int64_t e = 0; e < ne; e++) {
+			for (int k = 0; k < cnt[2 * e]; k++) {
+				int d = dofs[eb[e] + k];
+				for (int64_t t = dptr[d]; t < dptr[d + 1]; t++) {
+					int64_t o = dadj[t];
+					if (o < e && color[o] >= 0) {
+						if (color[o] >= (int) stamp.size()) stamp.resize(color[o] + 1, -1);
+						stamp[color[o]] = e;
+					}
+				}
+			}
+			int c = 0;
+			while (c < (int) stamp.size() && stamp[c] == e) c++;
+			color[e] = c;
+			ncol = std::max(ncol, c + 1);
+			if (c + 1 > (int) stamp.size()) stamp.resize(c + 1, -1);
+		}
+	}
+	P.ncolors = ncol;
+
+	// order: colour, class, decreasing work (nl^2 * points), element id
+	std::vector<int64_t> order_(ne);
+	for (int64_t e = 0; e < ne; e++) order_[e] = e;
+	auto work = [&](int64_t e) { return (int64_t) desc[e][9] * desc[e][9] * desc[e][3]; };
+	std::sort(order_.begin(), order_.end(), [&](int64_t x, int64_t y) {
+		if (color[x] != color[y]) return color[x] < color[y];
+		if (desc[x][10] != desc[y][10]) return desc[x][10] < desc[y][10];
+		int64_t wx = work(x), wy = work(y);
+		if (wx != wy) return wx > wy;
+		return x < y;
+	});
+	P.launch_ptr.assign((size_t) ncol * Plan::kClasses + 1, 0);
+	for (int64_t e = 0; e < ne; e++) P.launch_ptr[(size_t) color[e] * Plan::kClasses + desc[e][10] + 1]++;
+	for (size_t i = 0; i + 1 < P.launch_ptr.size(); i++) P.launch_ptr[i + 1] += P.launch_ptr[i];
+	P.color_ptr.assign(ncol + 1, 0);
+	for (int c = 0; c <= ncol; c++) P.color_ptr[c] = P.launch_ptr[(size_t) c * Plan::kClasses];
+
+	// per-element tables in assembly order
+	P.el_base.assign(ne + 1, 0);
+	P.el_obase.assign(ne + 1, 0);
+	for (int64_t k = 0; k < ne; k++) {
+		const int nl = desc[order_[k]][9];
+		P.el_base[k + 1] = P.el_base[k] + nl;
+		P.el_obase[k + 1] = P.el_obase[k] + (int64_t) nl * nl;
+	}
+	P.el_vtx.resize(8 * ne);
+	P.el_id.resize(ne);
+	P.el_cnt.resize(2 * ne);
+	P.el_desc.assign((size_t) ne * Plan::kDescInts, 0);
+	P.el_cdof.assign(P.el_base[ne], -1);
+	P.el_ccoef.assign(P.el_base[ne], 0.0);
+	P.el_offm.assign(P.el_obase[ne], 0);
+	parallel_for(ne, [&](int64_t lo, int64_t hi) {
+		for (int64_t k = lo; k < hi; k++) {
+			const int64_t e = order_[k];
+			const int nl = desc[e][9];
+			P.el_id[k] = (int32_t) e;
+			for (int v = 0; v < 8; v++) P.el_vtx[8 * k + v] = (int32_t) m.hex[8 * e + v];
+			for (int t = 0; t < 11; t++) P.el_desc[(size_t) k * Plan::kDescInts + t] = desc[e][t];
+			P.el_cnt[2 * k] = cnt[2 * e];
+			P.el_cnt[2 * k + 1] = cnt[2 * e + 1];
+			const int64_t cb = P.el_base[k], ob = P.el_obase[k];
+			for (int t = 0; t < cnt[2 * e] + cnt[2 * e + 1]; t++) {
+				const int sidx = ss[eb[e] + t];
+				P.el_cdof[cb + sidx] = dofs[eb[e] + t];
+				P.el_ccoef[cb + sidx] = cf[eb[e] + t];
+			}
+			const int mc = cnt[2 * e];
+			for (int b = 0; b < mc; b++) {
+				const int col = dofs[eb[e] + b], sj = ss[eb[e] + b];
+				const int32_t *c0 = &P.Ai[P.Ap[col]], *c1 = &P.Ai[P.Ap[col + 1]];
+				for (int a = 0; a < mc; a++) {
+					const int row = dofs[eb[e] + a], si = ss[eb[e] + a];
+					const int32_t *pos = std::lower_bound(c0, c1, row);
+					P.el_offm[ob + (int64_t) sj * nl + si] = (uint16_t) (pos - c0);
+				}
+			}
+		}
+	});
+	return 0;
+}
+
 } // namespace h3dg

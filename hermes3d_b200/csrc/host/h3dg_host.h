@@ -141,8 +141,30 @@ struct Plan {
 
 	// 1D tables (b): per direction, V[k][q] and D[k][q] (k <= p, q < nq) and rule
 	std::vector<double> qx, wx, qy, wy, qz, wz;
+
+	// mixed orders (batched path): every element has its own order triple and
+	// rule.  Canonical tables with per-element bases; el_offm is [j][i]
+	// (column-major: for one trial function j the rows i are contiguous).
+	bool mixed = false;
+	static constexpr int kClasses = 3;       // kernel classes by (max order, max points)
+	static constexpr int kClassP[kClasses] = { 2, 4, 6 };
+	static constexpr int kClassQ[kClasses] = { 4, 6, 8 };
+	static constexpr int kDescInts = 12;     // px py pz nqx nqy nqz ox oy oz nl class -
+	std::vector<int32_t> el_desc;            // ne x kDescInts (assembly order); o*: offsets (doubles) of the
+	                                         // direction's table set in mixed_tables
+	std::vector<int64_t> el_base;            // ne + 1: element k's nl entries of el_cdof / el_ccoef start here
+	std::vector<int64_t> el_obase;           // ne + 1: element k's nl * nl entries of el_offm start here
+	std::vector<uint16_t> el_offm;           // [j][i] row position of cdof_i in column cdof_j
+	std::vector<double> mixed_tables;        // per (p, nq) set: V[(p+1) nq], D[(p+1) nq], q[nq], w[nq]
+	std::vector<int64_t> launch_ptr;         // ncolors * kClasses + 1: (colour, class) ranges, assembly order
+	int max_nl = 0;
 };
 
 int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &plan, std::string &err, bool canon = false);
+
+// Mixed orders: per element p_d + qn points per direction (p_plus) or qn
+// (fixed).  Elements are grouped by colour, then by kernel class, and within
+// a (colour, class) range ordered by decreasing work.
+int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &plan, std::string &err);
 
 } // namespace h3dg

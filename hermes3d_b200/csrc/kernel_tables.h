@@ -13,6 +13,7 @@
 #include "kernels/common.cuh"
 #include "kernels/asm_fp64_ho.cuh"
 #include "kernels/adjoint.cuh"
+#include "kernels/asm_fp64_mixed.cuh"
 
 namespace h3dg_tables {
 
@@ -45,6 +46,17 @@ struct AdjSpec {
 	bool configured;
 };
 
+using MixFn = void (*)(h3dg::KArgsMixed, int64_t, int64_t, int);
+
+struct MixSpec {
+	int cls;                      // kernel class (Plan::kClassP / kClassQ)
+	MixFn fn;
+	int threads;
+	size_t (*smem)(int table_bytes);
+	bool configured;
+	size_t configured_smem;
+};
+
 // FP64 low-order kernels (register / shared-memory element matrix); the
 // autotuner times each candidate for an (order, points) pair on the actual
 // plan at the first assembly and keeps the fastest.
@@ -56,6 +68,8 @@ std::vector<HoSpec> &ho_tc_table();
 // tensor-core scatter stream from the canonical position map (async on st)
 cudaError_t build_offt(const uint16_t *offc, const int32_t *cdof, const int64_t *Ap, int64_t ne, int px, int nq,
                        uint16_t **offt, size_t *count, int *status, cudaStream_t st);
+// mixed-order kernels, several variants per class (timed once per plan)
+std::vector<MixSpec> &mix_table();
 // adjoint (element sensitivity) kernels
 std::vector<AdjSpec> &adj_table();
 

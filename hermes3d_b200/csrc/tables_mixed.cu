@@ -1,0 +1,21 @@
+// Kernel variant table (see kernel_tables.h).
+#include "kernel_tables.h"
+
+namespace h3dg_tables {
+
+template <int CLS, int PM, int QM, int NT, int MINB>
+static MixSpec mix_spec() {
+	return MixSpec { CLS, &h3dg::k_assemble_fp64_mixed<PM, QM, NT, MINB>, NT, &h3dg::MixShape<PM, QM>::smem_bytes, false, 0 };
+}
+
+// classes: (orders <= 2, <= 4 points), (<= 4, <= 6), (<= 6, <= 8)
+std::vector<MixSpec> &mix_table() {
+	static std::vector<MixSpec> t = {
+		mix_spec<0, 2, 4, 64, 8>(), mix_spec<0, 2, 4, 128, 4>(),
+		mix_spec<1, 4, 6, 128, 3>(), mix_spec<1, 4, 6, 256, 1>(),
+		mix_spec<2, 6, 8, 128, 2>(), mix_spec<2, 6, 8, 256, 1>(),
+	};
+	return t;
+}
+
+} // namespace h3dg_tables

@@ -21,8 +21,21 @@ def test_dof_count_and_assembly_lists(name):
         assert np.allclose(coef, g["al_coef"][a:b], rtol=1e-12, atol=1e-12), e
 
 
-@pytest.mark.parametrize("name", [n for n in golden_names() if not n.startswith("aniso")])
+@pytest.mark.parametrize("name", golden_names())
 def test_pattern_bit_exact(name):
+    g = load(name)
+    sp = space_of(g)
+    d = disc_of(g, sp)
+    M = h.UMFPackMatrix()
+    d.create(M, h.UMFPackVector())
+    assert np.array_equal(M.Ap, g["Ap"])
+    assert np.array_equal(M.Ai, g["Ai"])
+
+
+@pytest.mark.parametrize("name", ["c1_small", "perm_p2_lifting", "perm_p4_natural"])
+def test_mixed_plan_pattern_bit_exact(name, monkeypatch):
+    """Uniform spaces routed through the mixed-order plan give the same pattern."""
+    monkeypatch.setenv("H3DG_FORCE_MIXED", "1")
     g = load(name)
     sp = space_of(g)
     d = disc_of(g, sp)
