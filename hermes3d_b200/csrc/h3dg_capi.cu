@@ -76,6 +76,8 @@ struct h3dg_disc {
 	int qmode = H3DG_QUAD_FIXED, qn = 0;
 	bool have_plan = false;
 	bool on_device = false;
+	int nparts = 1, part = 0;  // z-slab partition of the next plan (1: whole mesh)
+	h3dg::PlanScope scope;     // element subset and owned DOFs of the current plan's part
 	int variant = -1;          // autotuned kernel variant (index into the kernel table)
 	float variant_ms = 0.0f;
 	h3dg::Plan plan;
@@ -380,11 +382,18 @@ h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nn
 	const char *force_mixed = std::getenv("H3DG_FORCE_MIXED");
 	if (force_mixed && force_mixed[0] == '1') mixed = true;
 	disc->reset_mixed();
+	const h3dg::PlanScope *scope = nullptr;
+	disc->scope = h3dg::PlanScope();
+	if (disc->nparts > 1) {
+		if (h3dg::make_partition_scope(sp, disc->nparts, disc->part, disc->scope, err) != 0)
+			return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
+		scope = &disc->scope;
+	}
 	if (mixed) {
-		if (h3dg::build_plan_mixed(sp, disc->qmode == H3DG_QUAD_P_PLUS, disc->qn, disc->plan, err) != 0)
+		if (h3dg::build_plan_mixed(sp, disc->qmode == H3DG_QUAD_P_PLUS, disc->qn, disc->plan, err, scope) != 0)
 			return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
 	}
-	else if (h3dg::build_plan(sp, nq[0], nq[1], nq[2], disc->plan, err, canon) != 0)
+	else if (h3dg::build_plan(sp, nq[0], nq[1], nq[2], disc->plan, err, canon, scope) != 0)
 		return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
 	const h3dg::Plan &P = disc->plan;
 	disc->on_device = false;
@@ -444,6 +453,41 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 	H3DG_CUDA_TRY(disc->status.alloc(1));
 	H3DG_CUDA_TRY(cudaMemset(disc->status.p, 0, sizeof(int)));
 	disc->on_device = true;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_set_partition(h3dg_disc *disc, int nparts, int part) {
+	if (!disc || nparts < 1 || part < 0 || part >= nparts) return fail(H3DG_ERR_INVALID_ARG, "set_partition: need 0 <= part < nparts");
+	disc->nparts = nparts;
+	disc->part = part;
+	disc->have_plan = false;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_get_partition(const h3dg_disc *disc, uint8_t *owned, int64_t *nslab, int64_t *nhalo, int64_t *nowned) {
+	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "get_partition: create_pattern() first");
+	const int64_t nd = disc->plan.ndof;
+	const bool whole = disc->nparts <= 1;
+	if (owned) {
+		if (whole) std::memset(owned, 1, (size_t) nd);
+		else
+			for (int64_t d = 0; d < nd; d++) owned[d] = (uint8_t) disc->scope.owned[d];
+	}
+	if (nslab) *nslab = whole ? disc->plan.ne : disc->scope.nslab;
+	if (nhalo) *nhalo = whole ? 0 : disc->scope.nhalo;
+	if (nowned) *nowned = whole ? nd : disc->scope.nowned;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_get_partition_elements(const h3dg_disc *disc, uint8_t *in_part, int64_t ne) {
+	if (!disc || !disc->have_plan || !in_part) return fail(H3DG_ERR_STATE, "get_partition_elements: create_pattern() first");
+	if (ne != disc->space->s.mesh->ne()) return fail(H3DG_ERR_INVALID_ARG, "get_partition_elements: ne must be the mesh's element count");
+	if (disc->nparts <= 1) {
+		std::memset(in_part, 1, (size_t) ne);
+		return H3DG_OK;
+	}
+	std::memset(in_part, 0, (size_t) ne);
+	for (int64_t e : disc->scope.elems) in_part[e] = 1;
 	return H3DG_OK;
 }
 

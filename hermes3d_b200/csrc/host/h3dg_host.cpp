@@ -535,6 +535,66 @@ static void parallel_for(int64_t n, F f) {
 	for (auto &t : th) t.join();
 }
 
+// z-slab partition (multi-GPU sharding, no communication on the data path).
+// Slabs: the elements ordered by centroid (z, then y, then x, then index),
+// cut into nparts contiguous ranges of equal count.  Owner of a DOF: the
+// part of the lowest-numbered element whose assembly list holds it as a
+// matrix entry.  Halo: elements outside the slab that hold an owned DOF.
+int make_partition_scope(const Space &sp, int nparts, int part, PlanScope &S, std::string &err) {
+	if (!sp.assigned) { err = "assign_dofs() has not been called"; return -1; }
+	if (nparts < 1 || part < 0 || part >= nparts) { err = "partition: need 0 <= part < nparts"; return -1; }
+	const Mesh &m = *sp.mesh;
+	const int64_t ne = m.ne(), nd = sp.ndof();
+	std::vector<std::array<double, 3>> cen(ne);
+	for (int64_t e = 0; e < ne; e++) {
+		double c[3] = { 0, 0, 0 };
+		for (int v = 0; v < 8; v++)
+			for (int r = 0; r < 3; r++) c[r] += m.xyz[3 * m.hex[8 * e + v] + r];
+		cen[e] = { c[0] / 8, c[1] / 8, c[2] / 8 };
+	}
+	std::vector<int64_t> ord(ne);
+	for (int64_t e = 0; e < ne; e++) ord[e] = e;
+	std::sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) {
+		if (cen[a][2] != cen[b][2]) return cen[a][2] < cen[b][2];
+		if (cen[a][1] != cen[b][1]) return cen[a][1] < cen[b][1];
+		if (cen[a][0] != cen[b][0]) return cen[a][0] < cen[b][0];
+		return a < b;
+	});
+	std::vector<int> epart(ne);
+	for (int64_t r = 0; r < ne; r++) epart[ord[r]] = (int) ((r * nparts) / std::max<int64_t>(ne, 1));
+	std::vector<int64_t> first(nd, -1);
+	std::vector<std::vector<int32_t>> edofs(ne);
+	parallel_for(ne, [&](int64_t lo, int64_t hi) {
+		std::vector<AsmEntry> al;
+		for (int64_t e = lo; e < hi; e++) {
+			sp.element_assembly_list(e, al);
+			for (auto &a : al)
+				if (a.dof >= 0) edofs[e].push_back(a.dof);
+		}
+	});
+	for (int64_t e = 0; e < ne; e++)
+		for (int32_t d : edofs[e])
+			if (first[d] < 0) first[d] = e;
+	S = PlanScope();
+	S.owned.assign(nd, 0);
+	for (int64_t d = 0; d < nd; d++)
+		if (first[d] >= 0 && epart[first[d]] == part) {
+			S.owned[d] = 1;
+			S.nowned++;
+		}
+	for (int64_t e = 0; e < ne; e++) {
+		bool take = epart[e] == part;
+		if (take) S.nslab++;
+		else {
+			for (int32_t d : edofs[e])
+				if (S.owned[d]) { take = true; break; }
+			if (take) S.nhalo++;
+		}
+		if (take) S.elems.push_back(e);
+	}
+	return 0;
+}
+
 // Discretization::create (src/discretization.cc:164-230) + SparseMatrix
 // pre_add_ij / sort_and_store_indices (src/matrix.cc:156-189) +
 // UMFPackMatrix::alloc (src/linsolver/umfpack.cc:46-71): per column (trial
@@ -542,16 +602,19 @@ static void parallel_for(int64_t n, F f) {
 // holds both.  Built here column by column from the DOF -> element adjacency
 // instead of page lists.  Also produces the per-element tables, the
 // row-position map used by the scatter and an element colouring.
-int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string &err, bool canon) {
+
+int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string &err, bool canon,
+               const PlanScope *scope) {
 	if (!sp.assigned) { err = "assign_dofs() has not been called"; return -1; }
 	const Mesh &m = *sp.mesh;
-	int64_t ne = m.ne();
+	const int64_t ne = scope ? (int64_t) scope->elems.size() : m.ne();
+	auto G = [&](int64_t e) -> int64_t { return scope ? scope->elems[e] : e; };   // plan element -> mesh element
 	P = Plan();
 	P.ne = ne;
 	P.ndof = sp.ndof();
 	P.px = sp.order[0]; P.py = sp.order[1]; P.pz = sp.order[2];
 	for (int64_t e = 0; e < ne; e++)
-		if (sp.order[3 * e] != P.px || sp.order[3 * e + 1] != P.py || sp.order[3 * e + 2] != P.pz) {
+		if (sp.order[3 * G(e)] != P.px || sp.order[3 * G(e) + 1] != P.py || sp.order[3 * G(e) + 2] != P.pz) {
 			err = "plan requires one element order triple; bucket mixed orders first";
 			return -1;
 		}
@@ -575,7 +638,7 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 	parallel_for(ne, [&](int64_t lo, int64_t hi) {
 		std::vector<AsmEntry> al;
 		for (int64_t e = lo; e < hi; e++) {
-			sp.element_assembly_list(e, al);
+			sp.element_assembly_list(G(e), al);
 			int mcount = 0, lcount = 0;
 			for (auto &a : al) (a.dof >= 0 ? mcount : lcount)++;
 			if (mcount + lcount > nl) { bad[e] = 1; continue; }
@@ -616,6 +679,7 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 	std::vector<int64_t> collen(nd, 0);
 	auto column = [&](int64_t d, std::vector<int32_t> &buf) {
 		buf.clear();
+		if (scope && !scope->owned[d]) return;                     // another part's column
 		for (int64_t k = dptr[d]; k < dptr[d + 1]; k++) {
 			int64_t e = dadj[k];
 			for (int j = 0; j < cnt[2 * e]; j++) buf.push_back(dofs[(size_t) e * nl + j]);
@@ -697,8 +761,8 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 		parallel_for(ne, [&](int64_t lo, int64_t hi) {
 			for (int64_t k = lo; k < hi; k++) {
 				int64_t e = order_[k];
-				P.el_id[k] = (int32_t) e;
-				for (int v = 0; v < 8; v++) P.el_vtx[8 * k + v] = (int32_t) m.hex[8 * e + v];
+				P.el_id[k] = (int32_t) G(e);
+				for (int v = 0; v < 8; v++) P.el_vtx[8 * k + v] = (int32_t) m.hex[8 * G(e) + v];
 				P.el_cnt[2 * k] = cnt[2 * e];
 				P.el_cnt[2 * k + 1] = cnt[2 * e + 1];
 				for (int t = 0; t < cnt[2 * e] + cnt[2 * e + 1]; t++) {
@@ -732,8 +796,8 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 	parallel_for(ne, [&](int64_t lo, int64_t hi) {
 		for (int64_t k = lo; k < hi; k++) {
 			int64_t e = order_[k];
-			P.el_id[k] = (int32_t) e;
-			for (int v = 0; v < 8; v++) P.el_vtx[8 * k + v] = (int32_t) m.hex[8 * e + v];
+			P.el_id[k] = (int32_t) G(e);
+			for (int v = 0; v < 8; v++) P.el_vtx[8 * k + v] = (int32_t) m.hex[8 * G(e) + v];
 			P.el_cnt[2 * k] = cnt[2 * e];
 			P.el_cnt[2 * k + 1] = cnt[2 * e + 1];
 			std::copy(&ss[(size_t) e * nl], &ss[(size_t) e * nl] + nl, &P.el_s[(size_t) k * nl]);
@@ -757,10 +821,11 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 // Mixed orders.  Same pattern rule as build_plan (the CSC pattern does not
 // depend on how the elements are grouped); the per-element tables are
 // variable-length, indexed by prefix bases.
-int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string &err) {
+int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string &err, const PlanScope *scope) {
 	if (!sp.assigned) { err = "assign_dofs() has not been called"; return -1; }
 	const Mesh &m = *sp.mesh;
-	const int64_t ne = m.ne();
+	const int64_t ne = scope ? (int64_t) scope->elems.size() : m.ne();
+	auto G = [&](int64_t e) -> int64_t { return scope ? scope->elems[e] : e; };   // plan element -> mesh element
 	P = Plan();
 	P.ne = ne;
 	P.ndof = sp.ndof();
@@ -795,7 +860,7 @@ int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string 
 		auto &d = desc[e];
 		int nl = 1, pmax = 0, qmax = 0;
 		for (int r = 0; r < 3; r++) {
-			const int p = sp.order[3 * e + r];
+			const int p = sp.order[3 * G(e) + r];
 			const int nq = p_plus ? p + qn : qn;
 			if (p < 1 || p > 10) { err = "element order out of range"; return -1; }
 			if (nq < 1 || nq > kMaxQuadPoints) { err = "Gauss points per direction must be in 1..13"; return -1; }
@@ -826,7 +891,7 @@ int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string 
 		std::vector<char> seen;
 		for (int64_t e = lo; e < hi; e++) {
 			const int nl = desc[e][9], py = desc[e][1], pz = desc[e][2];
-			sp.element_assembly_list(e, al);
+			sp.element_assembly_list(G(e), al);
 			int mcount = 0, lcount = 0;
 			for (auto &a : al) (a.dof >= 0 ? mcount : lcount)++;
 			if (mcount + lcount > nl) { bad[e] = 1; continue; }
@@ -867,6 +932,7 @@ int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string 
 	std::vector<int64_t> collen(nd, 0);
 	auto column = [&](int64_t d, std::vector<int32_t> &buf) {
 		buf.clear();
+		if (scope && !scope->owned[d]) return;                     // another part's column
 		for (int64_t k = dptr[d]; k < dptr[d + 1]; k++) {
 			int64_t e = dadj[k];
 			for (int j = 0; j < cnt[2 * e]; j++) buf.push_back(dofs[eb[e] + j]);
@@ -954,8 +1020,8 @@ int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string 
 		for (int64_t k = lo; k < hi; k++) {
 			const int64_t e = order_[k];
 			const int nl = desc[e][9];
-			P.el_id[k] = (int32_t) e;
-			for (int v = 0; v < 8; v++) P.el_vtx[8 * k + v] = (int32_t) m.hex[8 * e + v];
+			P.el_id[k] = (int32_t) G(e);
+			for (int v = 0; v < 8; v++) P.el_vtx[8 * k + v] = (int32_t) m.hex[8 * G(e) + v];
 			for (int t = 0; t < 11; t++) P.el_desc[(size_t) k * Plan::kDescInts + t] = desc[e][t];
 			P.el_cnt[2 * k] = cnt[2 * e];
 			P.el_cnt[2 * k + 1] = cnt[2 * e + 1];

@@ -160,11 +160,26 @@ struct Plan {
 	int max_nl = 0;
 };
 
-int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &plan, std::string &err, bool canon = false);
+// One part of a z-slab partition of the mesh (multi-GPU sharding without
+// communication): the part's slab of elements plus the one-element halo that
+// touches its DOFs, and the DOFs it owns.  A DOF belongs to the part whose
+// slab holds the lowest-numbered element with that DOF in its assembly list.
+// A plan built with a scope holds the full CSC columns of the owned DOFs
+// (global row and column numbering) and empty columns elsewhere, so every
+// owned column equals the one of the whole-mesh plan.
+struct PlanScope {
+	std::vector<int64_t> elems;              // element indices (0-based, ascending): slab + halo
+	std::vector<char> owned;                 // ndof: 1 where this part owns the DOF (CSC column)
+	int64_t nslab = 0, nhalo = 0, nowned = 0;
+};
+int make_partition_scope(const Space &sp, int nparts, int part, PlanScope &scope, std::string &err);
+
+int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &plan, std::string &err, bool canon = false,
+               const PlanScope *scope = nullptr);
 
 // Mixed orders: per element p_d + qn points per direction (p_plus) or qn
 // (fixed).  Elements are grouped by colour, then by kernel class, and within
 // a (colour, class) range ordered by decreasing work.
-int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &plan, std::string &err);
+int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &plan, std::string &err, const PlanScope *scope = nullptr);
 
 } // namespace h3dg

@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(NT, 1) k_assemble_fp64_ho(KArgsHO args, int64_
 							for (int q1 = 0; q1 < NQX; q1++) s += Vx[a * NQX + q1] * Z0[q1] + Dx[a * NQX + q1] * Z1[q1];
 							const int64_t pos = c0 + offrow[(int64_t) i * NL];
 							if (pos < c1) posted_add(args.Ax + pos, cc[i] * cj * s);
-							else atomicOr(args.status, kErrBounds);
+							else if (c1 > c0) atomicOr(args.status, kErrBounds);   // empty: column not owned
 						}
 					}
 				}

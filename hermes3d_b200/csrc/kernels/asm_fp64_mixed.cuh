@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(NT, MINB) k_assemble_fp64_mixed(KArgsMixed arg
 								if (q1 < nqx) s += Vx[a * nqx + q1] * Z0[q1] + Dx[a * nqx + q1] * Z1[q1];
 							const int64_t pos = c0 + offcol[i];
 							if (pos < c1) posted_add(args.Ax + pos, cc[i] * cj * s);
-							else atomicOr(args.status, kErrBounds);
+							else if (c1 > c0) atomicOr(args.status, kErrBounds);   // empty: column not owned
 						}
 					}
 				}

@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64_seq(KArgs args, int64_t kb
 							val[r] = Eb[S::E_C + a] * Eb[S::E_C + b] * (A[sa * NL + sb] + A[sb * NL + sa]);
 							const int64_t t = cs[b] + args.el_off[(k0 + e) * NL2 + b * NL + a];
 							if (t < cs[NL + b]) pos[r] = t;
-							else atomicOr(args.status, kErrBounds);
+							else if (cs[NL + b] > cs[b]) atomicOr(args.status, kErrBounds);   // empty: column not owned
 						}
 					}
 				}

@@ -111,8 +111,9 @@ __global__ void k_build_offt(const uint16_t *offc, const int32_t *cdof, const in
 				v = offc[(k * nl + i) * nl + j];
 				// every position is checked against its column once, here, so the
 				// epilogue can post without a bounds test
-				if (v == kOffSkip || (int64_t) v >= Ap[dj + 1] - Ap[dj]) {
-					atomicOr(status, kErrBounds);
+				const int64_t len = Ap[dj + 1] - Ap[dj];
+				if (v == kOffSkip || (int64_t) v >= len) {
+					if (len > 0) atomicOr(status, kErrBounds);     // an empty column is one this plan does not own
 					v = kOffSkip;
 				}
 			}

@@ -9,7 +9,8 @@ namespace h3dg {
 
 // error bits written to the plan's device status word
 constexpr int kErrTimeout = 1;
-constexpr int kErrBounds = 2;    // a scatter target fell outside its CSC column (store skipped)
+constexpr int kErrBounds = 2;    // a scatter target fell outside its (non-empty) CSC column (store skipped);
+                                 // an empty column belongs to another part of a partitioned plan: skipped silently
 
 // Everything a fused assembly kernel reads, as device pointers.
 struct KArgs {

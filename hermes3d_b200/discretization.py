@@ -193,6 +193,26 @@ class Discretization:
             self._quad = (capi.QUAD_P_PLUS, int(p_plus))
         capi.call("h3dg_disc_set_quadrature", self.handle, *self._quad)
 
+    def set_partition(self, nparts: int, part: int):
+        """Multi-GPU sharding without communication (no reference
+        counterpart): the next ``create`` builds part ``part`` of ``nparts``
+        z-slabs -- its slab of elements plus a one-element halo -- and
+        ``assemble`` then yields the full CSC columns of the DOFs it owns
+        (equal to the whole-mesh assembly's) with empty columns elsewhere."""
+        capi.call("h3dg_disc_set_partition", self.handle, int(nparts), int(part))
+
+    def partition(self):
+        """Owned-DOF mask and element counts of the current plan's part."""
+        owned = np.zeros(self.ndof, np.uint8)
+        ns, nh, no = C.c_int64(), C.c_int64(), C.c_int64()
+        capi.call("h3dg_disc_get_partition", self.handle, owned.ctypes.data_as(C.c_void_p), C.byref(ns), C.byref(nh),
+                  C.byref(no))
+        ne = self.space.mesh.num_elements
+        elems = np.zeros(ne, np.uint8)
+        capi.call("h3dg_disc_get_partition_elements", self.handle, elems.ctypes.data_as(C.c_void_p), ne)
+        return {"owned": owned.astype(bool), "elements": elems.astype(bool), "slab_elements": ns.value,
+                "halo_elements": nh.value, "owned_dofs": no.value}
+
     def create(self, matrix: Optional[UMFPackMatrix] = None, rhs: Optional[UMFPackVector] = None):
         """Discretization::create: sparsity pattern (+ device plan)."""
         capi.call("h3dg_disc_set_quadrature", self.handle, *self._quad)

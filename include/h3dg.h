@@ -128,6 +128,21 @@ h3dg_status h3dg_disc_set_quadrature(h3dg_disc *disc, int mode, int n);
 /* Discretization::create (src/discretization.cc:164-230) + UMFPackMatrix::alloc
  * (src/linsolver/umfpack.cc:46-71): builds the CSC pattern and the device plan */
 h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nnz);
+/* No reference counterpart (multi-GPU sharding, one process per GPU): build
+ * the next plan for part `part` of `nparts` z-slabs of the mesh.  The part
+ * assembles its slab of elements plus the one-element halo that touches its
+ * DOFs and produces the full CSC columns (and rhs entries) of the DOFs it
+ * owns -- equal to those of the whole-mesh assembly -- with empty columns
+ * elsewhere; no data moves between parts.  A DOF belongs to the part whose
+ * slab holds the lowest-numbered element listing it.  rhs entries of DOFs
+ * not owned hold partial sums: read the owned ones.  nparts = 1 (default):
+ * the whole mesh. */
+h3dg_status h3dg_disc_set_partition(h3dg_disc *disc, int nparts, int part);
+/* owned-DOF mask (ndof bytes, 1 = owned) and element counts of the current
+ * plan's part; any pointer may be NULL */
+h3dg_status h3dg_disc_get_partition(const h3dg_disc *disc, uint8_t *owned, int64_t *nslab, int64_t *nhalo, int64_t *nowned);
+/* elements the current plan's part assembles (slab + halo): ne bytes, 1 = in the part */
+h3dg_status h3dg_disc_get_partition_elements(const h3dg_disc *disc, uint8_t *in_part, int64_t ne);
 /* UMFPackMatrix Ap (ndof+1, widened to int64: nnz can exceed INT_MAX) and Ai (nnz) */
 h3dg_status h3dg_disc_get_pattern(const h3dg_disc *disc, int64_t *Ap, int32_t *Ai);
 /* Discretization::assemble (src/discretization.cc:232-422) into device arrays
