@@ -109,10 +109,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def build_problem(h, seed, device, side=N_ELEM_SIDE, workload="c2", partition=None):
+def build_problem(h, seed, device, side=None, workload="c2", partition=None):
     import numpy as np
     w = WORKLOADS[workload]
-    side = side if workload == "c2" else w["side"]
+    side = w["side"] if side is None else side
     mesh = h.unit_cube(side, w["jitter"], seed)
     mesh.ugh()
     sp = h.H1Space(mesh)
@@ -228,7 +228,7 @@ def main():
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--side", type=int, default=N_ELEM_SIDE, help="elements per cube side (profiling runs only)")
+    ap.add_argument("--side", type=int, default=None, help="elements per cube side (profiling runs only)")
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--partition", action="store_true",
                     help="N > 1: one mesh cut into N z-slab parts (strong scaling) instead of one subdomain per GPU")
@@ -351,7 +351,9 @@ def main():
         kms = kernel_ms if kernel_ms else ms_per_step
         achieved = B / (kms * 1e-3) / 1e9
         traffic = None
-        tf = os.path.join(ROOT, "profiles", "traffic_c2_assemble_fp64.json")
+        kern = {"c2": "assemble_fp64", "c3": "assemble_fp64_mixed", "c1": "assemble_fp64", "c5": "assemble_fp64",
+                "c4": "assemble_ho_tc" if prec != h.PREC_FP64 else "assemble_fp64_ho"}[args.workload]
+        tf = os.path.join(ROOT, "profiles", "traffic_%s_%s.json" % (args.workload, kern))
         if os.path.exists(tf):
             try:
                 traffic = json.load(open(tf)).get("bytes_per_step")
@@ -367,8 +369,8 @@ def main():
             "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "strong" if part else "weak",
             "vs_baseline": None, "dtype": "f64" if prec == h.PREC_FP64 else "tf32x3 (x stage) + f32 (z, y stages) + f64", "data": "synthetic (seeded jittered unit-cube mesh)",
-            "config": {"workload": WORKLOADS[args.workload]["desc"] if args.side == N_ELEM_SIDE or args.workload != "c2"
-                       else "C2 forms on %d^3 elements (profiling size)" % args.side,
+            "config": {"workload": WORKLOADS[args.workload]["desc"] if args.side in (None, WORKLOADS[args.workload]["side"])
+                       else "%s forms on %d^3 elements (profiling size)" % (args.workload.upper(), args.side),
                        "ndof": ndof, "nnz": nnz, "elements_per_gpu": elems_here,
                        "l2": "inputs larger than L2 (Ax alone %.2f GB)" % (8e-9 * nnz),
                        "parallelism": ("z-slab partition of one mesh into %d parts (halo elements replicated, owned "
