@@ -148,3 +148,34 @@ def test_c2_full_size_properties(gpu):
     d.assemble(M, V)
     assert np.array_equal(Ax1, M.Ax)
     assert np.all(np.isfinite(V.v)) and V.v.max() > 0
+
+
+@pytest.mark.parametrize("p,nq", [(1, 3), (2, 4), (3, 5)])
+def test_every_kernel_variant_is_bitwise_identical(gpu, monkeypatch, p, nq):
+    """The autotuner may pick any variant (CTA-per-element batches or one
+    element per warp): all of them must give the same bits."""
+    mesh = h.permute_vertices(h.unit_cube(4, 0.2, 9), seed=2)
+    mesh.ugh()
+    sp = h.H1Space(mesh)
+    sp.set_bc_values(lambda m, x, y, z: x * x + y * y + z * z)
+    sp.set_uniform_order(p)
+    sp.assign_dofs()
+    ref = None
+    for v in range(12):                       # indices past the last candidate pin the last one
+        monkeypatch.setenv("H3DG_FP64_VARIANT", str(v))
+        d = h.Discretization()
+        d.set_spaces(sp)
+        d.set_bilinear_form(h.int_grad_u_grad_v_plus_u_v, np.linspace(0.5, 2.0, mesh.num_elements))
+        d.set_linear_form(h.int_F_v("sin"))
+        d.set_quadrature(points=nq)
+        M, V = h.UMFPackMatrix(), h.UMFPackVector()
+        d.create(M, V)
+        d.assemble(M, V)
+        if ref is None:
+            ref = (M.Ax.copy(), V.v.copy())
+            al = port.asmlists_from_space(sp, mesh.num_elements)
+            Ax, rhs = port.assemble(mesh.xyz, mesh.hexes - 1, nq, al, sp.ndof, M.Ap, M.Ai, mass=True,
+                                    gradcoef=np.linspace(0.5, 2.0, mesh.num_elements), lf=2)
+            assert rel_err(M.Ax, Ax) < FP64_RTOL and rel_err(V.v, rhs) < FP64_RTOL
+        else:
+            assert np.array_equal(M.Ax, ref[0]) and np.array_equal(V.v, ref[1]), v
