@@ -220,6 +220,83 @@ def run_reference_arm(args):
     return 0
 
 
+def run_adjoint(args):
+    """C5 adjoint: dL_k/dg_{k,e} for 16 coefficient fields (one launch for all
+    fields), L_k = lam_k^T K(exp(g_k)) u_k - lam_k^T f(exp(g_k)).  value =
+    element-field sensitivities per second (device time); e2e = the same
+    through Discretization.adjoint with g, u, lam copied from pinned host
+    memory and the gradient copied back every step."""
+    import numpy as np
+    import torch
+    import hermes3d_b200 as h
+    from hermes3d_b200 import autograd as hag
+    nf = 16
+    torch.cuda.set_device(0)
+    mesh, sp, d = build_problem(h, seed=0, device=0, side=args.side, workload="c5")
+    ne, ndof = mesh.num_elements, d.ndof
+    rng = np.random.default_rng(5)
+    g = torch.from_numpy(rng.normal(0.0, 0.5, (nf, ne))).cuda()
+    u = torch.from_numpy(rng.normal(0.0, 1.0, (nf, ndof))).cuda()
+    lam = torch.from_numpy(rng.normal(0.0, 1.0, (nf, ndof))).cuda()
+    S = torch.empty(nf, ne, dtype=torch.float64, device="cuda")
+    grad = torch.empty_like(S)
+    stream = torch.cuda.current_stream()
+    for _ in range(max(3, args.warmup)):
+        d.adjoint(g, u, lam, S, grad, stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            d.adjoint(g, u, lam, S, grad, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = d.last_launch_count() * args.steps
+    # e2e through the public call with host buffers
+    gh, uh, lh = g.cpu().pin_memory(), u.cpu().pin_memory(), lam.cpu().pin_memory()
+    out = torch.empty(nf, ne, dtype=torch.float64).pin_memory()
+    nrep = max(1, args.e2e_steps)
+    torch.cuda.synchronize()
+    c0 = time.perf_counter()
+    for _ in range(nrep):
+        _, gr = d.adjoint(gh.cuda(non_blocking=True), uh.cuda(non_blocking=True), lh.cuda(non_blocking=True), S, grad)
+        out.copy_(gr, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - c0) * 1e3 / nrep
+    # forward (16 assemblies through the torch.autograd binding) + backward, for context
+    gg = g.clone().requires_grad_(True)
+    torch.cuda.synchronize()
+    c0 = time.perf_counter()
+    L = hag.assembly_energy(gg, u, lam, d)
+    L.sum().backward()
+    torch.cuda.synchronize()
+    fb_ms = (time.perf_counter() - c0) * 1e3
+    hbm, peak_kind = peaks()
+    B = 2 * 8 * nf * ndof + 3 * 8 * nf * ne + 24 * mesh.num_vertices + 32 * ne
+    achieved = B / (ms * 1e-3) / 1e9
+    print(json.dumps({
+        "metric": "hp adjoint element-field sensitivities/s (C5: 32^3 jittered hexahedra, p=3, 5^3 points, "
+                  "16 coefficient fields a=exp(g), g~N(0,0.5^2), u,lam~N(0,1))",
+        "value": nf * ne / (ms * 1e-3), "unit": "element-field sensitivities/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded jittered unit-cube mesh, seeded fields)",
+        "config": {"workload": "C5 adjoint, 16 fields, one launch per step", "ndof": ndof, "elements": ne,
+                   "fields": nf, "l2": "inputs larger than L2 (u, lam: %.2f GB)" % (16e-9 * nf * ndof)},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind,
+                     "algorithmic_bytes_per_step": B},
+        "e2e": {"value": nf * ne / (e2e_ms * 1e-3), "unit": "element-field sensitivities/s",
+                "h2d_bytes_per_step": 8 * nf * (ne + 2 * ndof), "d2h_bytes_per_step": 8 * nf * ne, "ms_per_step": e2e_ms},
+        "forward_backward_ms": fb_ms,
+        "cpu_baseline": None, "cpu_baseline_note": "the reference has no adjoint",
+        "clocks": clk.summary(),
+        "finite": bool(torch.isfinite(grad).all().item()),
+    }))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -234,9 +311,12 @@ def main():
                     help="N > 1: one mesh cut into N z-slab parts (strong scaling) instead of one subdomain per GPU")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3"],
                     help="tf32x3: split precision (tcgen05 3xTF32 x stage; high-order path)")
+    ap.add_argument("--adjoint", action="store_true", help="C5 adjoint line (16 fields) instead of an assembly line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.adjoint:
+        return run_adjoint(args)
 
     import numpy as np
     import torch
