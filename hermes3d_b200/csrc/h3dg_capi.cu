@@ -920,13 +920,14 @@ h3dg_status h3dg_disc_adjoint(h3dg_disc *disc, int nfields, const double *d_logc
 }
 
 h3dg_status h3dg_tc_selftest(int kind, const float *d_A, const float *d_B, float *d_C, int device) {
-	if (kind != 1 && kind != 2) return fail(H3DG_ERR_INVALID_ARG, "tc_selftest: kind must be 1 (bf16) or 2 (tf32)");
+	if (kind != 1 && kind != 2 && kind != 8) return fail(H3DG_ERR_INVALID_ARG, "tc_selftest: kind must be 1 (bf16), 2 (tf32) or 8 (int8)");
 	H3DG_CUDA_TRY(cudaSetDevice(device));
 	int *st = nullptr;
 	H3DG_CUDA_TRY(cudaMalloc(&st, sizeof(int)));
 	H3DG_CUDA_TRY(cudaMemset(st, 0, sizeof(int)));
 	if (kind == 2) h3dg::k_tc_selftest<h3dg::tc::kTF32><<<1, 128>>>(d_A, d_B, d_C, st);
-	else h3dg::k_tc_selftest<h3dg::tc::kBF16><<<1, 128>>>(d_A, d_B, d_C, st);
+	else if (kind == 1) h3dg::k_tc_selftest<h3dg::tc::kBF16><<<1, 128>>>(d_A, d_B, d_C, st);
+	else h3dg::k_tc_selftest<h3dg::tc::kI8><<<1, 128>>>(d_A, d_B, d_C, st);
 	cudaError_t e = cudaDeviceSynchronize();
 	int hs = 0;
 	if (e == cudaSuccess) e = cudaMemcpy(&hs, st, sizeof(int), cudaMemcpyDeviceToHost);

@@ -48,6 +48,12 @@ __host__ __device__ constexpr uint32_t instr_desc(int M, int N, int ab_format) {
 }
 
 constexpr int kTF32 = 2, kBF16 = 1;
+constexpr int kI8 = 8;   // selects kind::i8 (signed int8 operands, int32 accumulator)
+
+// kind::i8: c_format S32 (2), a / b format signed int8 (1)
+__host__ __device__ constexpr uint32_t instr_desc_i8(int M, int N) {
+	return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (N >> 3) << 17) | ((uint32_t) (M >> 4) << 24);
+}
 
 // Allocate ncols TMEM columns (power of two >= 32); warp-wide, one warp.
 // The address is written to *slot (shared memory).
@@ -75,6 +81,16 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint6
 		"{\n\t.reg .pred p;\n\t"
 		"setp.ne.b32 p, %4, 0;\n\t"
 		"tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}" ::"r"(d_tmem),
+		"l"(a_desc), "l"(b_desc), "r"(idesc), "r"((uint32_t) accumulate), "r"(0u)
+		: "memory");
+}
+
+// int8 x int8 -> int32, K = 32 per instruction
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc, bool accumulate) {
+	asm volatile(
+		"{\n\t.reg .pred p;\n\t"
+		"setp.ne.b32 p, %4, 0;\n\t"
+		"tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}" ::"r"(d_tmem),
 		"l"(a_desc), "l"(b_desc), "r"(idesc), "r"((uint32_t) accumulate), "r"(0u)
 		: "memory");
 }
@@ -124,6 +140,11 @@ __host__ __device__ __forceinline__ uint32_t kmaj_off32(int r, int k, int R) {
 // same for 2-byte elements
 __host__ __device__ __forceinline__ uint32_t kmaj_off16(int r, int k, int R) {
 	return (uint32_t) ((((k >> 3) * (R >> 3) + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
+}
+
+// same for 1-byte elements
+__host__ __device__ __forceinline__ uint32_t kmaj_off8(int r, int k, int R) {
+	return (uint32_t) ((((k >> 4) * (R >> 3) + (r >> 3)) << 7) + ((r & 7) << 4) + (k & 15));
 }
 
 // round to tf32 (nearest, ties away) and return as float

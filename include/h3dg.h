@@ -205,8 +205,9 @@ h3dg_status h3dg_disc_adjoint(h3dg_disc *disc, int nfields, const double *d_logc
 
 /* Diagnostic (no reference counterpart): one 128 x 128 tcgen05 MMA tile,
  * C = A B^T, A and B 128 x K row-major floats (K = 32 for kind 2 = tf32,
- * K = 64 for kind 1 = bf16), C 128 x 128; device pointers.  Checks the
- * tensor-core layer the split-precision kernels use. */
+ * K = 64 for kind 1 = bf16 and kind 8 = int8, integer values in -128..127;
+ * the int32 result is returned as floats), C 128 x 128; device pointers.
+ * Checks the tensor-core layer the split-precision kernels use. */
 h3dg_status h3dg_tc_selftest(int kind, const float *d_A, const float *d_B, float *d_C, int device);
 
 /* RefMap (src/refmap.cc:177-231, 265-316): per element (id order) and per point of the

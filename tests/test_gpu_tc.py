@@ -11,11 +11,14 @@ from hermes3d_b200 import _capi
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("kind,K", [(2, 32), (1, 64)])
-def test_tc_selftest_exact(gpu, kind, K):
+@pytest.mark.parametrize("kind,K,lim", [(2, 32, 4), (1, 64, 4), (8, 64, 127)])
+def test_tc_selftest_exact(gpu, kind, K, lim):
     rng = np.random.default_rng(kind)
-    A = rng.integers(-4, 5, size=(128, K)).astype(np.float32)
-    B = rng.integers(-4, 5, size=(128, K)).astype(np.float32)
+    A = rng.integers(-lim, lim + 1, size=(128, K)).astype(np.float32)
+    B = rng.integers(-lim, lim + 1, size=(128, K)).astype(np.float32)
+    if kind == 8:
+        A[0, :8] = -128                       # int8 extremes
+        B[0, :8] = -128
     # distinct row / column signatures so a permuted read-back cannot pass
     A[:, 0] = np.arange(128) % 7 - 3
     B[:, 1] = np.arange(128) % 5 - 2
