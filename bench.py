@@ -210,7 +210,7 @@ def run_reference_arm(args):
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if prec == h.PREC_FP64 else "tf32x3 (x stage) + f32 (z, y stages) + f64", "data": "synthetic", "impl": "reference",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
         "config": {"workload": "C2 sample: %d^3 jittered hexahedra per process, p=2, 4^3 Gauss points, grad+mass, "
                                "sin source" % n, "processes": ncores},
         "cpu_baseline": {"value": value, "unit": "elements/s", "cores": ncores, "kind": "reference",
@@ -309,8 +309,9 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--partition", action="store_true",
                     help="N > 1: one mesh cut into N z-slab parts (strong scaling) instead of one subdomain per GPU")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3"],
-                    help="tf32x3: split precision (tcgen05 3xTF32 x stage; high-order path)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3", "ozaki"],
+                    help="tf32x3 / ozaki: split precision on tcgen05 (3xTF32, or int8 slices with FP64 accuracy); "
+                         "high-order path")
     ap.add_argument("--adjoint", action="store_true", help="C5 adjoint line (16 fields) instead of an assembly line")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -349,7 +350,7 @@ def main():
         tn = torch.tensor([nnz], dtype=torch.int64, device="cuda")
         dist.all_reduce(tn)
         nnz_job = int(tn.item())
-    prec = h.PREC_TF32X3 if args.precision == "tf32x3" else h.PREC_FP64
+    prec = {"fp64": h.PREC_FP64, "tf32x3": h.PREC_TF32X3, "ozaki": h.PREC_OZAKI}[args.precision]
     stream = torch.cuda.current_stream()
     Ax = torch.empty(nnz, dtype=torch.float64, device="cuda")
     rhs = torch.empty(ndof, dtype=torch.float64, device="cuda")
@@ -422,7 +423,8 @@ def main():
         split_error = {
             "max_abs_over_max": float(diff.abs().max() / A64.abs().max()),
             "frobenius_rel": float(torch.linalg.vector_norm(diff) / torch.linalg.vector_norm(A64)),
-            "tolerance": 1e-6, "against": "FP64 kernel on the same plan (itself oracle-checked at 1e-12)"}
+            "tolerance": 1e-6 if prec == h.PREC_TF32X3 else 1e-12,
+            "against": "FP64 kernel on the same plan (itself oracle-checked at 1e-12)"}
         del diff, A64
 
     if rank == 0:
@@ -432,7 +434,8 @@ def main():
         achieved = B / (kms * 1e-3) / 1e9
         traffic = None
         kern = {"c2": "assemble_fp64", "c3": "assemble_fp64_mixed", "c1": "assemble_fp64", "c5": "assemble_fp64",
-                "c4": "assemble_ho_tc" if prec != h.PREC_FP64 else "assemble_fp64_ho"}[args.workload]
+                "c4": {h.PREC_FP64: "assemble_fp64_ho", h.PREC_TF32X3: "assemble_ho_tc",
+                       h.PREC_OZAKI: "assemble_ho_oz"}[prec]}[args.workload]
         tf = os.path.join(ROOT, "profiles", "traffic_%s_%s.json" % (args.workload, kern))
         if os.path.exists(tf):
             try:
@@ -441,14 +444,17 @@ def main():
                 traffic = None
         metric = METRIC if args.workload == "c2" else METRIC.replace("C2: 64^3 jittered, p=2, 4^3 pts, grad+mass, sin source",
                                                                         WORKLOADS[args.workload]["desc"])
-        if prec != h.PREC_FP64:
+        if prec == h.PREC_TF32X3:
             metric = metric.replace("(FP64, ", "(split precision 3xTF32 on tcgen05, FP64 geometry/scatter, ")
+        elif prec == h.PREC_OZAKI:
+            metric = metric.replace("(FP64, ", "(FP64-accurate split: int8-sliced x stage on tcgen05, FP64 elsewhere, ")
         out = {
             "metric": metric,
             "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "strong" if part else "weak",
-            "vs_baseline": None, "dtype": "f64" if prec == h.PREC_FP64 else "tf32x3 (x stage) + f32 (z, y stages) + f64", "data": "synthetic (seeded jittered unit-cube mesh)",
+            "vs_baseline": None, "dtype": {h.PREC_FP64: "f64", h.PREC_TF32X3: "tf32x3 (x stage) + f32 (z, y stages) + f64",
+                      h.PREC_OZAKI: "int8 x7 slices, int32 accumulate (x stage) + f64"}[prec], "data": "synthetic (seeded jittered unit-cube mesh)",
             "config": {"workload": WORKLOADS[args.workload]["desc"] if args.side in (None, WORKLOADS[args.workload]["side"])
                        else "%s forms on %d^3 elements (profiling size)" % (args.workload.upper(), args.side),
                        "ndof": ndof, "nnz": nnz, "elements_per_gpu": elems_here,

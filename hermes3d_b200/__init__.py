@@ -12,9 +12,10 @@ from .mesh import Mesh, load_mesh3d, permute_vertices, unit_cube
 
 PREC_FP64 = _capi.PREC_FP64
 PREC_TF32X3 = _capi.PREC_TF32X3
+PREC_OZAKI = _capi.PREC_OZAKI
 
 __all__ = [
     "Mesh", "load_mesh3d", "unit_cube", "permute_vertices", "H1Space", "Discretization", "UMFPackMatrix",
     "UMFPackVector", "int_grad_u_grad_v", "int_grad_u_grad_v_plus_u_v", "int_F_v", "UnsupportedForm",
-    "BC_ESSENTIAL", "BC_NATURAL", "BC_NONE", "PREC_FP64", "PREC_TF32X3",
+    "BC_ESSENTIAL", "BC_NATURAL", "BC_NONE", "PREC_FP64", "PREC_TF32X3", "PREC_OZAKI",
 ]

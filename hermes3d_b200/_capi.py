@@ -25,6 +25,7 @@ LF_NONE, LF_CONST, LF_SIN = 0, 1, 2
 QUAD_FIXED, QUAD_P_PLUS = 0, 1
 PREC_FP64 = 0
 PREC_TF32X3 = 1
+PREC_OZAKI = 2
 NOALLOC_SCRATCH_DOUBLES = 2 << 20
 
 BC_TYPE_FN = C.CFUNCTYPE(C.c_int, C.c_int, C.c_void_p)

@@ -506,7 +506,8 @@ extern "C" {
 
 static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, cudaStream_t st) {
 	const h3dg::Plan &P = disc->plan;
-	std::vector<HoSpec> &table = precision == H3DG_PREC_TF32X3 ? ho_tc_table() : ho_table();
+	std::vector<HoSpec> &table = precision == H3DG_PREC_TF32X3 ? ho_tc_table()
+	                             : precision == H3DG_PREC_OZAKI ? ho_oz_table() : ho_table();
 	std::vector<int> cands;
 	for (size_t i = 0; i < table.size(); i++)
 		if (table[i].p == P.px && table[i].nq == P.nqx) cands.push_back((int) i);
@@ -519,7 +520,7 @@ static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, dou
 	a.cdof = disc->el_cdof.p;
 	a.ccoef = disc->el_ccoef.p;
 	a.offc = disc->el_offc.p;
-	if (precision == H3DG_PREC_TF32X3 && d_Ax && !disc->el_offt.p && P.ne > 0) {
+	if ((precision == H3DG_PREC_TF32X3 || precision == H3DG_PREC_OZAKI) && d_Ax && !disc->el_offt.p && P.ne > 0) {
 		// built once per plan; the build validates every position against its
 		// column, so the split kernel posts without a per-entry bounds test
 		size_t cnt = 0;
@@ -741,7 +742,8 @@ static h3dg_status assemble_mixed(h3dg_disc *disc, double *d_Ax, double *d_rhs, 
 
 h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream) {
 	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "assemble: create_pattern() first");
-	if (precision != H3DG_PREC_FP64 && precision != H3DG_PREC_TF32X3) return fail(H3DG_ERR_INVALID_ARG, "assemble: unknown precision");
+	if (precision != H3DG_PREC_FP64 && precision != H3DG_PREC_TF32X3 && precision != H3DG_PREC_OZAKI)
+		return fail(H3DG_ERR_INVALID_ARG, "assemble: unknown precision");
 	const h3dg::Plan &P = disc->plan;
 	if (P.mixed) {
 		h3dg_status s0 = ensure_device(disc);
@@ -1018,7 +1020,7 @@ extern "C" {
 
 h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, double *Ax, double *rhs) {
 	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "assemble_host_noalloc: create_pattern() first");
-	if (precision != H3DG_PREC_FP64 && precision != H3DG_PREC_TF32X3)
+	if (precision != H3DG_PREC_FP64 && precision != H3DG_PREC_TF32X3 && precision != H3DG_PREC_OZAKI)
 		return fail(H3DG_ERR_INVALID_ARG, "assemble_host_noalloc: unknown precision");
 	const h3dg::Plan &P = disc->plan;
 	const size_t rhs_off = ((size_t) P.nnz + 31) / 32 * 32;          // 256-byte boundary
@@ -1031,7 +1033,7 @@ h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, doub
 	// everything h3dg_disc_assemble would allocate lazily must already exist
 	if (!disc->on_device || !disc->status.p)
 		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: device plan not uploaded; make one allocating assembly call first");
-	if (P.canon && precision == H3DG_PREC_TF32X3 && Ax && !disc->el_offt.p && P.ne > 0)
+	if (P.canon && (precision == H3DG_PREC_TF32X3 || precision == H3DG_PREC_OZAKI) && Ax && !disc->el_offt.p && P.ne > 0)
 		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: split-precision scatter stream not built; make one allocating "
 		                            "split-precision assembly call first");
 	if (P.mixed && disc->mx_variant[0] < 0)

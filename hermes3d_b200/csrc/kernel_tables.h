@@ -65,6 +65,8 @@ std::vector<KernelSpec> &kernel_table();
 std::vector<HoSpec> &ho_table();
 // split-precision high-order kernels (tcgen05 3xTF32 stage 3)
 std::vector<HoSpec> &ho_tc_table();
+// FP64-accurate high-order kernels (int8-sliced tcgen05 stage 3)
+std::vector<HoSpec> &ho_oz_table();
 // tensor-core scatter stream from the canonical position map (async on st)
 cudaError_t build_offt(const uint16_t *offc, const int32_t *cdof, const int64_t *Ap, int64_t ne, int px, int nq,
                        uint16_t **offt, size_t *count, int *status, cudaStream_t st);

@@ -1,0 +1,382 @@
+// FP64-accurate high-order assembly with the x stage on the int8 tensor
+// cores (Ozaki-style splitting).
+//
+// Same element matrix as k_assemble_fp64_ho (src/integrals/h1.h:115-177 per
+// pair, restated as sum factorisation).  Geometry, G, the load vector, the
+// lifting and stages 1 (zeta) and 2 (eta) are FP64.  Stage 3,
+//     K[(a,b,c)][(a',b',c')] = sum_k V[(b',b,c)][k] E[(a',a)][k],
+//     k = (f, q1): 4 x-classes x NQX points,
+// is a GEMM whose FP64 operands are split into NS = 7 int8 slices each:
+// every row of V (and of E) is scaled by a power of two 2^-e so that its
+// largest entry is below 1, and v 2^-e = sum_i a_i 2^{-7(i+1)} + r with
+// integers |a_i| <= 127 (a_i = trunc(128 r_i), r_{i+1} = 128 r_i - a_i, exact
+// in FP64) and |r| < 2^-49.  The slice products a_i b_j are summed by
+// tcgen05.mma kind::i8 into int32 accumulators in TMEM, one accumulator per
+// level l = i + j <= NS - 1 (products of one level share the scale
+// 2^{-7(l+2)}; |acc_l| <= 7 * 64 * 127^2 < 2^31, so every sum is exact), and
+// recombined in FP64 in the epilogue:
+//     K = 2^{e_row + e_col} sum_l acc_l 2^{-7(l+2)}.
+// The dropped levels and the slice residuals leave a relative error of
+// order K_dim 2^-49 of the row / column scales (measured ~1e-14, tolerance
+// 1e-12).
+//
+// Shared memory holds one V slice at a time (two buffers: slice i+1 is cut
+// from the FP64 values kept in registers while the MMAs of slice i run), so
+// the FP64 stage-1 products fit beside the constant E slices.  N (the (a',a)
+// pairs, padded to 16) is covered in NPASS passes of NC columns so that the
+// NS level accumulators fit in TMEM (NS * NC <= 512).  The epilogue and the
+// scatter stream are those of the split-precision kernel (one CSC column per
+// warp and trial x index, positions validated when the stream is built).
+// Every mbarrier wait is bounded; on timeout the kernel records kErrTimeout,
+// drains, frees its TMEM and leaves.
+#pragma once
+
+#include "asm_ho_tc.cuh"
+
+namespace h3dg {
+
+template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ>
+struct HoOzShape {
+	using B = HoShape<PX, PY, PZ, NQX, NQY, NQZ>;
+	static constexpr int NX = B::NX, NY = B::NY, NZ = B::NZ, NL = B::NL, NQ = B::NQ;
+	static constexpr int NS = 7;                              // slices per operand
+	static constexpr int NPAIR = NX * NX;
+	static constexpr int NB = ho_tc_align(NPAIR, 16);
+	static constexpr int NPASS = NB <= 64 ? 1 : 2;
+	static constexpr int NC = NB / NPASS;                     // MMA N per pass
+	static constexpr int KD = ho_tc_align(4 * NQX, 32);       // MMA K (int8: 32 per instruction)
+	static constexpr int NCOL = NY * NY * NZ;
+	static constexpr int TM = 128;
+	static constexpr int NTILE = (NCOL + TM - 1) / TM;
+	static constexpr int TMEM_COLS = 512;
+	static constexpr int H0 = (NQX + 1) / 2;
+	static constexpr int T1D = 9 * NQX * NQY * NZ;            // stage-1 products (doubles)
+	// dynamic shared memory, byte offsets
+	static constexpr int O_TAB = 0;
+	static constexpr int O_BOP = ho_tc_align(O_TAB + 8 * B::TABP, 128);   // NS slices of NB x KD int8
+	static constexpr int BOP_SLICE = NB * KD;
+	static constexpr int O_FEX = O_BOP + NS * BOP_SLICE;                  // NB int: column exponents
+	static constexpr int O_G = ho_tc_align(O_FEX + 4 * NB, 128);         // 8 x NQ doubles
+	static constexpr int O_U = O_G + 8 * 8 * NQ;                          // union, see below
+	//   FP64 phase: matrix-free work (MF doubles)
+	//   matrix phase: T1 (T1D doubles), row maxima (2 x TM doubles), row exponents (TM int),
+	//                 two V slice buffers (TM x KD int8 each)
+	static constexpr int U_FP64 = 8 * B::MF;
+	static constexpr int R_RMX = 8 * T1D;
+	static constexpr int R_REX = R_RMX + 8 * 2 * TM;
+	static constexpr int R_ASL = ho_tc_align(R_REX + 4 * TM, 128);
+	static constexpr int ASL = TM * KD;
+	static constexpr int U_MAT = R_ASL + 2 * ASL;
+	static constexpr int O_X = O_U + ho_tc_align(ho_tc_max(U_FP64, U_MAT), 16);
+	static constexpr int O_M = O_X + 24 * 8;
+	static constexpr int O_C = O_M + 24 * 8;
+	static constexpr int O_CS = O_C + NL * 8;
+	static constexpr int O_CE = O_CS + NL * 8;
+	static constexpr int O_D = O_CE + NL * 8;
+	static constexpr size_t SMEM_BYTES = (size_t) O_D + (size_t) NL * 4 + 16;
+	static_assert(NC % 16 == 0 && NC <= 256 && NS * NC <= TMEM_COLS, "MMA shape / TMEM budget");
+	static_assert(SMEM_BYTES <= 227 * 1024, "shared memory");
+};
+
+// 32 lanes x 32 bit, 4 consecutive columns per thread, no wait
+__device__ __forceinline__ void tmem_ld4_i32(uint32_t taddr, int v[4]) {
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+	             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+	             : "r"(taddr));
+}
+
+// stage 1 (FP64) for a fixed trial z index c': T1_kk[q1][q2][c]
+template <class S, int NT>
+__device__ __forceinline__ void ho_oz_stage1(const double *G, const double *tab, int c2, int mass, double *T1) {
+	using SB = typename S::B;
+	constexpr int NZ = S::NZ, NQ = S::NQ, NQX = SB::QX, NQY = SB::QY, NQZ = SB::QZ;
+	const double *Vz = tab + SB::OVZ, *Dz = tab + SB::ODZ;
+	for (int i = threadIdx.x; i < 9 * NQX * NQY; i += NT) {
+		const int kk = i / (NQX * NQY), q12 = i % (NQX * NQY);
+		const int fz = kHoFz[kk];
+		const double *eb = (fz & 1) ? Dz + c2 * NQZ : Vz + c2 * NQZ;
+		const double *gp = G + kHoG[kk] * NQ + q12 * NQZ;
+		const double *gm = G + 6 * NQ + q12 * NQZ;
+		const bool addm = kk == 2 && mass;
+		double h[NQZ], hm[NQZ];
+#pragma unroll
+		for (int q3 = 0; q3 < NQZ; q3++) {
+			h[q3] = gp[q3] * eb[q3];
+			hm[q3] = addm ? gm[q3] * Vz[c2 * NQZ + q3] : 0.0;
+		}
+		double *out = T1 + (kk * NQX * NQY + q12) * NZ;
+		for (int c = 0; c < NZ; c++) {
+			const double *ea = (fz >> 1) ? Dz + c * NQZ : Vz + c * NQZ;
+			double s = 0.0;
+#pragma unroll
+			for (int q3 = 0; q3 < NQZ; q3++) s += h[q3] * ea[q3];
+			if (addm) {
+#pragma unroll
+				for (int q3 = 0; q3 < NQZ; q3++) s += hm[q3] * Vz[c * NQZ + q3];
+			}
+			out[c] = s;
+		}
+	}
+}
+
+// cut slice `i` of the scaled values r0 (|r0| < 1) and store it, int8,
+// K-major at row m of a TM-row operand; K padding stays zero
+template <class S>
+__device__ __forceinline__ void ho_oz_put_slice(const double (&r0)[4][S::H0], int i, int m, int half, unsigned char *buf) {
+	using SB = typename S::B;
+	constexpr int NQX = SB::QX, H0 = S::H0, KD = S::KD, TM = S::TM;
+#pragma unroll
+	for (int f = 0; f < 4; f++)
+#pragma unroll
+		for (int j = 0; j < H0; j++) {
+			const int q1 = j + half * H0;
+			if (q1 < NQX) {
+				double r = r0[f][j];
+				int a = 0;
+				for (int t = 0; t <= i; t++) {
+					r *= 128.0;
+					a = (int) r;                 // trunc: |a| <= 127
+					r -= (double) a;             // exact
+				}
+				buf[tc::kmaj_off8(m, f * NQX + q1, TM)] = (unsigned char) (int8_t) a;
+			}
+		}
+	if (KD > 4 * NQX && half == 1)
+		for (int kq = 4 * NQX; kq < KD; kq++) buf[tc::kmaj_off8(m, kq, TM)] = 0;
+}
+
+template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ>
+__global__ void __launch_bounds__(256, 1) k_assemble_ho_oz(KArgsHO args, int64_t kbeg, int64_t kend) {
+	constexpr int NT = 256;
+	using S = HoOzShape<PX, PY, PZ, NQX, NQY, NQZ>;
+	using SB = typename S::B;
+	constexpr int NX = S::NX, NY = S::NY, NZ = S::NZ, NQ = S::NQ, NS = S::NS;
+	constexpr int NB = S::NB, NC = S::NC, KD = S::KD, TM = S::TM, H0 = S::H0;
+	extern __shared__ __align__(128) unsigned char smb[];
+	__shared__ uint64_t bar_tab, bar_mma[2];
+	__shared__ int s_nlift;
+	__shared__ uint32_t s_tmem;
+
+	double *tab = reinterpret_cast<double *>(smb + S::O_TAB);
+	unsigned char *bop = smb + S::O_BOP;
+	int *fex = reinterpret_cast<int *>(smb + S::O_FEX);
+	double *G = reinterpret_cast<double *>(smb + S::O_G);
+	double *MFw = reinterpret_cast<double *>(smb + S::O_U);
+	double *T1 = reinterpret_cast<double *>(smb + S::O_U);
+	double *rmx = reinterpret_cast<double *>(smb + S::O_U + S::R_RMX);
+	int *rex = reinterpret_cast<int *>(smb + S::O_U + S::R_REX);
+	unsigned char *asl = smb + S::O_U + S::R_ASL;          // buffer q at asl + q ASL
+	double *X = reinterpret_cast<double *>(smb + S::O_X), *Mo = reinterpret_cast<double *>(smb + S::O_M);
+	double *cc = reinterpret_cast<double *>(smb + S::O_C);
+	int64_t *cs = reinterpret_cast<int64_t *>(smb + S::O_CS), *ce = reinterpret_cast<int64_t *>(smb + S::O_CE);
+	int *cd = reinterpret_cast<int *>(smb + S::O_D);
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+	if (!stage_tables(tab, args.tables, args.table_bytes, &bar_tab, args.status)) return;
+	if (warp == 0) tc::tmem_alloc(&s_tmem, S::TMEM_COLS);
+	if (tid == 0) {
+		mbar_init(&bar_mma[0], 1);
+		mbar_init(&bar_mma[1], 1);
+		fence_mbar_init();
+	}
+	// constant E operand: per pair row n its exponent and NS int8 slices
+	auto eval_e = [&](int n, int kq) -> double {
+		if (n >= S::NPAIR || kq >= 4 * NQX) return 0.0;
+		const int a2 = n / NX, a = n % NX, f = kq / NQX, q1 = kq % NQX;
+		const double ea = (f >> 1) ? tab[SB::ODX + a * NQX + q1] : tab[SB::OVX + a * NQX + q1];
+		const double eb = (f & 1) ? tab[SB::ODX + a2 * NQX + q1] : tab[SB::OVX + a2 * NQX + q1];
+		return ea * eb;
+	};
+	for (int n = tid; n < NB; n += NT) {
+		double mx = 0.0;
+#pragma unroll 1
+		for (int kq = 0; kq < 4 * NQX; kq++) mx = fmax(mx, fabs(eval_e(n, kq)));
+		int e = 0;
+		if (mx > 0.0) frexp(mx, &e);
+		fex[n] = e;
+#pragma unroll 1
+		for (int kq = 0; kq < KD; kq++) {
+			double r = ldexp(eval_e(n, kq), -e);
+#pragma unroll 1
+			for (int i = 0; i < NS; i++) {
+				r *= 128.0;
+				const int a = (int) r;
+				r -= (double) a;
+				bop[i * S::BOP_SLICE + tc::kmaj_off8(n, kq, NB)] = (unsigned char) (int8_t) a;
+			}
+		}
+	}
+	tc::fence_async_smem();
+	tc::fence_before_sync();
+	__syncthreads();
+	tc::fence_after_sync();
+	const uint32_t tmem = s_tmem;
+	const double *Vy = tab + SB::OVY, *Dy = tab + SB::ODY;
+	const bool do_rhs = args.rhs && args.lf;
+	// per slice buffer: commits issued and waited (all threads keep the same counts)
+	uint32_t iss0 = 0u, iss1 = 0u, wt0 = 0u, wt1 = 0u;
+	bool alive = true;
+	const int quarter = warp & 3, chalf = warp >> 2;
+
+	auto drain = [&](int q) -> bool {                     // wait for buffer q's outstanding commit
+		const uint32_t iss = q ? iss1 : iss0, wt = q ? wt1 : wt0;
+		if (iss == wt) return true;
+		const uint32_t par = wt & 1u;
+		bool ok = mbar_wait_bounded(&bar_mma[q], par, args.status);
+		if (!ok) mbar_wait_bounded(&bar_mma[q], par, nullptr, 1u << 26);
+		if (q) wt1++;
+		else wt0++;
+		return ok;
+	};
+
+	for (int64_t k = kbeg + blockIdx.x; k < kend && alive; k += gridDim.x) {
+		const double cgrad = ho_element_setup<SB, NT>(args, k, X, Mo, cc, cd, cs, ce, &s_nlift);
+		ho_geometry<SB, NT>(args, tab, Mo, cgrad, G);
+		if (do_rhs) ho_rhs<SB, NT>(args, tab, G, MFw, cd, cc, s_nlift > 0);
+		if (!args.Ax) continue;
+		const uint16_t *offe = args.offt + (size_t) k * NZ * S::NCOL * NB;
+
+		for (int c2 = 0; c2 < NZ && alive; c2++) {
+			ho_oz_stage1<S, NT>(G, tab, c2, args.mass, T1);
+			__syncthreads();
+			for (int tt = 0; tt < S::NTILE && alive; tt++) {
+				// ---- stage 2 (FP64): V_f[q1] of row col = (b', b, c), q1 split over two threads
+				const int m = tid & (TM - 1), half = tid >> 7;
+				const int col = tt * TM + m;
+				double V[4][H0];
+#pragma unroll
+				for (int f = 0; f < 4; f++)
+#pragma unroll
+					for (int j = 0; j < H0; j++) V[f][j] = 0.0;
+				if (col < S::NCOL) {
+					const int b2 = col / (NY * NZ), b = (col / NZ) % NY, c = col % NZ;
+#pragma unroll
+					for (int kk = 0; kk < 9; kk++) {
+						constexpr int kFy[9] = { 0, 3, 0, 1, 2, 0, 0, 2, 1 };
+						constexpr int kCls[9] = { 3, 0, 0, 2, 1, 2, 1, 0, 0 };
+						const int fy = kFy[kk], f = kCls[kk];
+						const double *ea = (fy >> 1) ? Dy + b * NQY : Vy + b * NQY;
+						const double *eb = (fy & 1) ? Dy + b2 * NQY : Vy + b2 * NQY;
+						double wy[NQY];
+#pragma unroll
+						for (int q2 = 0; q2 < NQY; q2++) wy[q2] = ea[q2] * eb[q2];
+						const double *t1 = T1 + kk * NQX * NQY * NZ + c;
+#pragma unroll
+						for (int j = 0; j < H0; j++) {
+							const int q1 = j + half * H0;
+							if (q1 < NQX) {
+								double s = V[f][j];
+#pragma unroll
+								for (int q2 = 0; q2 < NQY; q2++) s += wy[q2] * t1[(q1 * NQY + q2) * NZ];
+								V[f][j] = s;
+							}
+						}
+					}
+				}
+				// row exponent from both halves' maxima
+				double mx = 0.0;
+#pragma unroll
+				for (int f = 0; f < 4; f++)
+#pragma unroll
+					for (int j = 0; j < H0; j++) mx = fmax(mx, fabs(V[f][j]));
+				rmx[half * TM + m] = mx;
+				__syncthreads();
+				mx = fmax(rmx[m], rmx[TM + m]);
+				int erow = 0;
+				if (mx > 0.0) frexp(mx, &erow);
+				if (half == 0) rex[m] = erow;
+#pragma unroll
+				for (int f = 0; f < 4; f++)
+#pragma unroll
+					for (int j = 0; j < H0; j++) V[f][j] = ldexp(V[f][j], -erow);   // |V| < 1 now
+
+				for (int pass = 0; pass < S::NPASS && alive; pass++) {
+					// ---- slices: cut slice i into buffer (step & 1), MMAs of all pairs (i, j <= NS-1-i)
+					for (int i = 0; i < NS; i++) {
+						const int q = i & 1;
+						if (!__syncthreads_and(drain(q) ? 1 : 0)) {
+							alive = false;
+							break;
+						}
+						unsigned char *buf = asl + q * S::ASL;
+						ho_oz_put_slice<S>(V, i, m, half, buf);
+						tc::fence_async_smem();
+						tc::fence_before_sync();
+						__syncthreads();
+						if (tid == 0) {
+							tc::fence_after_sync();
+							constexpr uint32_t idesc = tc::instr_desc_i8(TM, NC);
+							constexpr uint32_t lbo_a = (TM / 8) * 128, lbo_b = (NB / 8) * 128;
+							for (int j = 0; j + i < NS; j++) {
+								const unsigned char *pb = bop + j * S::BOP_SLICE + (pass * NC / 8) * 128;
+								const uint32_t dacc = tmem + (uint32_t) ((i + j) * NC);
+#pragma unroll
+								for (int s = 0; s < KD / 32; s++) {
+									const uint64_t da = tc::smem_desc(buf + s * 2 * lbo_a, lbo_a, 128);
+									const uint64_t db = tc::smem_desc(pb + s * 2 * lbo_b, lbo_b, 128);
+									tc::mma_i8(dacc, da, db, idesc, i > 0 || s > 0);
+								}
+							}
+							tc::mma_commit(&bar_mma[q]);
+						}
+						if (q) iss1++;
+						else iss0++;
+					}
+					if (!alive) break;
+					// ---- all levels of this pass complete
+					bool ok = drain(0);
+					ok = drain(1) && ok;
+					if (!__syncthreads_and(ok ? 1 : 0)) {
+						alive = false;
+						break;
+					}
+					tc::fence_after_sync();
+					// ---- epilogue: TMEM row = (b', b, c), columns n = pass NC + u, u < NC
+					{
+						const int mrow = quarter * 32 + lane;
+						const int colr = tt * TM + mrow;
+						const bool live = colr < S::NCOL;
+						const int b2 = live ? colr / (NY * NZ) : 0, b = live ? (colr / NZ) % NY : 0, c = live ? colr % NZ : 0;
+						const int er = rex[mrow];
+						const uint16_t *rec = offe + ((size_t) c2 * S::NCOL + (live ? colr : 0)) * NB;
+						const uint32_t tl = tmem + ((uint32_t) (quarter * 32) << 16);
+						constexpr int NCH4 = NC / 4;                      // 4-column chunks
+						constexpr int CHH = (NCH4 + 1) / 2;
+						const int ch0 = chalf ? CHH : 0, ch1 = chalf ? NCH4 : CHH;
+						for (int ch = ch0; ch < ch1; ch++) {
+							int acc[NS][4];
+#pragma unroll
+							for (int l = 0; l < NS; l++) tmem_ld4_i32(tl + (uint32_t) (l * NC + ch * 4), acc[l]);
+							tc::tmem_wait_ld();
+							if (!live) continue;
+#pragma unroll
+							for (int u = 0; u < 4; u++) {
+								const int n = pass * NC + ch * 4 + u;
+								if (n >= S::NPAIR) break;
+								const uint16_t off = rec[n];
+								if (off == kOffSkip) continue;
+								double t = (double) acc[NS - 1][u];
+#pragma unroll
+								for (int l = NS - 2; l >= 0; l--) t = fma(t, 0.0078125, (double) acc[l][u]);   // Horner in 2^-7
+								const double kv = ldexp(t, er + fex[n] - 14);
+								const int a2 = n / NX, a = n - a2 * NX;
+								const int i_ = (a * NY + b) * NZ + c, j_ = (a2 * NY + b2) * NZ + c2;
+								posted_add(args.Ax + cs[j_] + off, cc[i_] * cc[j_] * kv);
+							}
+						}
+					}
+					tc::fence_before_sync();
+					__syncthreads();
+				}
+			}
+		}
+	}
+	// never free TMEM under an MMA still in flight (only reachable after a timeout)
+	drain(0);
+	drain(1);
+	__syncthreads();
+	tc::fence_after_sync();
+	if (warp == 0) tc::tmem_dealloc(tmem, S::TMEM_COLS);
+}
+
+} // namespace h3dg

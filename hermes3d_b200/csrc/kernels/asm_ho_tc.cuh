@@ -90,7 +90,7 @@ struct HoTcShape {
 // its half with 16-byte loads.
 constexpr uint16_t kOffSkip = 0xFFFF;
 
-__global__ void k_build_offt(const uint16_t *offc, const int32_t *cdof, const int64_t *Ap, int64_t ne, int nx, int ny,
+static __global__ void k_build_offt(const uint16_t *offc, const int32_t *cdof, const int64_t *Ap, int64_t ne, int nx, int ny,
                              int nz, int nb, uint16_t *offt, int *status) {
 	const int nl = nx * ny * nz, ncol = ny * ny * nz;
 	const int64_t total = ne * nz * ncol * nb;

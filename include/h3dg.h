@@ -65,6 +65,12 @@ typedef int h3dg_status;
  * the high-order path; where the FP64 kernels are the faster choice (low
  * orders) the matrix is assembled in FP64. */
 #define H3DG_PREC_TF32X3  1
+/* FP64-accurate split (no reference counterpart): geometry, load vector,
+ * lifting and the z / y stages in FP64; the x stage on the tensor cores with
+ * each FP64 operand cut into 7 int8 slices (Ozaki-style), exact int32
+ * accumulation per slice level, recombined in FP64.  Relative error of the
+ * matrix below 1e-12.  High-order path; low orders assemble in FP64. */
+#define H3DG_PREC_OZAKI   2
 
 typedef struct h3dg_mesh h3dg_mesh;
 typedef struct h3dg_space h3dg_space;

@@ -1,10 +1,11 @@
-"""Split precision (PREC_TF32X3: FP64 geometry / load vector / lifting,
-FP32 z and y stages, 3xTF32 x stage on tcgen05) against the FP64 kernel,
-the reference fixtures and the restatement oracle.
-
-Tolerance: 1e-6 of the largest matrix entry, entrywise (max |dA| / max |A|),
-and 1e-6 normwise (||dA||_2 / ||A||_2).  The load vector is FP64 throughout,
-so it keeps the FP64 tolerance."""
+"""Split precision on tcgen05 against the FP64 kernel, the reference
+fixtures and the restatement oracle:
+  PREC_TF32X3: FP32 z and y stages, 3xTF32 x stage; tolerance 1e-6;
+  PREC_OZAKI:  FP64 z and y stages, x stage on int8 slices (7 per operand,
+               exact int32 accumulation); tolerance 1e-12.
+Tolerances are of the largest matrix entry, entrywise (max |dA| / max |A|),
+and normwise (||dA||_2 / ||A||_2).  The load vector is FP64 throughout, so
+it keeps the FP64 tolerance."""
 import os
 
 import numpy as np
@@ -17,6 +18,8 @@ from oracle import port
 pytestmark = pytest.mark.gpu
 
 SPLIT_RTOL = 1e-6
+TOL = {h.PREC_TF32X3: 1e-6, h.PREC_OZAKI: 1e-12}
+PRECS = [h.PREC_TF32X3, h.PREC_OZAKI]
 
 
 def _norm_err(a, b):
@@ -30,22 +33,24 @@ def force_high_order():
     del os.environ["H3DG_FORCE_HIGH_ORDER"]
 
 
+@pytest.mark.parametrize("prec", PRECS)
 @pytest.mark.parametrize("name", ["c1_small", "perm_p3_mass_sin", "perm_p2_lifting", "coef_p3"])
-def test_split_on_reference_fixtures(gpu, force_high_order, name):
+def test_split_on_reference_fixtures(gpu, force_high_order, name, prec):
     g = load(name)
     sp = space_of(g)
     d = disc_of(g, sp)
     M, V = h.UMFPackMatrix(), h.UMFPackVector()
     d.create(M, V)
-    d.assemble(M, V, precision=h.PREC_TF32X3)
+    d.assemble(M, V, precision=prec)
     e_max, e_norm = rel_err(M.Ax, g["Ax"]), _norm_err(M.Ax, g["Ax"])
-    print("%s: split error max %.2e norm %.2e" % (name, e_max, e_norm))
-    assert e_max < SPLIT_RTOL and e_norm < SPLIT_RTOL
+    print("%s prec %d: split error max %.2e norm %.2e" % (name, prec, e_max, e_norm))
+    assert e_max < TOL[prec] and e_norm < TOL[prec]
     assert rel_err(V.v, g["rhs"]) < FP64_RTOL
 
 
-@pytest.mark.parametrize("p,bc,n", [(5, "lifting", 2), (6, "dirichlet0", 2), (8, "natural", 1)])
-def test_split_matches_restatement(gpu, p, bc, n):
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("p,bc,n", [(5, "lifting", 2), (6, "dirichlet0", 2), (7, "lifting", 1), (8, "natural", 1)])
+def test_split_matches_restatement(gpu, p, bc, n, prec):
     mesh = h.permute_vertices(h.unit_cube(n, 0.15, 3), seed=p)
     mesh.ugh()
     sp = h.H1Space(mesh)
@@ -63,17 +68,18 @@ def test_split_matches_restatement(gpu, p, bc, n):
     d.set_quadrature(p_plus=2)
     M, V = h.UMFPackMatrix(), h.UMFPackVector()
     d.create(M, V)
-    d.assemble(M, V, precision=h.PREC_TF32X3)
+    d.assemble(M, V, precision=prec)
     al = port.asmlists_from_space(sp, mesh.num_elements)
     Ax, rhs = port.assemble(mesh.xyz, mesh.hexes - 1, p + 2, al, sp.ndof, M.Ap, M.Ai, mass=(bc != "dirichlet0"),
                             gradcoef=coef, lf=1 if bc == "lifting" else 2, lf_value=-6.0)
     e_max, e_norm = rel_err(M.Ax, Ax), _norm_err(M.Ax, Ax)
-    print("p=%d %s: split error max %.2e norm %.2e" % (p, bc, e_max, e_norm))
-    assert e_max < SPLIT_RTOL and e_norm < SPLIT_RTOL
+    print("p=%d %s prec %d: split error max %.2e norm %.2e" % (p, bc, prec, e_max, e_norm))
+    assert e_max < TOL[prec] and e_norm < TOL[prec]
     assert rel_err(V.v, rhs) < FP64_RTOL
 
 
-def test_split_is_deterministic_and_close_to_fp64(gpu):
+@pytest.mark.parametrize("prec", PRECS)
+def test_split_is_deterministic_and_close_to_fp64(gpu, prec):
     import torch
     mesh = h.unit_cube(3, 0.2, 11)
     mesh.ugh()
@@ -89,12 +95,13 @@ def test_split_is_deterministic_and_close_to_fp64(gpu):
     A64 = torch.empty(d.nnz, dtype=torch.float64, device="cuda")
     A1, A2 = torch.empty_like(A64), torch.empty_like(A64)
     d.assemble_device(A64)
-    d.assemble_device(A1, precision=h.PREC_TF32X3)
-    d.assemble_device(A2, precision=h.PREC_TF32X3)
+    d.assemble_device(A1, precision=prec)
+    d.assemble_device(A2, precision=prec)
     torch.cuda.synchronize()
     assert torch.equal(A1, A2)
     a, b = A1.cpu().numpy(), A64.cpu().numpy()
-    assert rel_err(a, b) < SPLIT_RTOL and _norm_err(a, b) < SPLIT_RTOL
+    print("prec %d vs FP64: max %.2e norm %.2e" % (prec, rel_err(a, b), _norm_err(a, b)))
+    assert rel_err(a, b) < TOL[prec] and _norm_err(a, b) < TOL[prec]
     # the split result is not the FP64 one (the tensor path really ran)
     assert not np.array_equal(a, b)
 
