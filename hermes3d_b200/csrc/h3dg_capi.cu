@@ -89,6 +89,7 @@ struct h3dg_disc {
 	DBuf<int32_t> Ai, el_vtx, el_cnt, el_dof, el_id;
 	DBuf<uint16_t> el_s, el_off, el_offc;
 	DBuf<uint16_t> el_offt;    // tensor-core scatter stream (built at the first split-precision assembly)
+	DBuf<double> ho_scratch;   // per-CTA global work area of the FP64-accurate split kernel
 	DBuf<int32_t> el_cdof;
 	DBuf<double> el_ccoef;
 	DBuf<double> el_coef;
@@ -558,6 +559,13 @@ static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, dou
 	int per_sm = 1;
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, k.smem);
 	if (per_sm < 1) per_sm = 1;
+	a.gscratch = nullptr;
+	if (precision == H3DG_PREC_OZAKI) {
+		// G of every resident CTA: 8 x points doubles each (L2-resident)
+		const size_t need = (size_t) nsm * per_sm * 8 * (size_t) P.nqx * P.nqy * P.nqz;
+		if (disc->ho_scratch.n < need) H3DG_CUDA_TRY(disc->ho_scratch.alloc(need));
+		a.gscratch = disc->ho_scratch.p;
+	}
 	const bool rec = disc->tn < disc->tcap;
 	if (rec) H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn], st));
 	int32_t launches = 0;
@@ -1033,6 +1041,9 @@ h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, doub
 	// everything h3dg_disc_assemble would allocate lazily must already exist
 	if (!disc->on_device || !disc->status.p)
 		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: device plan not uploaded; make one allocating assembly call first");
+	if (P.canon && precision == H3DG_PREC_OZAKI && Ax && !disc->ho_scratch.p && P.ne > 0)
+		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: split-precision work area not allocated; make one allocating "
+		                            "assembly call with this precision first");
 	if (P.canon && (precision == H3DG_PREC_TF32X3 || precision == H3DG_PREC_OZAKI) && Ax && !disc->el_offt.p && P.ne > 0)
 		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: split-precision scatter stream not built; make one allocating "
 		                            "split-precision assembly call first");

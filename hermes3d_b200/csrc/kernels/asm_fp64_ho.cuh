@@ -43,6 +43,7 @@ struct KArgsHO {
 	double lf_value;
 	double *Ax, *rhs;
 	int *status;
+	double *gscratch;          // per-CTA global work area (kernels that keep G out of shared memory), or nullptr
 };
 
 template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ>

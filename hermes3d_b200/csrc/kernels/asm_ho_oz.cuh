@@ -20,9 +20,11 @@
 // order K_dim 2^-49 of the row / column scales (measured ~1e-14, tolerance
 // 1e-12).
 //
-// Shared memory holds one V slice at a time (two buffers: slice i+1 is cut
-// from the FP64 values kept in registers while the MMAs of slice i run), so
-// the FP64 stage-1 products fit beside the constant E slices.  N (the (a',a)
+// The FP64 geometric factors G live in a per-CTA global work area (read from
+// L2 by stage 1), so shared memory holds the FP64 stage-1 products, the
+// constant E slices and all NS V slices of a tile: each tile is cut once
+// (one conversion to fixed point per value, digits by shifts) and each pass
+// issues all its MMAs behind one barrier and one commit.  N (the (a',a)
 // pairs, padded to 16) is covered in NPASS passes of NC columns so that the
 // NS level accumulators fit in TMEM (NS * NC <= 512).  The epilogue and the
 // scatter stream are those of the split-precision kernel (one CSC column per
@@ -55,18 +57,19 @@ struct HoOzShape {
 	static constexpr int O_TAB = 0;
 	static constexpr int O_BOP = ho_tc_align(O_TAB + 8 * B::TABP, 128);   // NS slices of NB x KD int8
 	static constexpr int BOP_SLICE = NB * KD;
-	static constexpr int O_FEX = O_BOP + NS * BOP_SLICE;                  // NB int: column exponents
-	static constexpr int O_G = ho_tc_align(O_FEX + 4 * NB, 128);         // 8 x NQ doubles
-	static constexpr int O_U = O_G + 8 * 8 * NQ;                          // union, see below
+	static constexpr int O_FEX = O_BOP + NS * BOP_SLICE;                  // NB doubles: column scales
+	static constexpr int O_U = ho_tc_align(O_FEX + 8 * NB, 128);         // union, see below
 	//   FP64 phase: matrix-free work (MF doubles)
 	//   matrix phase: T1 (T1D doubles), row maxima (2 x TM doubles), row exponents (TM int),
-	//                 two V slice buffers (TM x KD int8 each)
+	//                 the NS V slices of the tile (TM x KD int8 each)
+	// G (8 x NQ doubles) lives in a per-CTA global work area (L2-resident)
+	static constexpr int G_DOUBLES = 8 * NQ;
 	static constexpr int U_FP64 = 8 * B::MF;
 	static constexpr int R_RMX = 8 * T1D;
 	static constexpr int R_REX = R_RMX + 8 * 2 * TM;
 	static constexpr int R_ASL = ho_tc_align(R_REX + 4 * TM, 128);
 	static constexpr int ASL = TM * KD;
-	static constexpr int U_MAT = R_ASL + 2 * ASL;
+	static constexpr int U_MAT = R_ASL + NS * ASL;
 	static constexpr int O_X = O_U + ho_tc_align(ho_tc_max(U_FP64, U_MAT), 16);
 	static constexpr int O_M = O_X + 24 * 8;
 	static constexpr int O_C = O_M + 24 * 8;
@@ -119,10 +122,25 @@ __device__ __forceinline__ void ho_oz_stage1(const double *G, const double *tab,
 	}
 }
 
-// cut slice `i` of the scaled values r0 (|r0| < 1) and store it, int8,
-// K-major at row m of a TM-row operand; K padding stays zero
+// Fixed-point form of a scaled value r (|r| < 1): sign and M = trunc(|r| 2^49),
+// so that r = sign M 2^-49 + (|residual| < 2^-49) and slice i is the 7-bit
+// digit a_i = sign ((M >> (42 - 7 i)) & 127): one conversion per value,
+// every slice by shifts.
+__device__ __forceinline__ long long oz_fixed(double r) {
+	const long long mag = (long long) (fabs(r) * 562949953421312.0);   // 2^49, exact scaling
+	return r < 0.0 ? -mag : mag;
+}
+
+__device__ __forceinline__ int oz_digit(long long fx, int i) {
+	const long long mag = fx < 0 ? -fx : fx;
+	const int d = (int) ((mag >> (42 - 7 * i)) & 127);
+	return fx < 0 ? -d : d;
+}
+
+// store slice i of this thread's values, int8, K-major at row m of a TM-row
+// operand; K padding stays zero
 template <class S>
-__device__ __forceinline__ void ho_oz_put_slice(const double (&r0)[4][S::H0], int i, int m, int half, unsigned char *buf) {
+__device__ __forceinline__ void ho_oz_put_slice(const long long (&fx)[4][S::H0], int i, int m, int half, unsigned char *buf) {
 	using SB = typename S::B;
 	constexpr int NQX = SB::QX, H0 = S::H0, KD = S::KD, TM = S::TM;
 #pragma unroll
@@ -130,20 +148,14 @@ __device__ __forceinline__ void ho_oz_put_slice(const double (&r0)[4][S::H0], in
 #pragma unroll
 		for (int j = 0; j < H0; j++) {
 			const int q1 = j + half * H0;
-			if (q1 < NQX) {
-				double r = r0[f][j];
-				int a = 0;
-				for (int t = 0; t <= i; t++) {
-					r *= 128.0;
-					a = (int) r;                 // trunc: |a| <= 127
-					r -= (double) a;             // exact
-				}
-				buf[tc::kmaj_off8(m, f * NQX + q1, TM)] = (unsigned char) (int8_t) a;
-			}
+			if (q1 < NQX) buf[tc::kmaj_off8(m, f * NQX + q1, TM)] = (unsigned char) (int8_t) oz_digit(fx[f][j], i);
 		}
 	if (KD > 4 * NQX && half == 1)
 		for (int kq = 4 * NQX; kq < KD; kq++) buf[tc::kmaj_off8(m, kq, TM)] = 0;
 }
+
+// 2^e as a double (|e| well inside the normal range)
+__device__ __forceinline__ double oz_pow2(int e) { return __longlong_as_double((long long) (1023 + e) << 52); }
 
 template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ>
 __global__ void __launch_bounds__(256, 1) k_assemble_ho_oz(KArgsHO args, int64_t kbeg, int64_t kend) {
@@ -159,13 +171,13 @@ __global__ void __launch_bounds__(256, 1) k_assemble_ho_oz(KArgsHO args, int64_t
 
 	double *tab = reinterpret_cast<double *>(smb + S::O_TAB);
 	unsigned char *bop = smb + S::O_BOP;
-	int *fex = reinterpret_cast<int *>(smb + S::O_FEX);
-	double *G = reinterpret_cast<double *>(smb + S::O_G);
+	double *fsc = reinterpret_cast<double *>(smb + S::O_FEX);   // column scale 2^{e_col - 14}
+	double *G = args.gscratch + (size_t) blockIdx.x * S::G_DOUBLES;
 	double *MFw = reinterpret_cast<double *>(smb + S::O_U);
 	double *T1 = reinterpret_cast<double *>(smb + S::O_U);
 	double *rmx = reinterpret_cast<double *>(smb + S::O_U + S::R_RMX);
 	int *rex = reinterpret_cast<int *>(smb + S::O_U + S::R_REX);
-	unsigned char *asl = smb + S::O_U + S::R_ASL;          // buffer q at asl + q ASL
+	unsigned char *asl = smb + S::O_U + S::R_ASL;          // slice i at asl + i ASL
 	double *X = reinterpret_cast<double *>(smb + S::O_X), *Mo = reinterpret_cast<double *>(smb + S::O_M);
 	double *cc = reinterpret_cast<double *>(smb + S::O_C);
 	int64_t *cs = reinterpret_cast<int64_t *>(smb + S::O_CS), *ce = reinterpret_cast<int64_t *>(smb + S::O_CE);
@@ -193,17 +205,13 @@ __global__ void __launch_bounds__(256, 1) k_assemble_ho_oz(KArgsHO args, int64_t
 		for (int kq = 0; kq < 4 * NQX; kq++) mx = fmax(mx, fabs(eval_e(n, kq)));
 		int e = 0;
 		if (mx > 0.0) frexp(mx, &e);
-		fex[n] = e;
+		fsc[n] = oz_pow2(e - 14);
 #pragma unroll 1
 		for (int kq = 0; kq < KD; kq++) {
-			double r = ldexp(eval_e(n, kq), -e);
+			const long long fxv = oz_fixed(eval_e(n, kq) * oz_pow2(-e));
 #pragma unroll 1
-			for (int i = 0; i < NS; i++) {
-				r *= 128.0;
-				const int a = (int) r;
-				r -= (double) a;
-				bop[i * S::BOP_SLICE + tc::kmaj_off8(n, kq, NB)] = (unsigned char) (int8_t) a;
-			}
+			for (int i = 0; i < NS; i++)
+				bop[i * S::BOP_SLICE + tc::kmaj_off8(n, kq, NB)] = (unsigned char) (int8_t) oz_digit(fxv, i);
 		}
 	}
 	tc::fence_async_smem();
@@ -285,28 +293,29 @@ __global__ void __launch_bounds__(256, 1) k_assemble_ho_oz(KArgsHO args, int64_t
 				int erow = 0;
 				if (mx > 0.0) frexp(mx, &erow);
 				if (half == 0) rex[m] = erow;
+				long long FX[4][H0];                                 // fixed-point digits source, |V 2^-erow| < 1
+				{
+					const double sc = oz_pow2(-erow);
 #pragma unroll
-				for (int f = 0; f < 4; f++)
+					for (int f = 0; f < 4; f++)
 #pragma unroll
-					for (int j = 0; j < H0; j++) V[f][j] = ldexp(V[f][j], -erow);   // |V| < 1 now
+						for (int j = 0; j < H0; j++) FX[f][j] = oz_fixed(V[f][j] * sc);
+				}
 
+				// ---- the NS slices of this tile (the previous tile's MMAs are complete)
+#pragma unroll 1
+				for (int i = 0; i < NS; i++) ho_oz_put_slice<S>(FX, i, m, half, asl + i * S::ASL);
+				tc::fence_async_smem();
+				tc::fence_before_sync();
+				__syncthreads();
 				for (int pass = 0; pass < S::NPASS && alive; pass++) {
-					// ---- slices: cut slice i into buffer (step & 1), MMAs of all pairs (i, j <= NS-1-i)
-					for (int i = 0; i < NS; i++) {
-						const int q = i & 1;
-						if (!__syncthreads_and(drain(q) ? 1 : 0)) {
-							alive = false;
-							break;
-						}
-						unsigned char *buf = asl + q * S::ASL;
-						ho_oz_put_slice<S>(V, i, m, half, buf);
-						tc::fence_async_smem();
-						tc::fence_before_sync();
-						__syncthreads();
-						if (tid == 0) {
-							tc::fence_after_sync();
-							constexpr uint32_t idesc = tc::instr_desc_i8(TM, NC);
-							constexpr uint32_t lbo_a = (TM / 8) * 128, lbo_b = (NB / 8) * 128;
+					// ---- all pairs (i, j), i + j < NS, into the level accumulators of this pass
+					if (tid == 0) {
+						tc::fence_after_sync();
+						constexpr uint32_t idesc = tc::instr_desc_i8(TM, NC);
+						constexpr uint32_t lbo_a = (TM / 8) * 128, lbo_b = (NB / 8) * 128;
+						for (int i = 0; i < NS; i++) {
+							const unsigned char *buf = asl + i * S::ASL;
 							for (int j = 0; j + i < NS; j++) {
 								const unsigned char *pb = bop + j * S::BOP_SLICE + (pass * NC / 8) * 128;
 								const uint32_t dacc = tmem + (uint32_t) ((i + j) * NC);
@@ -317,15 +326,12 @@ __global__ void __launch_bounds__(256, 1) k_assemble_ho_oz(KArgsHO args, int64_t
 									tc::mma_i8(dacc, da, db, idesc, i > 0 || s > 0);
 								}
 							}
-							tc::mma_commit(&bar_mma[q]);
 						}
-						if (q) iss1++;
-						else iss0++;
+						tc::mma_commit(&bar_mma[0]);
 					}
-					if (!alive) break;
+					iss0++;
 					// ---- all levels of this pass complete
-					bool ok = drain(0);
-					ok = drain(1) && ok;
+					const bool ok = drain(0);
 					if (!__syncthreads_and(ok ? 1 : 0)) {
 						alive = false;
 						break;
@@ -337,7 +343,7 @@ __global__ void __launch_bounds__(256, 1) k_assemble_ho_oz(KArgsHO args, int64_t
 						const int colr = tt * TM + mrow;
 						const bool live = colr < S::NCOL;
 						const int b2 = live ? colr / (NY * NZ) : 0, b = live ? (colr / NZ) % NY : 0, c = live ? colr % NZ : 0;
-						const int er = rex[mrow];
+						const double rsc = oz_pow2(rex[mrow]);
 						const uint16_t *rec = offe + ((size_t) c2 * S::NCOL + (live ? colr : 0)) * NB;
 						const uint32_t tl = tmem + ((uint32_t) (quarter * 32) << 16);
 						constexpr int NCH4 = NC / 4;                      // 4-column chunks
@@ -358,7 +364,7 @@ __global__ void __launch_bounds__(256, 1) k_assemble_ho_oz(KArgsHO args, int64_t
 								double t = (double) acc[NS - 1][u];
 #pragma unroll
 								for (int l = NS - 2; l >= 0; l--) t = fma(t, 0.0078125, (double) acc[l][u]);   // Horner in 2^-7
-								const double kv = ldexp(t, er + fex[n] - 14);
+								const double kv = t * rsc * fsc[n];           // exact power-of-two scalings
 								const int a2 = n / NX, a = n - a2 * NX;
 								const int i_ = (a * NY + b) * NZ + c, j_ = (a2 * NY + b2) * NZ + c2;
 								posted_add(args.Ax + cs[j_] + off, cc[i_] * cc[j_] * kv);
