@@ -179,3 +179,35 @@ def test_every_kernel_variant_is_bitwise_identical(gpu, monkeypatch, p, nq):
             assert rel_err(M.Ax, Ax) < FP64_RTOL and rel_err(V.v, rhs) < FP64_RTOL
         else:
             assert np.array_equal(M.Ax, ref[0]) and np.array_equal(V.v, ref[1]), v
+
+
+@pytest.mark.parametrize("name", ["hex1", "hex2", "hex4", "hex8", "hex27"])
+def test_geometry_kernel_matches_reference_refmap_dumps(gpu, name):
+    """k_geometry against the reference's own RefMap known answers
+    (tests/refmap/dump/*.dump via tests/golden/kat/refmap_dumps.npz): Jacobian
+    determinant, transposed inverse map and physical points at the 2x2x2
+    Gauss points, printed to 6 decimals by the reference."""
+    import os
+    import torch
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "kat", "refmap_dumps.npz"))
+    mesh = h.Mesh().set_arrays(z[name + "_xyz"], z[name + "_hexes"], z[name + "_bquads"], z[name + "_bmarkers"])
+    mesh.ugh()
+    sp = h.H1Space(mesh)
+    sp.set_bc_types(lambda m: h.BC_NATURAL)
+    sp.set_uniform_order(1)
+    sp.assign_dofs()
+    d = h.Discretization()
+    d.set_spaces(sp)
+    d.set_bilinear_form(h.int_grad_u_grad_v)
+    d.set_quadrature(points=2)
+    d.create()
+    ne, nq = mesh.num_elements, 8
+    jac = torch.zeros(ne * nq, dtype=torch.float64, device="cuda")
+    irm = torch.zeros(ne * nq * 9, dtype=torch.float64, device="cuda")
+    xyz = torch.zeros(ne * nq * 3, dtype=torch.float64, device="cuda")
+    d.geometry(jac, irm, xyz)
+    torch.cuda.synchronize()
+    tol = 1.5e-6                                  # 6 printed decimals
+    assert np.max(np.abs(jac.cpu().numpy().reshape(ne, nq) - z[name + "_jac"])) < tol
+    assert np.max(np.abs(irm.cpu().numpy().reshape(ne, nq, 3, 3) - z[name + "_irm"])) < tol
+    assert np.max(np.abs(xyz.cpu().numpy().reshape(ne, nq, 3) - z[name + "_phys"])) < tol

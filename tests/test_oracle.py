@@ -61,3 +61,15 @@ def test_reference_driver_reproduces_golden():
     r = ref_driver.run(mesh, **g["params"])
     assert np.array_equal(r["Ap"], g["Ap"]) and np.array_equal(r["Ai"], g["Ai"])
     assert np.array_equal(r["Ax"], g["Ax"]) and np.array_equal(r["rhs"], g["rhs"])
+
+
+def test_refmap_fixture_is_consistent():
+    """The reference's RefMap dumps (fixture) are self-consistent: irm is the
+    transposed inverse of the printed Jacobian matrix (to 6 decimals)."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "kat", "refmap_dumps.npz"))
+    for name in ["hex1", "hex2", "hex4", "hex8", "hex27"]:
+        rm, irm = z[name + "_rm"], z[name + "_irm"]
+        prod = np.einsum("eqrc,eqrd->eqcd", irm, rm)      # irm^T rm = I  (irm = J^-T)
+        assert np.allclose(prod, np.eye(3), atol=2e-5), name
+        assert np.allclose(np.linalg.det(rm), z[name + "_jac"], atol=2e-5), name
