@@ -297,6 +297,74 @@ def run_adjoint(args):
     return 0
 
 
+def run_sweep(args):
+    """Orders p = 1..8 (p+2 points per direction, jittered cube, a_e grad.grad,
+    32^3 elements for p <= 4, 16^3 above): elements/s of the FP64 path (the
+    kernel the library picks: low-order kernels up to p = 4, the high-order
+    kernel above) against the two tensor-core split precisions (forced onto
+    the high-order path at every order), with each split result's error
+    against the FP64 matrix.  One JSON line; not the headline."""
+    import numpy as np
+    import torch
+    import hermes3d_b200 as h
+    torch.cuda.set_device(0)
+    rows = []
+    for p in range(1, 9):
+        side = args.side or (32 if p <= 4 else 16)
+        rec = {"p": p, "elements": side ** 3}
+        ref = None
+        for name, prec, force in [("fp64", h.PREC_FP64, False), ("tf32x3", h.PREC_TF32X3, True),
+                                  ("ozaki", h.PREC_OZAKI, True)]:
+            if force:
+                os.environ["H3DG_FORCE_HIGH_ORDER"] = "1"
+            try:
+                mesh = h.unit_cube(side, 0.2, 0)
+                mesh.ugh()
+                sp = h.H1Space(mesh)
+                sp.set_uniform_order(p)
+                sp.assign_dofs()
+                d = h.Discretization(0)
+                d.set_spaces(sp)
+                d.set_bilinear_form(h.int_grad_u_grad_v, np.random.default_rng(0).uniform(0.5, 2.0, side ** 3))
+                d.set_linear_form(None)
+                d.set_quadrature(p_plus=2)
+                d.create()
+            finally:
+                os.environ.pop("H3DG_FORCE_HIGH_ORDER", None)
+            A = torch.empty(d.nnz, dtype=torch.float64, device="cuda")
+            for _ in range(max(3, args.warmup)):
+                d.assemble_device(A, None, precision=prec)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(args.steps):
+                d.assemble_device(A, None, precision=prec)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+            rec[name + "_ms"] = ms
+            rec[name + "_elements_per_s"] = side ** 3 / (ms * 1e-3)
+            if ref is None:
+                ref = A
+            else:
+                diff = A - ref
+                rec[name + "_err_max_over_max"] = float(diff.abs().max() / ref.abs().max())
+                rec[name + "_err_frobenius"] = float(torch.linalg.vector_norm(diff) / torch.linalg.vector_norm(ref))
+                del diff
+                rec[name + "_speedup_vs_fp64"] = rec["fp64_ms"] / ms
+                del A
+            del d
+            torch.cuda.empty_cache()
+        del ref
+        torch.cuda.empty_cache()
+        rows.append(rec)
+        print(json.dumps(rec), file=sys.stderr, flush=True)
+    print(json.dumps({"metric": "hp assembly elements/s by order: FP64 vs split precision (3xTF32 <= 1e-6, "
+                                "int8-sliced Ozaki <= 1e-12)", "unit": "elements/s", "n_gpus": 1, "steps": args.steps,
+                      "data": "synthetic (jittered unit cube, a_e ~ U[0.5,2], seed 0)", "sweep": rows}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -313,11 +381,14 @@ def main():
                     help="tf32x3 / ozaki: split precision on tcgen05 (3xTF32, or int8 slices with FP64 accuracy); "
                          "high-order path")
     ap.add_argument("--adjoint", action="store_true", help="C5 adjoint line (16 fields) instead of an assembly line")
+    ap.add_argument("--sweep", action="store_true", help="orders 1..8: FP64 against both split precisions")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.adjoint:
         return run_adjoint(args)
+    if args.sweep:
+        return run_sweep(args)
 
     import numpy as np
     import torch

@@ -11,7 +11,7 @@ static HoSpec ho_spec() {
 
 std::vector<HoSpec> &ho_table() {
 	static std::vector<HoSpec> t = {
-		ho_spec<2, 4, 128>(), ho_spec<3, 5, 256>(),
+		ho_spec<1, 3, 128>(), ho_spec<2, 4, 128>(), ho_spec<3, 5, 256>(), ho_spec<4, 6, 256>(),
 		ho_spec<5, 6, 256>(), ho_spec<5, 7, 256>(), ho_spec<6, 7, 256>(), ho_spec<6, 8, 256>(),
 		ho_spec<7, 8, 256>(), ho_spec<7, 9, 256>(), ho_spec<8, 9, 256>(), ho_spec<8, 10, 256>(),
 		ho_spec<8, 10, 384>(),

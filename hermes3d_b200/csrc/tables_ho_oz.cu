@@ -12,7 +12,7 @@ static HoSpec ho_oz_spec() {
 
 std::vector<HoSpec> &ho_oz_table() {
 	static std::vector<HoSpec> t = {
-		ho_oz_spec<2, 4>(), ho_oz_spec<3, 5>(), ho_oz_spec<5, 6>(), ho_oz_spec<5, 7>(), ho_oz_spec<6, 7>(),
+		ho_oz_spec<1, 3>(), ho_oz_spec<2, 4>(), ho_oz_spec<3, 5>(), ho_oz_spec<4, 6>(), ho_oz_spec<5, 6>(), ho_oz_spec<5, 7>(), ho_oz_spec<6, 7>(),
 		ho_oz_spec<6, 8>(), ho_oz_spec<7, 8>(), ho_oz_spec<7, 9>(), ho_oz_spec<8, 9>(), ho_oz_spec<8, 10>(),
 	};
 	return t;

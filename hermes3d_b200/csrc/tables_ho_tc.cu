@@ -12,7 +12,7 @@ static HoSpec ho_tc_spec() {
 
 std::vector<HoSpec> &ho_tc_table() {
 	static std::vector<HoSpec> t = {
-		ho_tc_spec<2, 4>(), ho_tc_spec<3, 5>(), ho_tc_spec<5, 6>(), ho_tc_spec<5, 7>(), ho_tc_spec<6, 7>(),
+		ho_tc_spec<1, 3>(), ho_tc_spec<2, 4>(), ho_tc_spec<3, 5>(), ho_tc_spec<4, 6>(), ho_tc_spec<5, 6>(), ho_tc_spec<5, 7>(), ho_tc_spec<6, 7>(),
 		ho_tc_spec<6, 8>(), ho_tc_spec<7, 8>(), ho_tc_spec<7, 9>(), ho_tc_spec<8, 9>(), ho_tc_spec<8, 10>(),
 	};
 	return t;
