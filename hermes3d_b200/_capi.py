@@ -76,6 +76,7 @@ SIGNATURES = {
     "h3dg_tc_selftest": [C.c_int, _p, _p, _p, C.c_int],
     "h3dg_disc_assemble_host_noalloc": [_p, C.c_int, _p, _p],
     "h3dg_disc_set_partition": [_p, C.c_int, C.c_int],
+    "h3dg_disc_set_precision": [_p, C.c_int],
     "h3dg_disc_get_partition": [_p, _p, _p, _p, _p],
     "h3dg_disc_get_partition_elements": [_p, _p, C.c_int64],
     "h3dg_disc_enable_kernel_timing": [_p, _i32],

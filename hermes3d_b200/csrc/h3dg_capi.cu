@@ -77,6 +77,7 @@ struct h3dg_disc {
 	bool have_plan = false;
 	bool on_device = false;
 	int nparts = 1, part = 0;  // z-slab partition of the next plan (1: whole mesh)
+	int prec_hint = H3DG_PREC_FP64;   // precision the next plan is built for
 	h3dg::PlanScope scope;     // element subset and owned DOFs of the current plan's part
 	int variant = -1;          // autotuned kernel variant (index into the kernel table)
 	float variant_ms = 0.0f;
@@ -373,7 +374,9 @@ h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nn
 	// H3DG_FORCE_HIGH_ORDER=1 routes every order through the high-order kernel
 	// (used by the parity tests to check that kernel on the low-order fixtures)
 	const char *force = std::getenv("H3DG_FORCE_HIGH_ORDER");
-	const bool canon = pmax >= 5 || (force && force[0] == '1');
+	// with 3xTF32 intended, the tensor-core kernel is already the faster one at p = 4
+	const int canon_from = disc->prec_hint == H3DG_PREC_TF32X3 ? 4 : 5;
+	const bool canon = pmax >= canon_from || (force && force[0] == '1');
 	// elements of different order triples: the mixed-order (batched) path;
 	// H3DG_FORCE_MIXED=1 routes uniform spaces there too (parity tests)
 	bool mixed = false;
@@ -454,6 +457,14 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 	H3DG_CUDA_TRY(disc->status.alloc(1));
 	H3DG_CUDA_TRY(cudaMemset(disc->status.p, 0, sizeof(int)));
 	disc->on_device = true;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_set_precision(h3dg_disc *disc, int precision) {
+	if (!disc || (precision != H3DG_PREC_FP64 && precision != H3DG_PREC_TF32X3 && precision != H3DG_PREC_OZAKI))
+		return fail(H3DG_ERR_INVALID_ARG, "set_precision: unknown precision");
+	disc->prec_hint = precision;
+	disc->have_plan = false;
 	return H3DG_OK;
 }
 

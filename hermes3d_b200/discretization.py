@@ -193,6 +193,11 @@ class Discretization:
             self._quad = (capi.QUAD_P_PLUS, int(p_plus))
         capi.call("h3dg_disc_set_quadrature", self.handle, *self._quad)
 
+    def set_precision(self, precision: int):
+        """Precision the next ``create`` plans for (no reference counterpart):
+        with PREC_TF32X3 order-4 spaces already take the tensor-core path."""
+        capi.call("h3dg_disc_set_precision", self.handle, int(precision))
+
     def set_partition(self, nparts: int, part: int):
         """Multi-GPU sharding without communication (no reference
         counterpart): the next ``create`` builds part ``part`` of ``nparts``

@@ -134,6 +134,11 @@ h3dg_status h3dg_disc_set_quadrature(h3dg_disc *disc, int mode, int n);
 /* Discretization::create (src/discretization.cc:164-230) + UMFPackMatrix::alloc
  * (src/linsolver/umfpack.cc:46-71): builds the CSC pattern and the device plan */
 h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nnz);
+/* No reference counterpart: the precision the next create_pattern plans for.
+ * With H3DG_PREC_TF32X3 the plan takes the high-order (tensor-core capable)
+ * form from order 4 up instead of 5, where the 3xTF32 kernel is already the
+ * faster one; assemble's precision argument still selects the arithmetic. */
+h3dg_status h3dg_disc_set_precision(h3dg_disc *disc, int precision);
 /* No reference counterpart (multi-GPU sharding, one process per GPU): build
  * the next plan for part `part` of `nparts` z-slabs of the mesh.  The part
  * assembles its slab of elements plus the one-element halo that touches its

@@ -119,3 +119,31 @@ def test_split_low_order_uses_fp64(gpu):
     d.create(M2, V2)
     d.assemble(M2, V2)
     assert np.array_equal(M.Ax, M2.Ax)
+
+
+def test_precision_hint_puts_order_4_on_the_tensor_cores(gpu):
+    """set_precision(PREC_TF32X3) before create(): p = 4 takes the tensor-core
+    kernel (faster there), still within 1e-6 of the FP64 assembly."""
+    def build(hint):
+        mesh = h.unit_cube(3, 0.2, 4)
+        mesh.ugh()
+        sp = h.H1Space(mesh)
+        sp.set_uniform_order(4)
+        sp.assign_dofs()
+        d = h.Discretization()
+        d.set_spaces(sp)
+        d.set_bilinear_form(h.int_grad_u_grad_v)
+        d.set_linear_form(h.int_F_v(1.0))
+        d.set_quadrature(points=6)
+        if hint is not None:
+            d.set_precision(hint)
+        M, V = h.UMFPackMatrix(), h.UMFPackVector()
+        d.create(M, V)
+        return d, M, V
+    d64, M64, V64 = build(None)
+    d64.assemble(M64, V64)
+    d, M, V = build(h.PREC_TF32X3)
+    d.assemble(M, V, precision=h.PREC_TF32X3)
+    assert np.array_equal(M.Ap, M64.Ap) and np.array_equal(M.Ai, M64.Ai)
+    assert rel_err(M.Ax, M64.Ax) < SPLIT_RTOL and not np.array_equal(M.Ax, M64.Ax)
+    assert rel_err(V.v, V64.v) < FP64_RTOL
