@@ -70,6 +70,7 @@ SIGNATURES = {
     "h3dg_disc_assemble_host": [_p, C.c_int, _pd, _pd],
     "h3dg_disc_update_vertices": [_p, _pd, _i64],
     "h3dg_disc_update_coefficients": [_p, _pd, _i64],
+    "h3dg_disc_update_coefficients_device": [_p, _p, _i64, _p],
     "h3dg_disc_last_launch_count": [_p, _pi32],
     "h3dg_disc_geometry": [_p, _p, _p, _p, _p],
     "h3dg_disc_adjoint": [_p, C.c_int, _p, _p, _p, _p, _p, _p],

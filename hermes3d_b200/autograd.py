@@ -22,7 +22,8 @@ def _csr_transpose_matvec(disc, Ax, x):
     """y = A^T x for the CSC matrix (Ap, Ai, Ax): the CSC arrays of A are the CSR arrays of A^T."""
     crow = disc._Ap_dev
     col = disc._Ai_dev
-    AT = torch.sparse_csr_tensor(crow, col, Ax, size=(disc.ndof, disc.ndof), dtype=torch.float64)
+    AT = torch.sparse_csr_tensor(crow, col, Ax, size=(disc.ndof, disc.ndof), dtype=torch.float64,
+                                 check_invariants=False)
     return AT @ x
 
 
@@ -44,8 +45,8 @@ def energy(disc, g, u, lam):
     rhs = torch.empty(disc.ndof, dtype=torch.float64, device=dev)
     out = torch.empty(nf, dtype=torch.float64, device=dev)
     for k in range(nf):
-        torch.cuda.current_stream(dev).synchronize()
-        disc.update_coefficients(torch.exp(g[k]).double().cpu().numpy())
+        a = torch.exp(g[k]).double()
+        disc.update_coefficients_device(a)          # stream-ordered, no host round trip
         disc.assemble_device(Ax, rhs)
         ATl = _csr_transpose_matvec(disc, Ax, lam[k])
         out[k] = torch.dot(ATl, u[k]) - torch.dot(lam[k], rhs)

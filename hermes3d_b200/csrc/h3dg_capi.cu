@@ -109,6 +109,7 @@ struct h3dg_disc {
 	int mx_variant[h3dg::Plan::kClasses] = { -1, -1, -1 };
 	cudaGraphExec_t mx_exec = nullptr;
 	double *mx_ax = nullptr, *mx_rhs = nullptr;
+	const double *mx_coef = nullptr;   // coefficient array the graph was captured with
 	int32_t mx_launches = 0;
 	cudaStream_t mx_s[2] = { nullptr, nullptr };
 	cudaEvent_t mx_ev[3] = { nullptr, nullptr, nullptr };
@@ -720,7 +721,7 @@ static h3dg_status assemble_mixed(h3dg_disc *disc, double *d_Ax, double *d_rhs, 
 		if (s != H3DG_OK) return s;
 	}
 	else {
-		if (!disc->mx_exec || disc->mx_ax != d_Ax || disc->mx_rhs != d_rhs) {
+		if (!disc->mx_exec || disc->mx_ax != d_Ax || disc->mx_rhs != d_rhs || disc->mx_coef != disc->coef.p) {
 			if (disc->mx_exec) cudaGraphExecDestroy(disc->mx_exec);
 			disc->mx_exec = nullptr;
 			for (auto &s : disc->mx_s)
@@ -747,6 +748,7 @@ static h3dg_status assemble_mixed(h3dg_disc *disc, double *d_Ax, double *d_rhs, 
 			}
 			disc->mx_ax = d_Ax;
 			disc->mx_rhs = d_rhs;
+			disc->mx_coef = disc->coef.p;
 		}
 		if (rec) H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn], st));
 		H3DG_CUDA_TRY(cudaGraphLaunch(disc->mx_exec, st));
@@ -1108,6 +1110,16 @@ h3dg_status h3dg_disc_update_coefficients(h3dg_disc *disc, const double *elem_co
 	if (disc->coef.n != (size_t) ne) H3DG_CUDA_TRY(disc->coef.alloc(ne));
 	H3DG_CUDA_TRY(cudaMemcpy(disc->coef.p, elem_coef, sizeof(double) * ne, cudaMemcpyHostToDevice));
 	disc->ecoef.assign(elem_coef, elem_coef + ne);
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_update_coefficients_device(h3dg_disc *disc, const double *d_elem_coef, int64_t ne, void *stream) {
+	if (!disc || !disc->have_plan || !d_elem_coef || ne != disc->plan.ne)
+		return fail(H3DG_ERR_INVALID_ARG, "update_coefficients_device: bad arguments or no plan");
+	{ h3dg_status s0 = ensure_device(disc); if (s0 != H3DG_OK) return s0; }
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	if (disc->coef.n != (size_t) ne) H3DG_CUDA_TRY(disc->coef.alloc(ne));
+	H3DG_CUDA_TRY(cudaMemcpyAsync(disc->coef.p, d_elem_coef, sizeof(double) * ne, cudaMemcpyDeviceToDevice, (cudaStream_t) stream));
 	return H3DG_OK;
 }
 

@@ -310,6 +310,16 @@ class Discretization:
         a = np.ascontiguousarray(coef, dtype=np.float64)
         capi.call("h3dg_disc_update_coefficients", self.handle, capi.ptr(a, C.c_double), len(a))
 
+    def update_coefficients_device(self, coef, stream=None):
+        """Per-element coefficients from a CUDA float64 tensor (element-id
+        order), ordered on ``stream``; no host round trip."""
+        import torch
+        coef = coef.contiguous()
+        if stream is None:
+            stream = torch.cuda.current_stream(coef.device)
+        capi.call("h3dg_disc_update_coefficients_device", self.handle, C.c_void_p(coef.data_ptr()), coef.numel(),
+                  C.c_void_p(stream.cuda_stream))
+
     def enable_kernel_timing(self, n):
         capi.call("h3dg_disc_enable_kernel_timing", self.handle, int(n))
 

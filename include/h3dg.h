@@ -184,6 +184,9 @@ h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, doub
 h3dg_status h3dg_disc_update_vertices(h3dg_disc *disc, const double *xyz, int64_t nv);
 /* replace the per-element coefficient (ne values, element-id order) from host memory */
 h3dg_status h3dg_disc_update_coefficients(h3dg_disc *disc, const double *elem_coef, int64_t ne);
+/* the same from device memory, ordered on `stream` (no host copy, no
+ * synchronisation; the host-side copy of the coefficients is not updated) */
+h3dg_status h3dg_disc_update_coefficients_device(h3dg_disc *disc, const double *d_elem_coef, int64_t ne, void *stream);
 /* number of kernels launched by the last assemble call */
 h3dg_status h3dg_disc_last_launch_count(const h3dg_disc *disc, int32_t *count);
 

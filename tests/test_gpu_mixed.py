@@ -94,3 +94,31 @@ def test_mixed_replay_is_bitwise_reproducible(gpu):
     torch.cuda.synchronize()
     assert torch.equal(A1, A2) and torch.equal(b1, b2)
     assert d.last_launch_count() >= 1
+
+
+def test_mixed_graph_follows_coefficient_updates(gpu):
+    """The replayed graph must see coefficients set after its capture, from
+    host or device memory."""
+    import torch
+    mesh = h.unit_cube(3, 0.2, 6)
+    mesh.ugh()
+    sp = h.H1Space(mesh)
+    sp.set_element_orders(_random_orders(mesh.num_elements, 8))
+    sp.assign_dofs()
+    d = h.Discretization()
+    d.set_spaces(sp)
+    d.set_bilinear_form(h.int_grad_u_grad_v)
+    d.set_linear_form(None)
+    d.set_quadrature(p_plus=2)
+    d.create()
+    A = torch.empty(d.nnz, dtype=torch.float64, device="cuda")
+    d.assemble_device(A)
+    base = A.clone()
+    d.update_coefficients_device(torch.full((mesh.num_elements,), 2.0, dtype=torch.float64, device="cuda"))
+    d.assemble_device(A)
+    torch.cuda.synchronize()
+    assert torch.allclose(A, 2.0 * base, rtol=1e-14, atol=0)
+    d.update_coefficients(np.full(mesh.num_elements, 3.0))
+    d.assemble_device(A)
+    torch.cuda.synchronize()
+    assert torch.allclose(A, 3.0 * base, rtol=1e-14, atol=0)
