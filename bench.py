@@ -264,14 +264,16 @@ def run_adjoint(args):
         out.copy_(gr, non_blocking=True)
         torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - c0) * 1e3 / nrep
-    # forward (16 assemblies through the torch.autograd binding) + backward, for context
-    gg = g.clone().requires_grad_(True)
-    torch.cuda.synchronize()
-    c0 = time.perf_counter()
-    L = hag.assembly_energy(gg, u, lam, d)
-    L.sum().backward()
-    torch.cuda.synchronize()
-    fb_ms = (time.perf_counter() - c0) * 1e3
+    # forward (16 assemblies through the torch.autograd binding) + backward, for context;
+    # the first call also uploads the pattern for the transposed products (not timed)
+    for rep in range(2):
+        gg = g.clone().requires_grad_(True)
+        torch.cuda.synchronize()
+        c0 = time.perf_counter()
+        L = hag.assembly_energy(gg, u, lam, d)
+        L.sum().backward()
+        torch.cuda.synchronize()
+        fb_ms = (time.perf_counter() - c0) * 1e3
     hbm, peak_kind = peaks()
     B = 2 * 8 * nf * ndof + 3 * 8 * nf * ne + 24 * mesh.num_vertices + 32 * ne
     achieved = B / (ms * 1e-3) / 1e9
