@@ -94,7 +94,12 @@ static __device__ __constant__ int kT1Flags[6][3] = {
 	{ 3, 0, 0 }, { 0, 3, 0 }, { 0, 0, 3 }, { 2, 1, 0 }, { 2, 0, 1 }, { 0, 2, 1 }
 };
 
-template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ, int NT, int EB, int MINB>
+// PF: software prefetch.  The plan data of the CTA's next batch (position
+// map, DOFs, coefficients, shape indices, column bounds, vertex coordinates)
+// are loaded into registers while the current batch is being computed, so
+// their global-memory latency overlaps the arithmetic; the arithmetic itself
+// is unchanged (bitwise identical results).
+template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ, int NT, int EB, int MINB, bool PF = false>
 __global__ void __launch_bounds__(NT, MINB) k_assemble_fp64(KArgs args, int64_t kbeg, int64_t kend) {
 	using S = SfShape<PX, PY, PZ, NQX, NQY, NQZ, EB>;
 	constexpr int NX = S::NX, NY = S::NY, NZ = S::NZ, NL = S::NL, NQ = S::NQ;
@@ -135,33 +140,125 @@ __global__ void __launch_bounds__(NT, MINB) k_assemble_fp64(KArgs args, int64_t 
 
 	const bool do_rhs = args.rhs && args.lf;
 	const int64_t nbatch = (kend - kbeg + EB - 1) / EB;
+
+	// prefetch registers (PF): per thread its share of the batch's items
+	constexpr int UOFF = PF ? (EB * NL2 + NT - 1) / NT : 1;   // position-map entries
+	constexpr int VEL = PF ? (EB * NL + NT - 1) / NT : 1;     // functions
+	constexpr int VX = PF ? (EB * 24 + NT - 1) / NT : 1;      // vertex coordinates
+	uint16_t off_n[UOFF], off_c[UOFF];
+	int dof_n[VEL], vtx_n[VX], m_n = 0, l_n = 0, id_n = 0;
+	double coef_n[VEL], x_n[VX], cg_n = 1.0;
+	uint16_t s_n[VEL];
+	int64_t cs_n[VEL], ce_n[VEL];
+	// first-level loads of batch bt (no dependent addresses)
+	auto prefetch1 = [&](int64_t bt) {
+		const int64_t k0 = kbeg + bt * EB;
+		const int ne = (int) (kend - k0 < EB ? kend - k0 : EB);
+#pragma unroll
+		for (int u = 0; u < UOFF; u++) {
+			const int p = tid + u * NT;
+			off_n[u] = p < ne * NL2 ? args.el_off[k0 * NL2 + p] : (uint16_t) 0;
+		}
+#pragma unroll
+		for (int v = 0; v < VEL; v++) {
+			const int i = tid + v * NT, e = i / NL, j = i % NL;
+			const bool live = i < EB * NL && e < ne;
+			const int64_t g = (k0 + e) * NL + j;
+			dof_n[v] = live ? args.el_dof[g] : -1;
+			coef_n[v] = live ? args.el_coef[g] : 0.0;
+			s_n[v] = live ? args.el_s[g] : (uint16_t) 0;
+		}
+#pragma unroll
+		for (int v = 0; v < VX; v++) {
+			const int i = tid + v * NT, e = i / 24, r = i % 24;
+			vtx_n[v] = i < EB * 24 && e < ne ? args.el_vtx[8 * (k0 + e) + r / 3] : -1;
+		}
+		if (tid < EB) {
+			const bool live = tid < ne;
+			m_n = live ? args.el_cnt[2 * (k0 + tid)] : 0;
+			l_n = live ? args.el_cnt[2 * (k0 + tid) + 1] : 0;
+			id_n = live ? args.el_id[k0 + tid] : -1;
+		}
+	};
+	// second-level loads (addresses from the first level)
+	auto prefetch2 = [&]() {
+#pragma unroll
+		for (int v = 0; v < VEL; v++) {
+			cs_n[v] = dof_n[v] >= 0 ? args.Ap[dof_n[v]] : 0;
+			ce_n[v] = dof_n[v] >= 0 ? args.Ap[dof_n[v] + 1] : 0;
+		}
+#pragma unroll
+		for (int v = 0; v < VX; v++) {
+			const int r = (tid + v * NT) % 24;
+			x_n[v] = vtx_n[v] >= 0 ? args.xyz[3 * (int64_t) vtx_n[v] + r % 3] : 0.0;
+		}
+		if (tid < EB) cg_n = id_n >= 0 && args.ecoef ? args.ecoef[id_n] : 1.0;
+	};
+	if (PF && (int64_t) blockIdx.x < nbatch) {
+		prefetch1(blockIdx.x);
+		prefetch2();
+	}
+
 	for (int64_t bt = blockIdx.x; bt < nbatch; bt += gridDim.x) {
 		const int64_t k0 = kbeg + bt * EB;
 		const int ne = (int) (kend - k0 < EB ? kend - k0 : EB);
 
 		// ---- element data
-		if (tid < EB) {
-			const bool live = tid < ne;
-			s_m[tid] = live ? args.el_cnt[2 * (k0 + tid)] : 0;
-			s_l[tid] = live ? args.el_cnt[2 * (k0 + tid) + 1] : 0;
-			s_cg[tid] = live && args.ecoef ? args.ecoef[args.el_id[k0 + tid]] : 1.0;
+		if (PF) {
+			// this batch's data are in the prefetch registers; start the next batch's loads
+			if (tid < EB) {
+				s_m[tid] = m_n;
+				s_l[tid] = l_n;
+				s_cg[tid] = cg_n;
+			}
+#pragma unroll
+			for (int v = 0; v < VX; v++) {
+				const int i = tid + v * NT;
+				if (i < EB * 24) E0[(i / 24) * S::E_SIZE + S::E_X + i % 24] = x_n[v];
+			}
+#pragma unroll
+			for (int v = 0; v < VEL; v++) {
+				const int i = tid + v * NT;
+				if (i < EB * NL) {
+					const int e = i / NL, j = i % NL;
+					double *Eb = E0 + e * S::E_SIZE;
+					int *ei = reinterpret_cast<int *>(Eb + S::E_I);
+					int64_t *cs = reinterpret_cast<int64_t *>(Eb + S::E_CS);
+					Eb[S::E_C + j] = coef_n[v];
+					ei[j] = dof_n[v];
+					ei[NL + j] = s_n[v];
+					cs[j] = cs_n[v];
+					cs[NL + j] = ce_n[v];
+				}
+			}
+#pragma unroll
+			for (int u = 0; u < UOFF; u++) off_c[u] = off_n[u];
+			if (bt + gridDim.x < nbatch) prefetch1(bt + gridDim.x);
 		}
-		for (int i = tid; i < EB * 24; i += NT) {
-			const int e = i / 24, r = i % 24;
-			E0[e * S::E_SIZE + S::E_X + r] = e < ne ? args.xyz[3 * (int64_t) args.el_vtx[8 * (k0 + e) + r / 3] + r % 3] : 0.0;
-		}
-		for (int i = tid; i < EB * NL; i += NT) {
-			const int e = i / NL, j = i % NL;
-			double *Eb = E0 + e * S::E_SIZE;
-			int *ei = reinterpret_cast<int *>(Eb + S::E_I);
-			const int64_t g = (k0 + e) * NL + j;
-			const int dof = e < ne ? args.el_dof[g] : -1;
-			Eb[S::E_C + j] = e < ne ? args.el_coef[g] : 0.0;
-			ei[j] = dof;
-			ei[NL + j] = e < ne ? args.el_s[g] : 0;
-			int64_t *cs = reinterpret_cast<int64_t *>(Eb + S::E_CS);
-			cs[j] = dof >= 0 ? args.Ap[dof] : 0;
-			cs[NL + j] = dof >= 0 ? args.Ap[dof + 1] : 0;
+		else {
+			if (tid < EB) {
+				const bool live = tid < ne;
+				s_m[tid] = live ? args.el_cnt[2 * (k0 + tid)] : 0;
+				s_l[tid] = live ? args.el_cnt[2 * (k0 + tid) + 1] : 0;
+				s_cg[tid] = live && args.ecoef ? args.ecoef[args.el_id[k0 + tid]] : 1.0;
+			}
+			for (int i = tid; i < EB * 24; i += NT) {
+				const int e = i / 24, r = i % 24;
+				E0[e * S::E_SIZE + S::E_X + r] = e < ne ? args.xyz[3 * (int64_t) args.el_vtx[8 * (k0 + e) + r / 3] + r % 3] : 0.0;
+			}
+			for (int i = tid; i < EB * NL; i += NT) {
+				const int e = i / NL, j = i % NL;
+				double *Eb = E0 + e * S::E_SIZE;
+				int *ei = reinterpret_cast<int *>(Eb + S::E_I);
+				const int64_t g = (k0 + e) * NL + j;
+				const int dof = e < ne ? args.el_dof[g] : -1;
+				Eb[S::E_C + j] = e < ne ? args.el_coef[g] : 0.0;
+				ei[j] = dof;
+				ei[NL + j] = e < ne ? args.el_s[g] : 0;
+				int64_t *cs = reinterpret_cast<int64_t *>(Eb + S::E_CS);
+				cs[j] = dof >= 0 ? args.Ap[dof] : 0;
+				cs[NL + j] = dof >= 0 ? args.Ap[dof + 1] : 0;
+			}
 		}
 		__syncthreads();
 
@@ -303,6 +400,7 @@ __global__ void __launch_bounds__(NT, MINB) k_assemble_fp64(KArgs args, int64_t 
 			}
 		}
 		__syncthreads();
+		if (PF && bt + gridDim.x < nbatch) prefetch2();   // the first-level loads have had stage 1 to land
 		// ---- stages 2+3: thread owns column (e, b, b', c, c'); it accumulates
 		// the stage-2 values of the 3 x-classes in registers,
 		//   V_f[q1] = sum_k(class f) sum_q2 Wy_k[b][b'][q2] T1_k[q1][q2][c][c'],
@@ -365,6 +463,7 @@ __global__ void __launch_bounds__(NT, MINB) k_assemble_fp64(KArgs args, int64_t 
 		// ---- scatter into the CSC matrix (exclusive within a colour)
 		if (args.Ax) {
 			double *__restrict__ Ax = args.Ax;
+#pragma unroll
 			for (int base = 0; base < EB * NL2; base += NT * CH) {
 				int64_t pos[CH];
 				double val[CH];
@@ -384,7 +483,9 @@ __global__ void __launch_bounds__(NT, MINB) k_assemble_fp64(KArgs args, int64_t 
 							const int sa = ei[NL + a], sb = ei[NL + b];
 							const double *A = Eb + S::E_A;
 							val[r] = Eb[S::E_C + a] * Eb[S::E_C + b] * (A[sa * NL + sb] + A[sb * NL + sa]);
-							const int64_t t = cs[b] + args.el_off[(k0 + e) * NL2 + b * NL + a];
+							const int uu = (base / (NT * CH)) * CH + r;     // = (p - tid) / NT, compile-time when unrolled
+							const int64_t t = cs[b] + (PF ? (int64_t) off_c[uu < UOFF ? uu : UOFF - 1]
+							                              : (int64_t) args.el_off[(k0 + e) * NL2 + b * NL + a]);
 							if (t < cs[NL + b]) pos[r] = t;
 							else if (cs[NL + b] > cs[b]) atomicOr(args.status, kErrBounds);   // empty: column not owned
 						}

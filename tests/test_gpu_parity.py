@@ -161,7 +161,7 @@ def test_every_kernel_variant_is_bitwise_identical(gpu, monkeypatch, p, nq):
     sp.set_uniform_order(p)
     sp.assign_dofs()
     ref = None
-    for v in range(12):                       # indices past the last candidate pin the last one
+    for v in range(20):                       # indices past the last candidate pin the last one
         monkeypatch.setenv("H3DG_FP64_VARIANT", str(v))
         d = h.Discretization()
         d.set_spaces(sp)
