@@ -62,14 +62,51 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every ~2 ms from a thread (the timed regions are tens
+    of milliseconds), nvidia-smi as the fallback.  Reads only."""
+
+    REASONS = [(0x8, "hw_slowdown"), (0x40, "hw_thermal_slowdown"), (0x20, "sw_thermal_slowdown"),
+               (0x4, "sw_power_cap")]
 
     def __init__(self, index):
         self.index = index
-        self.samples = []
+        self.samples = []            # (sm_mhz, max_mhz, reason bits)
         self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _poll_nvml(self):
+        nv, h = self.nvml
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while True:
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), mx,
+                                     int(nv.nvmlDeviceGetCurrentClocksThrottleReasons(h))))
+            except Exception:
+                break
+            if self.stop.wait(0.002):
+                break
 
     def __enter__(self):
+        try:
+            self.nvml = self._handle()
+            self.thread = threading.Thread(target=self._poll_nvml, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index),
@@ -77,19 +114,23 @@ class ClockSampler:
                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
                  "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread = threading.Thread(target=self._read_smi, daemon=True)
             self.thread.start()
         except Exception:
             self.proc = None
         return self
 
-    def _read(self):
+    def _read_smi(self):
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 7:
-                self.samples.append(parts)
+            if len(parts) >= 7 and parts[0].replace(".", "").isdigit():
+                bits = sum(b for (b, _), v in zip(self.REASONS, parts[3:7]) if v.lower() == "active")
+                self.samples.append((float(parts[0]), float(parts[1]), bits))
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nvml:
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -101,12 +142,13 @@ class ClockSampler:
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         import statistics
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        bits = 0
+        for smp in self.samples:
+            bits |= smp[2]
+        return {"sm_mhz": statistics.median(smp[0] for smp in self.samples),
+                "sm_max_mhz": max(smp[1] for smp in self.samples),
+                "reasons": sorted(n for b, n in self.REASONS if bits & b), "samples": len(self.samples),
+                "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
 def build_problem(h, seed, device, side=None, workload="c2", partition=None):
