@@ -590,7 +590,7 @@ def main():
                          # the combined bound: the dense B^T D B contraction at the FP64 peak or the compulsory
                          # bytes at the HBM peak, whichever takes longer, over the kernel time (sum factorisation
                          # does less than the dense work, so this can exceed 1)
-                         "combined": {
+                         "combined": None if prec != h.PREC_FP64 else {
                              "definition": "max(dense-equivalent flops / FP64 peak, algorithmic bytes / HBM peak) / time",
                              "fp64_peak_tflops": FP64_PEAK_TFLOPS, "fp64_peak_source": "nominal (no measured FP64 figure)",
                              "frac": max(ne * dense_flops_per_element(args.workload) / (FP64_PEAK_TFLOPS * 1e12),
