@@ -354,7 +354,7 @@ def run_sweep(args):
     import hermes3d_b200 as h
     torch.cuda.set_device(0)
     rows = []
-    for p in range(1, 9):
+    for p in [int(x) for x in args.sweep_orders.split(",")]:
         side = args.side or (32 if p <= 4 else 16)
         rec = {"p": p, "elements": side ** 3}
         ref = None
@@ -427,6 +427,7 @@ def main():
                          "high-order path")
     ap.add_argument("--adjoint", action="store_true", help="C5 adjoint line (16 fields) instead of an assembly line")
     ap.add_argument("--sweep", action="store_true", help="orders 1..8: FP64 against both split precisions")
+    ap.add_argument("--sweep-orders", default="1,2,3,4,5,6,7,8", help="orders of --sweep")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -81,10 +81,10 @@ struct HoOzShape {
 	static_assert(SMEM_BYTES <= 227 * 1024, "shared memory");
 };
 
-// 32 lanes x 32 bit, 4 consecutive columns per thread, no wait
-__device__ __forceinline__ void tmem_ld4_i32(uint32_t taddr, int v[4]) {
-	asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
-	             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+// 32 lanes x 32 bit, 8 consecutive columns per thread, no wait
+__device__ __forceinline__ void tmem_ld8_i32(uint32_t taddr, int v[8]) {
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+	             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
 	             : "r"(taddr));
 }
 
@@ -346,18 +346,18 @@ __global__ void __launch_bounds__(256, 1) k_assemble_ho_oz(KArgsHO args, int64_t
 						const double rsc = oz_pow2(rex[mrow]);
 						const uint16_t *rec = offe + ((size_t) c2 * S::NCOL + (live ? colr : 0)) * NB;
 						const uint32_t tl = tmem + ((uint32_t) (quarter * 32) << 16);
-						constexpr int NCH4 = NC / 4;                      // 4-column chunks
-						constexpr int CHH = (NCH4 + 1) / 2;
-						const int ch0 = chalf ? CHH : 0, ch1 = chalf ? NCH4 : CHH;
+						constexpr int NCH8 = NC / 8;                      // 8-column chunks
+						constexpr int CHH = (NCH8 + 1) / 2;
+						const int ch0 = chalf ? CHH : 0, ch1 = chalf ? NCH8 : CHH;
 						for (int ch = ch0; ch < ch1; ch++) {
-							int acc[NS][4];
+							int acc[NS][8];
 #pragma unroll
-							for (int l = 0; l < NS; l++) tmem_ld4_i32(tl + (uint32_t) (l * NC + ch * 4), acc[l]);
+							for (int l = 0; l < NS; l++) tmem_ld8_i32(tl + (uint32_t) (l * NC + ch * 8), acc[l]);
 							tc::tmem_wait_ld();
 							if (!live) continue;
 #pragma unroll
-							for (int u = 0; u < 4; u++) {
-								const int n = pass * NC + ch * 4 + u;
+							for (int u = 0; u < 8; u++) {
+								const int n = pass * NC + ch * 8 + u;
 								if (n >= S::NPAIR) break;
 								const uint16_t off = rec[n];
 								if (off == kOffSkip) continue;
