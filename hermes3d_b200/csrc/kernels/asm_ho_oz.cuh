@@ -50,7 +50,7 @@ struct HoOzShape {
 	static constexpr int NCOL = NY * NY * NZ;
 	static constexpr int TM = 128;
 	static constexpr int NTILE = (NCOL + TM - 1) / TM;
-	static constexpr int TMEM_COLS = 512;
+	static constexpr int TMEM_COLS = NS * NC <= 128 ? 128 : NS * NC <= 256 ? 256 : 512;   // power of two >= NS NC
 	static constexpr int H0 = (NQX + 1) / 2;
 	static constexpr int T1D = 9 * NQX * NQY * NZ;            // stage-1 products (doubles)
 	// dynamic shared memory, byte offsets
@@ -157,8 +157,9 @@ __device__ __forceinline__ void ho_oz_put_slice(const long long (&fx)[4][S::H0],
 // 2^e as a double (|e| well inside the normal range)
 __device__ __forceinline__ double oz_pow2(int e) { return __longlong_as_double((long long) (1023 + e) << 52); }
 
-template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ>
-__global__ void __launch_bounds__(256, 1) k_assemble_ho_oz(KArgsHO args, int64_t kbeg, int64_t kend) {
+// MINB > 1 (low orders): several CTAs share an SM; their TMEM allocations fit side by side
+template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_assemble_ho_oz(KArgsHO args, int64_t kbeg, int64_t kend) {
 	constexpr int NT = 256;
 	using S = HoOzShape<PX, PY, PZ, NQX, NQY, NQZ>;
 	using SB = typename S::B;

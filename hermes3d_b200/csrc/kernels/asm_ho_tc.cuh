@@ -300,8 +300,9 @@ __device__ __forceinline__ void ho_tc_epilogue(uint32_t tacc, const uint4 *offv,
 	}
 }
 
-template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ>
-__global__ void __launch_bounds__(256, 1) k_assemble_ho_tc(KArgsHO args, int64_t kbeg, int64_t kend) {
+// MINB > 1 (low orders): several CTAs share an SM; their TMEM allocations fit side by side
+template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_assemble_ho_tc(KArgsHO args, int64_t kbeg, int64_t kend) {
 	constexpr int NT = 256;
 	using S = HoTcShape<PX, PY, PZ, NQX, NQY, NQZ>;
 	using SB = typename S::B;
