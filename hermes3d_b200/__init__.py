@@ -10,6 +10,7 @@ from .discretization import (BC_ESSENTIAL, BC_NATURAL, BC_NONE, Discretization, 
                              int_grad_u_grad_v_plus_u_v)
 from .mesh import Mesh, load_mesh3d, permute_vertices, unit_cube
 
+H3dgError = _capi.H3dgError
 PREC_FP64 = _capi.PREC_FP64
 PREC_TF32X3 = _capi.PREC_TF32X3
 PREC_OZAKI = _capi.PREC_OZAKI
@@ -17,5 +18,5 @@ PREC_OZAKI = _capi.PREC_OZAKI
 __all__ = [
     "Mesh", "load_mesh3d", "unit_cube", "permute_vertices", "H1Space", "Discretization", "UMFPackMatrix",
     "UMFPackVector", "int_grad_u_grad_v", "int_grad_u_grad_v_plus_u_v", "int_F_v", "UnsupportedForm",
-    "BC_ESSENTIAL", "BC_NATURAL", "BC_NONE", "PREC_FP64", "PREC_TF32X3", "PREC_OZAKI",
+    "BC_ESSENTIAL", "BC_NATURAL", "BC_NONE", "PREC_FP64", "PREC_TF32X3", "PREC_OZAKI", "H3dgError",
 ]

@@ -50,6 +50,8 @@ SIGNATURES = {
     "h3dg_mesh_add_quad_boundaries": [_p, _pi64, _pi32, _i64],
     "h3dg_mesh_finalize": [_p],
     "h3dg_mesh_counts": [_p, _pi64, _pi64, _pi64, _pi64],
+    "h3dg_mesh_refine_element": [_p, _i64, C.c_int],
+    "h3dg_mesh_get_arrays": [_p, _pd, _pi64, _pi64],
     "h3dg_space_create": [_p, C.POINTER(_p)],
     "h3dg_space_destroy": [_p],
     "h3dg_space_set_bc_types": [_p, BC_TYPE_FN, _p],

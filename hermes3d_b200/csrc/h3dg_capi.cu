@@ -106,6 +106,13 @@ struct h3dg_disc {
 	DBuf<int64_t> el_base, el_obase;
 	DBuf<uint16_t> el_offm;
 	DBuf<unsigned> mx_counters;
+	// elements with constrained nodes: W columns, slot map, per-CTA scratch
+	DBuf<int32_t> ce_desc, ce_vtx, ce_id, ce_udof;
+	DBuf<int64_t> ce_ubase, ce_wptr, ce_obase;
+	DBuf<uint16_t> ce_ws, ce_off;
+	DBuf<double> ce_ww, ce_scratch;
+	int64_t ce_stride = 0;
+	int ce_per_sm[h3dg::Plan::kCedClasses] = { 1, 1, 1 };
 	int mx_variant[h3dg::Plan::kClasses] = { -1, -1, -1 };
 	cudaGraphExec_t mx_exec = nullptr;
 	double *mx_ax = nullptr, *mx_rhs = nullptr;
@@ -191,6 +198,27 @@ h3dg_status h3dg_mesh_finalize(h3dg_mesh *mesh) {
 	if (!mesh) return fail(H3DG_ERR_INVALID_ARG, "finalize: null mesh");
 	std::string err;
 	if (mesh->m.finalize(err) != 0) return fail(H3DG_ERR_MESH, err);
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_mesh_refine_element(h3dg_mesh *mesh, int64_t elem_id, int reft) {
+	if (!mesh) return fail(H3DG_ERR_INVALID_ARG, "refine_element: null mesh");
+	if (!mesh->m.finalized) return fail(H3DG_ERR_STATE, "refine_element: mesh not finalized");
+	if (reft != 7) return fail(H3DG_ERR_MESH, "refine_element: only REFT_HEX_XYZ (7) is supported");
+	if (elem_id < 1 || elem_id > mesh->m.ne()) return fail(H3DG_ERR_INVALID_ARG, "refine_element: element id out of range");
+	std::string err;
+	if (mesh->m.refine_xyz(elem_id - 1, err) != 0) return fail(H3DG_ERR_MESH, err);
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_mesh_get_arrays(const h3dg_mesh *mesh, double *xyz, int64_t *hex, int64_t *parent) {
+	if (!mesh) return fail(H3DG_ERR_INVALID_ARG, "get_arrays: null mesh");
+	const h3dg::Mesh &m = mesh->m;
+	if (xyz) std::copy(m.xyz.begin(), m.xyz.end(), xyz);
+	if (hex)
+		for (size_t i = 0; i < m.hex.size(); i++) hex[i] = m.hex[i] + 1;
+	if (parent)
+		for (int64_t e = 0; e < m.ne(); e++) parent[e] = m.parent.empty() ? 0 : m.parent[e] + 1;
 	return H3DG_OK;
 }
 
@@ -386,6 +414,8 @@ h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nn
 			if (sp.order[3 * e + d] != sp.order[d]) mixed = true;
 	const char *force_mixed = std::getenv("H3DG_FORCE_MIXED");
 	if (force_mixed && force_mixed[0] == '1') mixed = true;
+	// refined meshes (hanging nodes) always take the batched path
+	if (sp.mesh->nrefined) mixed = true;
 	disc->reset_mixed();
 	const h3dg::PlanScope *scope = nullptr;
 	disc->scope = h3dg::PlanScope();
@@ -429,7 +459,39 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 		H3DG_CUDA_TRY(disc->el_cdof.upload(P.el_cdof));
 		H3DG_CUDA_TRY(disc->el_ccoef.upload(P.el_ccoef));
 		H3DG_CUDA_TRY(disc->el_offm.upload(P.el_offm));
-		H3DG_CUDA_TRY(disc->mx_counters.alloc((size_t) P.ncolors * h3dg::Plan::kClasses));
+		H3DG_CUDA_TRY(disc->mx_counters.alloc((size_t) P.ncolors * (h3dg::Plan::kClasses + h3dg::Plan::kCedClasses)));
+		if (P.nce > 0) {
+			H3DG_CUDA_TRY(disc->ce_desc.upload(P.ce_desc));
+			H3DG_CUDA_TRY(disc->ce_vtx.upload(P.ce_vtx));
+			H3DG_CUDA_TRY(disc->ce_id.upload(P.ce_id));
+			H3DG_CUDA_TRY(disc->ce_udof.upload(P.ce_udof));
+			H3DG_CUDA_TRY(disc->ce_ubase.upload(P.ce_ubase));
+			H3DG_CUDA_TRY(disc->ce_wptr.upload(P.ce_wptr));
+			H3DG_CUDA_TRY(disc->ce_obase.upload(P.ce_obase));
+			H3DG_CUDA_TRY(disc->ce_ws.upload(P.ce_ws));
+			H3DG_CUDA_TRY(disc->ce_off.upload(P.ce_off));
+			H3DG_CUDA_TRY(disc->ce_ww.upload(P.ce_ww));
+			// per-CTA scratch (element matrix + load vector) for every resident CTA
+			int nsm = 148;
+			cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
+			const int table_bytes = (int) (P.mixed_tables.size() * sizeof(double));
+			int64_t blocks = 0;
+			for (int cls = 0; cls < h3dg::Plan::kCedClasses; cls++) {
+				h3dg_tables::CedSpec &k = h3dg_tables::ced_table()[cls];
+				const size_t smem = k.smem(table_bytes);
+				if (!k.configured || k.configured_smem < smem) {
+					H3DG_CUDA_TRY(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+					k.configured = true;
+					k.configured_smem = smem;
+				}
+				int per_sm = 1;
+				cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, smem);
+				disc->ce_per_sm[cls] = per_sm < 1 ? 1 : per_sm;
+				blocks = std::max<int64_t>(blocks, (int64_t) nsm * disc->ce_per_sm[cls]);
+			}
+			disc->ce_stride = ((int64_t) P.ce_max_nl * P.ce_max_nl + P.ce_max_nl + 1) / 2 * 2;
+			H3DG_CUDA_TRY(disc->ce_scratch.alloc((size_t) (disc->ce_stride * blocks)));
+		}
 		disc->el_offc.release();
 		disc->el_offt.release();
 	}
@@ -651,7 +713,47 @@ static h3dg_status assemble_mixed(h3dg_disc *disc, double *d_Ax, double *d_rhs, 
 		k.fn<<<(unsigned) grid, k.threads, k.smem(disc->table_bytes), s>>>(a, kb, ke, li);
 		return true;
 	};
-	const size_t ncnt = sizeof(unsigned) * (size_t) P.ncolors * NC;
+	constexpr int NCE = h3dg::Plan::kCedClasses;
+	const size_t ncnt = sizeof(unsigned) * (size_t) P.ncolors * (NC + NCE);
+	// constrained elements: one kernel per class, scratch for every resident CTA
+	h3dg::KArgsCed ca;
+	int ce_per_sm[NCE] = { 1, 1, 1 };
+	if (P.nce > 0) {
+		ca.xyz = disc->xyz.p;
+		ca.el_vtx = disc->ce_vtx.p;
+		ca.el_id = disc->ce_id.p;
+		ca.ecoef = disc->coef.p;
+		ca.el_desc = disc->ce_desc.p;
+		ca.ubase = disc->ce_ubase.p;
+		ca.udof = disc->ce_udof.p;
+		ca.wptr = disc->ce_wptr.p;
+		ca.ws = disc->ce_ws.p;
+		ca.ww = disc->ce_ww.p;
+		ca.obase = disc->ce_obase.p;
+		ca.off = disc->ce_off.p;
+		ca.Ap = disc->Ap.p;
+		ca.tables = disc->tables.p;
+		ca.table_bytes = disc->table_bytes;
+		ca.mass = a.mass;
+		ca.lf = a.lf;
+		ca.lf_value = a.lf_value;
+		ca.Ax = d_Ax;
+		ca.rhs = a.rhs;
+		ca.status = disc->status.p;
+		ca.counters = disc->mx_counters.p + (size_t) P.ncolors * NC;
+		ca.scratch = disc->ce_scratch.p;
+		ca.scratch_stride = disc->ce_stride;
+		for (int cls = 0; cls < NCE; cls++) ce_per_sm[cls] = disc->ce_per_sm[cls];
+	}
+	auto launch_ced = [&](int c, int cls, cudaStream_t s) -> bool {
+		const int li = c * NCE + cls;
+		const int64_t kb = P.ce_launch_ptr[li], ke = P.ce_launch_ptr[li + 1];
+		if (ke <= kb) return false;
+		CedSpec &k = ced_table()[cls];
+		const int64_t grid = std::min<int64_t>(ke - kb, (int64_t) nsm * ce_per_sm[cls]);
+		k.fn<<<(unsigned) grid, k.threads, k.smem(disc->table_bytes), s>>>(ca, kb, ke, li);
+		return true;
+	};
 	// variants: time each class's launches once per plan, keep the fastest
 	if (disc->mx_variant[0] < 0) {
 		cudaEvent_t e0, e1;
@@ -703,6 +805,9 @@ static h3dg_status assemble_mixed(h3dg_disc *disc, double *d_Ax, double *d_rhs, 
 			cudaStream_t ss[NC] = { s0, s1, s2 };
 			for (int cls = 0; cls < NC; cls++)
 				if (launch(mix_table()[disc->mx_variant[cls]], per_sm[cls], c, cls, ss[cls])) n++;
+			if (P.nce > 0)
+				for (int cls = 0; cls < NCE; cls++)
+					if (launch_ced(c, cls, s0)) n++;
 			if (fork) {
 				H3DG_CUDA_TRY(cudaEventRecord(disc->mx_ev[1], s1));
 				H3DG_CUDA_TRY(cudaEventRecord(disc->mx_ev[2], s2));
@@ -1103,7 +1208,7 @@ h3dg_status h3dg_disc_update_vertices(h3dg_disc *disc, const double *xyz, int64_
 }
 
 h3dg_status h3dg_disc_update_coefficients(h3dg_disc *disc, const double *elem_coef, int64_t ne) {
-	if (!disc || !disc->have_plan || !elem_coef || ne != disc->plan.ne)
+	if (!disc || !disc->have_plan || !elem_coef || ne != disc->plan.ne_ids)
 		return fail(H3DG_ERR_INVALID_ARG, "update_coefficients: bad arguments or no plan");
 	{ h3dg_status s0 = ensure_device(disc); if (s0 != H3DG_OK) return s0; }
 	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
@@ -1114,7 +1219,7 @@ h3dg_status h3dg_disc_update_coefficients(h3dg_disc *disc, const double *elem_co
 }
 
 h3dg_status h3dg_disc_update_coefficients_device(h3dg_disc *disc, const double *d_elem_coef, int64_t ne, void *stream) {
-	if (!disc || !disc->have_plan || !d_elem_coef || ne != disc->plan.ne)
+	if (!disc || !disc->have_plan || !d_elem_coef || ne != disc->plan.ne_ids)
 		return fail(H3DG_ERR_INVALID_ARG, "update_coefficients_device: bad arguments or no plan");
 	{ h3dg_status s0 = ensure_device(disc); if (s0 != H3DG_OK) return s0; }
 	H3DG_CUDA_TRY(cudaSetDevice(disc->device));

@@ -95,11 +95,15 @@ struct Key2Hash {
 // Mesh::add_hex / add_quad_boundary / ugh (src/mesh.cc:975-1102) and the
 // loader's outer-face check (src/loader/mesh3d.cc:272-282).  Facet and edge
 // ids are handed out in creation order, which is the order the reference's
-// FOR_ALL_FACETS / FOR_ALL_EDGES loops visit them.
+// FOR_ALL_FACETS / FOR_ALL_EDGES loops visit them.  With refined elements
+// the facets of all elements (active or not) are kept: a parent's face and
+// the quarter faces of its children are distinct facets, as in the
+// reference's facet tree (refine_quad_facet, src/mesh.cc:1843-2018).
 int Mesh::finalize(std::string &err) {
 	int64_t n = ne(), nvert = nv();
 	for (int64_t i = 0; i < 8 * n; i++)
 		if (hex[i] < 0 || hex[i] >= nvert) { err = "Invalid vertex index was found in the section defining hexes."; return -1; }
+	const bool tree = nrefined > 0;
 	std::unordered_map<std::array<int64_t, 4>, int64_t, Key4Hash> fmap;
 	std::unordered_map<std::pair<int64_t, int64_t>, int64_t, Key2Hash> emap;
 	fmap.reserve(4 * n);
@@ -107,6 +111,7 @@ int Mesh::finalize(std::string &err) {
 	elem_face.assign(6 * n, -1);
 	elem_edge.assign(12 * n, -1);
 	facet_left.clear(); facet_left_face.clear(); facet_right.clear();
+	edge_vtx.clear();
 	for (int64_t e = 0; e < n; e++) {
 		const int64_t *v = &hex[8 * e];
 		// Mesh::ref_edges: edges in local order
@@ -114,7 +119,10 @@ int Mesh::finalize(std::string &err) {
 			int64_t a = v[kHexEdgeVtx[ie][0]], b = v[kHexEdgeVtx[ie][1]];
 			std::pair<int64_t, int64_t> k(std::min(a, b), std::max(a, b));
 			auto it = emap.find(k);
-			if (it == emap.end()) it = emap.emplace(k, (int64_t) emap.size()).first;
+			if (it == emap.end()) {
+				it = emap.emplace(k, (int64_t) emap.size()).first;
+				edge_vtx.push_back(k);
+			}
 			elem_edge[12 * e + ie] = it->second;
 		}
 		for (int f = 0; f < 6; f++) {
@@ -140,6 +148,7 @@ int Mesh::finalize(std::string &err) {
 	nedges = (int64_t) emap.size();
 	facet_outer.assign(nfacets, 0);
 	facet_marker.assign(nfacets, MARKER_UNDEFINED);
+	facet_ced.assign(nfacets, 0);
 	for (size_t b = 0; b < bquad.size(); b++) {
 		std::array<int64_t, 4> k = bquad[b];
 		std::sort(k.begin(), k.end());
@@ -149,8 +158,30 @@ int Mesh::finalize(std::string &err) {
 		facet_outer[it->second] = 1;
 		facet_marker[it->second] = bmarker[b];
 	}
+	if (tree) {
+		// a child's face with no second element lies on its parent's face:
+		// outer (with the parent's marker) if that face is, else it is a quarter
+		// of a face whose other side is an active, unrefined element
+		for (int64_t f = 0; f < nfacets; f++) {
+			if (facet_right[f] >= 0 || facet_outer[f]) continue;
+			const int64_t e = facet_left[f], P = parent[e];
+			if (P < 0) continue;
+			const int lf = (int) facet_left_face[f];
+			int i = 0;
+			while (i < 8 && sons[8 * P + i] != e) i++;
+			bool on_parent_face = false;
+			for (int k = 0; k < 4; k++) on_parent_face |= kHexFaceVtx[lf][k] == i;
+			if (!on_parent_face) { err = "refinement: inner child face without a neighbour"; return -1; }
+			const int64_t pf = elem_face[6 * P + lf];
+			if (facet_outer[pf]) {
+				facet_outer[f] = 1;
+				facet_marker[f] = facet_marker[pf];
+			}
+			else facet_ced[f] = 1;
+		}
+	}
 	for (int64_t f = 0; f < nfacets; f++)
-		if (!facet_outer[f] && facet_right[f] < 0) { err = "Not all outer faces have defined boundary condition."; return -1; }
+		if (!facet_outer[f] && facet_right[f] < 0 && !facet_ced[f]) { err = "Not all outer faces have defined boundary condition."; return -1; }
 	edge_bnd.assign(nedges, 0);
 	for (int64_t f = 0; f < nfacets; f++)
 		if (facet_outer[f]) {
@@ -158,8 +189,103 @@ int Mesh::finalize(std::string &err) {
 			int lf = (int) facet_left_face[f];
 			for (int k = 0; k < 4; k++) edge_bnd[elem_edge[12 * e + kHexFaceEdges[lf][k]]] = 1;
 		}
+	// hanging nodes (Space::fc_element / fc_face, src/space.cc:598-736): every
+	// face of an inactive element whose neighbour across it is active
+	vertex_ced.assign(nvert, 0);
+	edge_ced.assign(nedges, 0);
+	interfaces.clear();
+	if (tree) {
+		for (int64_t P = 0; P < n; P++) {
+			if (sons[8 * P] < 0) continue;
+			for (int f = 0; f < 6; f++) {
+				const int64_t pf = elem_face[6 * P + f];
+				if (facet_outer[pf]) continue;
+				const int64_t N = facet_left[pf] == P ? facet_right[pf] : facet_left[pf];
+				if (N < 0 || !active(N)) continue;
+				const int Nf = facet_left[pf] == N ? (int) facet_left_face[pf] : -1;
+				int fN = Nf;
+				if (fN < 0)
+					for (int g = 0; g < 6; g++)
+						if (elem_face[6 * N + g] == pf) fN = g;
+				interfaces.push_back(Interface { P, f, N, fN });
+				for (int k = 0; k < 4; k++) {
+					const int i = kHexFaceVtx[f][k];
+					const int64_t c = sons[8 * P + i];
+					facet_ced[elem_face[6 * c + f]] = 1;
+					for (int q = 0; q < 4; q++) {
+						const int lv = kHexFaceVtx[f][q];
+						if (lv != i) vertex_ced[hex[8 * c + lv]] = 1;
+						edge_ced[elem_edge[12 * c + kHexFaceEdges[f][q]]] = 1;
+					}
+				}
+			}
+		}
+	}
 	finalized = true;
 	return 0;
+}
+
+// Mesh::refine_element with REFT_HEX_XYZ (src/mesh.cc:1262-1323, refine_hex_8
+// :1555-1633): the 12 edge midpoints, the 6 face midpoints (registered for
+// both diagonals) and the centre are looked up or created in that order
+// (get_midpoint / set_midpoint, :2064-2101, the vertex at (a + b) / 2), and the
+// 8 children keep the parent's orientation.  Child i holds the parent's
+// corner i; its vertex j is the point halfway between the parent's corners i
+// and j in the reference domain (corner, edge midpoint, face midpoint or
+// centre).  Only base elements are refined (one level).
+int Mesh::refine_xyz(int64_t e, std::string &err) {
+	if (!finalized) { err = "refine: mesh not finalized"; return -1; }
+	if (e < 0 || e >= ne()) { err = "refine: element id out of range"; return -1; }
+	if (parent.empty()) {
+		parent.assign(ne(), -1);
+		sons.assign(8 * ne(), -1);
+	}
+	if (sons[8 * e] >= 0) { err = "refine: element is not active"; return -1; }
+	if (parent[e] >= 0) { err = "refine: only base elements can be refined (one refinement level)"; return -1; }
+	int64_t vtx[8];
+	for (int k = 0; k < 8; k++) vtx[k] = hex[8 * e + k];
+	auto key = [](int64_t a, int64_t b) { return std::make_pair(std::min(a, b), std::max(a, b)); };
+	auto get_mid = [&](int64_t a, int64_t b) -> int64_t {
+		auto it = midpoints.find(key(a, b));
+		if (it != midpoints.end()) return it->second;
+		const int64_t id = nv();
+		for (int r = 0; r < 3; r++) xyz.push_back((xyz[3 * a + r] + xyz[3 * b + r]) / 2.0);
+		midpoints[key(a, b)] = id;
+		return id;
+	};
+	int64_t emp[12], fmp[6];
+	for (int ie = 0; ie < 12; ie++) emp[ie] = get_mid(vtx[kHexEdgeVtx[ie][0]], vtx[kHexEdgeVtx[ie][1]]);
+	for (int f = 0; f < 6; f++) {
+		fmp[f] = get_mid(emp[kHexFaceEdges[f][0]], emp[kHexFaceEdges[f][2]]);
+		midpoints[key(emp[kHexFaceEdges[f][1]], emp[kHexFaceEdges[f][3]])] = fmp[f];
+	}
+	const int64_t ctr = get_mid(fmp[0], fmp[1]);
+	midpoints[key(fmp[2], fmp[3])] = ctr;
+	midpoints[key(fmp[4], fmp[5])] = ctr;
+	for (int i = 0; i < 8; i++) {
+		const int64_t c = ne();
+		for (int j = 0; j < 8; j++) {
+			int diff = 0, same_dir = -1;
+			for (int d = 0; d < 3; d++) {
+				if (kRefVtx[i][d] != kRefVtx[j][d]) diff++;
+				else same_dir = d;
+			}
+			int64_t v = vtx[i];
+			if (diff == 1) {
+				for (int ie = 0; ie < 12; ie++)
+					if ((kHexEdgeVtx[ie][0] == i && kHexEdgeVtx[ie][1] == j) || (kHexEdgeVtx[ie][0] == j && kHexEdgeVtx[ie][1] == i)) v = emp[ie];
+			}
+			else if (diff == 2) v = fmp[2 * same_dir + (kRefVtx[i][same_dir] > 0 ? 1 : 0)];
+			else if (diff == 3) v = ctr;
+			hex.push_back(v);
+		}
+		parent.push_back(e);
+		for (int k = 0; k < 8; k++) sons.push_back(-1);
+		sons[8 * e + i] = c;
+	}
+	nrefined++;
+	finalized = false;
+	return finalize(err);
 }
 
 // Hex::get_edge_orientation (src/mesh.cc:274-284)
@@ -314,7 +440,26 @@ void Space::lift_face(int64_t e, int iface) {
 	std::vector<int64_t> tmp;
 	for (int k = 0; k < 4; k++) {
 		int le = kHexFaceEdges[iface][k];
-		const EData &en = ed[mesh->elem_edge[12 * e + le]];
+		const int64_t eid = mesh->elem_edge[12 * e + le];
+		const EData &en = ed[eid];
+		if (en.ced) {
+			// a constrained edge contributes the restriction of the constraining
+			// edge's lifting (src/space/h1.cc:311-322)
+			auto it = econs.find(eid);
+			if (it == econs.end()) continue;
+			const CedEdge &ce = it->second;
+			const bool flip = mesh->hex[8 * e + kHexEdgeVtx[le][0]] > mesh->hex[8 * e + kHexEdgeVtx[le][1]];
+			for (size_t j = 0; j < ce.dof.size(); j++) {
+				if (ce.dof[j] >= 0) continue;
+				for (int mm = 2; mm <= ce.order; mm++) {
+					int t[3];
+					for (int d = 0; d < 3; d++) t[d] = kEdgePat[le][d] < 0 ? mm : kEdgePat[le][d];
+					bidx.push_back(encode_index(SHFN_EDGE, le, t[0], t[1], t[2], 0));
+					bcoef.push_back(((flip && (mm & 1)) ? -1.0 : 1.0) * ce.c[j * (ce.order - 1) + mm - 2]);
+				}
+			}
+			continue;
+		}
 		if (en.n > 0) {
 			edge_indices(le, mesh->edge_orientation(e, le), en.order, tmp);
 			for (int i = 0; i < en.n; i++) {
@@ -359,27 +504,39 @@ static void set_bc_info(int &bc, int &marker, int newbc, int newmarker) {
 	}
 }
 
-// Space::assign_dofs (src/space.cc:1991-2028) for meshes without hanging
-// nodes: enforce_minimum_rule, set_bc_information, H1Space::assign_dofs_internal
-// and update_constraints (boundary projections).
+// Space::assign_dofs (src/space.cc:1991-2028): find constraints (the mesh's
+// hanging-node flags), enforce_minimum_rule, set_bc_information,
+// H1Space::assign_dofs_internal and update_constraints (boundary projections,
+// then the constraints of the hanging nodes).  Only active elements carry
+// DOFs; constrained nodes get none.
 int Space::assign_dofs(int first, int strd, std::string &err) {
 	if (!mesh || !mesh->finalized) { err = "mesh not finalized"; return -1; }
 	int64_t ne = mesh->ne();
 	if ((int64_t) order.size() != 3 * ne) { err = "element orders not set"; return -1; }
 	for (int64_t i = 0; i < 3 * ne; i++)
-		if (order[i] < 1 || order[i] > kMaxOrder) { err = "element order out of range 1..10"; return -1; }
+		if (mesh->active(i / 3) && (order[i] < 1 || order[i] > kMaxOrder)) { err = "element order out of range 1..10"; return -1; }
 	first_dof = next_dof = first;
 	stride = strd;
 	vd.assign(mesh->nv(), VData());
 	ed.assign(mesh->nedges, EData());
 	fd.assign(mesh->nfacets, FData());
 	bd.assign(ne, BData());
+	vcons.clear();
+	econs.clear();
+	fcons.clear();
+	if (mesh->nrefined) {
+		for (int64_t v = 0; v < mesh->nv(); v++) vd[v].ced = mesh->vertex_ced[v];
+		for (int64_t i = 0; i < mesh->nedges; i++) ed[i].ced = mesh->edge_ced[i];
+		for (int64_t f = 0; f < mesh->nfacets; f++) fd[f].ced = mesh->facet_ced[f];
+	}
 
 	// enforce_minimum_rule (src/space.cc:172-239)
 	for (int64_t e = 0; e < ne; e++) {
+		if (!mesh->active(e)) continue;
 		const int *o = &order[3 * e];
 		for (int f = 0; f < 6; f++) {
 			FData &fn = fd[mesh->elem_face[6 * e + f]];
+			if (fn.ced) continue;
 			int h, v;
 			face_order_of(o, f, h, v);
 			if (mesh->face_orientation(e, f) >= 4) std::swap(h, v);
@@ -388,12 +545,14 @@ int Space::assign_dofs(int first, int strd, std::string &err) {
 		}
 		for (int ie = 0; ie < 12; ie++) {
 			EData &en = ed[mesh->elem_edge[12 * e + ie]];
+			if (en.ced) continue;
 			int eo = edge_order_of(o, ie);
 			if (en.order < 0 || eo < en.order) en.order = eo;
 		}
 	}
 
-	// set_bc_information (src/space.cc:472-502)
+	// set_bc_information (src/space.cc:472-502): every outer facet, those of
+	// refined elements included
 	for (int64_t f = 0; f < mesh->nfacets; f++) {
 		if (!mesh->facet_outer[f]) continue;
 		int marker = mesh->facet_marker[f];
@@ -414,19 +573,22 @@ int Space::assign_dofs(int first, int strd, std::string &err) {
 
 	// H1Space::assign_dofs_internal (src/space/h1.cc:75-126)
 	std::vector<char> seen(mesh->nv(), 0);
-	for (int64_t e = 0; e < ne; e++)
+	for (int64_t e = 0; e < ne; e++) {
+		if (!mesh->active(e)) continue;
 		for (int iv = 0; iv < 8; iv++) {
 			int64_t v = mesh->hex[8 * e + iv];
-			if (seen[v]) continue;
+			if (seen[v] || vd[v].ced) continue;
 			seen[v] = 1;
 			if (vd[v].bc == BC_ESSENTIAL) vd[v].dof = DIRICHLET_DOF;
 			else { vd[v].dof = next_dof; next_dof += stride; }
 		}
+	}
 	std::vector<char> eseen(mesh->nedges, 0);
-	for (int64_t e = 0; e < ne; e++)
+	for (int64_t e = 0; e < ne; e++) {
+		if (!mesh->active(e)) continue;
 		for (int ie = 0; ie < 12; ie++) {
 			int64_t id = mesh->elem_edge[12 * e + ie];
-			if (eseen[id]) continue;
+			if (eseen[id] || ed[id].ced) continue;
 			eseen[id] = 1;
 			EData &en = ed[id];
 			int n = en.order - 1;
@@ -434,11 +596,13 @@ int Space::assign_dofs(int first, int strd, std::string &err) {
 			else { en.dof = next_dof; next_dof += n * stride; }
 			en.n = n;
 		}
+	}
 	std::vector<char> fseen(mesh->nfacets, 0);
-	for (int64_t e = 0; e < ne; e++)
+	for (int64_t e = 0; e < ne; e++) {
+		if (!mesh->active(e)) continue;
 		for (int f = 0; f < 6; f++) {
 			int64_t id = mesh->elem_face[6 * e + f];
-			if (fseen[id]) continue;
+			if (fseen[id] || fd[id].ced) continue;
 			fseen[id] = 1;
 			FData &fn = fd[id];
 			int n = (fn.ox - 1) * (fn.oy - 1);
@@ -446,7 +610,9 @@ int Space::assign_dofs(int first, int strd, std::string &err) {
 			else { fn.dof = next_dof; next_dof += n * stride; }
 			fn.n = n;
 		}
+	}
 	for (int64_t e = 0; e < ne; e++) {
+		if (!mesh->active(e)) continue;
 		const int *o = &order[3 * e];
 		int n = (o[0] - 1) * (o[1] - 1) * (o[2] - 1);
 		bd[e].n = n;
@@ -454,9 +620,11 @@ int Space::assign_dofs(int first, int strd, std::string &err) {
 		next_dof += n * stride;
 	}
 
-	// update_constraints (src/space.cc:2030-2066): vertex projections first,
-	// then edge and face projections element by element (uc_element, :1943-1987)
-	for (int64_t e = 0; e < ne; e++)
+	// update_constraints (src/space.cc:2030-2066): vertex projections on the
+	// outer faces of active elements, then edge and face projections element
+	// by element over all elements (uc_element, :1943-1987)
+	for (int64_t e = 0; e < ne; e++) {
+		if (!mesh->active(e)) continue;
 		for (int f = 0; f < 6; f++) {
 			if (!mesh->facet_outer[mesh->elem_face[6 * e + f]]) continue;
 			for (int k = 0; k < 4; k++) {
@@ -468,11 +636,22 @@ int Space::assign_dofs(int first, int strd, std::string &err) {
 				}
 			}
 		}
-	for (int64_t e = 0; e < ne; e++) {
+	}
+	// element id order; the constraints of the hanging nodes (computed by
+	// uc_element of the refined base element) come after every base element
+	// and before the children, whose boundary projections use them
+	auto lift_element = [&](int64_t e) {
 		for (int ie = 0; ie < 12; ie++) lift_edge(e, ie);
+		if (!mesh->active(e)) return;
 		for (int f = 0; f < 6; f++)
 			if (mesh->facet_outer[mesh->elem_face[6 * e + f]]) lift_face(e, f);
-	}
+	};
+	for (int64_t e = 0; e < ne; e++)
+		if (!mesh->nrefined || mesh->parent[e] < 0) lift_element(e);
+	if (!mesh->interfaces.empty() && build_constraints(err) != 0) return -1;
+	if (mesh->nrefined)
+		for (int64_t e = 0; e < ne; e++)
+			if (mesh->parent[e] >= 0) lift_element(e);
 	assigned = true;
 	return 0;
 }
@@ -485,6 +664,7 @@ static inline void al_add(std::vector<AsmEntry> &al, int64_t idx, int dof, doubl
 // H1Space::get_element_assembly_list (src/space/h1.cc:130-137) with the
 // vertex / edge / face / bubble lists of src/space.cc:296-450.
 void Space::element_assembly_list(int64_t e, std::vector<AsmEntry> &al) const {
+	if (element_constrained(e)) { constrained_assembly_list(e, al); return; }
 	al.clear();
 	for (int iv = 0; iv < 8; iv++) {
 		const VData &v = vd[mesh->hex[8 * e + iv]];
@@ -512,6 +692,258 @@ void Space::element_assembly_list(int64_t e, std::vector<AsmEntry> &al) const {
 		else if (fn.has_proj) {
 			for (int j = 0; j < fn.n; j++) al_add(al, idx[j], DIRICHLET_DOF, fn.proj[j]);
 		}
+	}
+	if (bd[e].n > 0) {
+		bubble_indices(&order[3 * e], idx);
+		for (int j = 0; j < bd[e].n; j++) al_add(al, idx[j], bd[e].dof + j * stride, 1.0);
+	}
+}
+
+// ---------------------------------------------------------------- hanging nodes
+//
+// The reference expresses a constrained function as a combination of the
+// element's own edge / face functions whose coefficients it finds by
+// collocation at Chebyshev points (calc_constrained_*_combination,
+// src/shapeset/h1lobattohex.cc:428-719) and attaches it to the DOFs of the
+// constraining nodes through base lists (src/space.cc:739-1941).  That
+// combination is the restriction of the constraining global function to the
+// constrained node: a polynomial of the same degree, so the expansion in the
+// node's Lobatto functions is exact and unique.  Here it is computed directly:
+// a global function's trace on the big face is a product l_a(x1) l_b(x2) in
+// the big element's face coordinates; restricted to a half interval each
+// factor is expanded as f(u) = f(-1) l_0(u) + f(1) l_1(u) + sum_m R_m l_m(u),
+// R_m = int f'(u) l_m'(u) du (the l_m', m >= 2, are orthonormal on [-1, 1]).
+// Vertex coefficients are function values at the hanging vertex
+// (calc_vertex_*_ced), edge coefficients the R_m of the varying factor times
+// the value of the fixed one (calc_edge_edge_ced, calc_mid_edge_edge_ced,
+// calc_edge_face_ced), face coefficients products of R_m (calc_face_face_ced).
+
+// bubble coefficients R_2..R_k of u -> l_k(mid + half u)
+static void restrict_bubbles(int k, double mid, double half, double *R) {
+	std::vector<double> q, w;
+	gauss_legendre(std::max(2, k), q, w);
+	for (int m = 2; m <= k; m++) {
+		double s = 0.0;
+		for (size_t i = 0; i < q.size(); i++) s += w[i] * half * lobatto_deriv(k, mid + half * q[i]) * lobatto_deriv(m, q[i]);
+		R[m - 2] = s;
+	}
+}
+
+bool Space::element_constrained(int64_t e) const {
+	if (!mesh->nrefined || !mesh->active(e)) return false;
+	for (int iv = 0; iv < 8; iv++)
+		if (vd[mesh->hex[8 * e + iv]].ced) return true;
+	for (int ie = 0; ie < 12; ie++)
+		if (ed[mesh->elem_edge[12 * e + ie]].ced) return true;
+	for (int f = 0; f < 6; f++)
+		if (fd[mesh->elem_face[6 * e + f]].ced) return true;
+	return false;
+}
+
+// Space::update_constraints -> uc_element / uc_face (src/space.cc:1574-1987)
+// for one refinement level: every constrained node lies on a quarter of an
+// interface face (the face of an active element whose other side is
+// refined); its constraint is computed once, from the first such face.
+int Space::build_constraints(std::string &err) {
+	const Mesh &m = *mesh;
+	std::vector<AsmEntry> al;
+	for (const Mesh::Interface &I : m.interfaces) {
+		const int64_t N = I.big, P = I.small_parent;
+		const int fN = I.big_face, dN = kFaceFixedDir[fN], vN = kFaceFixedVal[fN];
+		const int d1N = kFaceDirs[fN][0], d2N = kFaceDirs[fN][1];
+		// traces of the big element's global functions on the interface face
+		struct Trace { int dof; double coef; int a1, a2; };
+		std::vector<Trace> tr;
+		element_assembly_list(N, al);
+		for (const AsmEntry &x : al) {
+			const Canon c = decode_index(x.idx);
+			const int ind[3] = { c.a, c.b, c.c };
+			if (ind[dN] != vN) continue;
+			tr.push_back(Trace { x.dof, c.sign * x.coef, ind[d1N], ind[d2N] });
+		}
+		// positions of the 9 points of the refined face in the big face's coordinates
+		std::unordered_map<int64_t, std::array<double, 2>> pos;
+		int64_t corner[4];
+		for (int k = 0; k < 4; k++) {
+			const int lv = kHexFaceVtx[fN][k];
+			corner[k] = m.hex[8 * N + lv];
+			pos[corner[k]] = { kRefVtx[lv][d1N], kRefVtx[lv][d2N] };
+		}
+		auto mid = [&](int64_t a, int64_t b) -> int64_t {
+			auto it = m.midpoints.find(std::make_pair(std::min(a, b), std::max(a, b)));
+			return it == m.midpoints.end() ? -1 : it->second;
+		};
+		int64_t emp[4];
+		for (int k = 0; k < 4; k++) {
+			const int64_t a = corner[k], b = corner[(k + 1) % 4];
+			emp[k] = mid(a, b);
+			if (emp[k] < 0) { err = "constraints: missing edge midpoint"; return -1; }
+			pos[emp[k]] = { 0.5 * (pos[a][0] + pos[b][0]), 0.5 * (pos[a][1] + pos[b][1]) };
+		}
+		const int64_t fmp = mid(emp[0], emp[2]);
+		if (fmp < 0) { err = "constraints: missing face midpoint"; return -1; }
+		pos[fmp] = { 0.0, 0.0 };
+		auto value = [&](const Trace &t, double x1, double x2) { return t.coef * lobatto_value(t.a1, x1) * lobatto_value(t.a2, x2); };
+
+		for (int k = 0; k < 4; k++) {
+			const int i = kHexFaceVtx[I.face][k];
+			const int64_t c = m.sons[8 * P + i];
+			// hanging vertices: values of the global functions
+			for (int q = 0; q < 4; q++) {
+				const int64_t vid = m.hex[8 * c + kHexFaceVtx[I.face][q]];
+				if (!vd[vid].ced || vcons.count(vid)) continue;
+				auto it = pos.find(vid);
+				if (it == pos.end()) { err = "constraints: vertex off the interface"; return -1; }
+				CedVertex cv;
+				for (const Trace &t : tr) {
+					const double v = value(t, it->second[0], it->second[1]);
+					if (v == 0.0) continue;
+					cv.dof.push_back(t.dof);
+					cv.val.push_back(v);
+				}
+				vcons[vid] = cv;
+			}
+			// constrained edges: bubble part of the restriction, parametrised
+			// from the lower to the higher vertex id
+			for (int q = 0; q < 4; q++) {
+				const int64_t eid = m.elem_edge[12 * c + kHexFaceEdges[I.face][q]];
+				if (!ed[eid].ced || econs.count(eid)) continue;
+				const auto &A = pos.at(m.edge_vtx[eid].first), &B = pos.at(m.edge_vtx[eid].second);
+				const int r = A[0] != B[0] ? 0 : 1;                  // varying face coordinate
+				const double emid = 0.5 * (A[r] + B[r]), ehalf = 0.5 * (B[r] - A[r]), fixed = A[1 - r];
+				CedEdge ce;
+				for (const Trace &t : tr) ce.order = std::max(ce.order, r == 0 ? t.a1 : t.a2);
+				const int nb = ce.order - 1;
+				std::vector<double> R(std::max(nb, 1));
+				for (const Trace &t : tr) {
+					const int kv = r == 0 ? t.a1 : t.a2, kf = r == 0 ? t.a2 : t.a1;
+					if (kv < 2) continue;
+					const double fv = t.coef * lobatto_value(kf, fixed);
+					if (fv == 0.0) continue;
+					restrict_bubbles(kv, emid, ehalf, R.data());
+					ce.dof.push_back(t.dof);
+					for (int mm = 2; mm <= ce.order; mm++) ce.c.push_back(mm <= kv ? fv * R[mm - 2] : 0.0);
+				}
+				econs[eid] = ce;
+			}
+			// the quarter face: products of bubble parts; axes from the lowest
+			// vertex id (h towards its lower-id neighbour, v towards the other)
+			const int64_t qf = m.elem_face[6 * c + I.face];
+			if (fd[qf].ced && !fcons.count(qf)) {
+				int64_t qv[4];
+				for (int q = 0; q < 4; q++) qv[q] = m.hex[8 * c + kHexFaceVtx[I.face][q]];
+				int o = 0;
+				for (int q = 1; q < 4; q++)
+					if (qv[q] < qv[o]) o = q;
+				int64_t vh = qv[(o + 1) % 4], vv = qv[(o + 3) % 4];
+				if (vv < vh) std::swap(vh, vv);
+				const auto &O = pos.at(qv[o]), &H = pos.at(vh), &V = pos.at(vv);
+				const int rh = O[0] != H[0] ? 0 : 1;                 // face coordinate along h
+				const double hmid = 0.5 * (O[rh] + H[rh]), hhalf = 0.5 * (H[rh] - O[rh]);
+				const double vmid = 0.5 * (O[1 - rh] + V[1 - rh]), vhalf = 0.5 * (V[1 - rh] - O[1 - rh]);
+				CedFace cf;
+				for (const Trace &t : tr) {
+					cf.oh = std::max(cf.oh, rh == 0 ? t.a1 : t.a2);
+					cf.ov = std::max(cf.ov, rh == 0 ? t.a2 : t.a1);
+				}
+				std::vector<double> Rh(std::max(cf.oh - 1, 1)), Rv(std::max(cf.ov - 1, 1));
+				for (const Trace &t : tr) {
+					const int kh = rh == 0 ? t.a1 : t.a2, kv = rh == 0 ? t.a2 : t.a1;
+					if (kh < 2 || kv < 2) continue;
+					restrict_bubbles(kh, hmid, hhalf, Rh.data());
+					restrict_bubbles(kv, vmid, vhalf, Rv.data());
+					cf.dof.push_back(t.dof);
+					for (int a = 2; a <= cf.oh; a++)
+						for (int b = 2; b <= cf.ov; b++) cf.c.push_back(a <= kh && b <= kv ? t.coef * Rh[a - 2] * Rv[b - 2] : 0.0);
+				}
+				fcons[qf] = cf;
+			}
+		}
+	}
+	return 0;
+}
+
+// assembly list of an element with constrained nodes (expanded form): the
+// unconstrained nodes as in element_assembly_list, each constrained node's
+// functions tied to the global functions of its constraint
+void Space::constrained_assembly_list(int64_t e, std::vector<AsmEntry> &al) const {
+	const Mesh &m = *mesh;
+	al.clear();
+	auto canon = [](int type, int ef, const int t[3]) { return encode_index(type, ef, t[0], t[1], t[2], 0); };
+	for (int iv = 0; iv < 8; iv++) {
+		const int64_t vid = m.hex[8 * e + iv];
+		const VData &v = vd[vid];
+		if (!v.ced) { al_add(al, vertex_index(iv), v.dof, v.dof >= 0 ? 1.0 : v.proj); continue; }
+		const CedVertex &cv = vcons.at(vid);
+		for (size_t k = 0; k < cv.dof.size(); k++) al_add(al, vertex_index(iv), cv.dof[k], cv.val[k]);
+	}
+	std::vector<int64_t> idx;
+	for (int ie = 0; ie < 12; ie++) {
+		const int64_t eid = m.elem_edge[12 * e + ie];
+		const EData &en = ed[eid];
+		if (!en.ced) {
+			if (en.n <= 0) continue;
+			edge_indices(ie, m.edge_orientation(e, ie), en.order, idx);
+			if (en.dof >= 0) {
+				for (int j = 0; j < en.n; j++) al_add(al, idx[j], en.dof + j * stride, 1.0);
+			}
+			else if (en.has_proj) {
+				for (int j = 0; j < en.n; j++) al_add(al, idx[j], DIRICHLET_DOF, en.proj[j]);
+			}
+			continue;
+		}
+		const CedEdge &ce = econs.at(eid);
+		const bool flip = m.hex[8 * e + kHexEdgeVtx[ie][0]] > m.hex[8 * e + kHexEdgeVtx[ie][1]];
+		const int nb = ce.order - 1;
+		for (size_t k = 0; k < ce.dof.size(); k++)
+			for (int mm = 2; mm <= ce.order; mm++) {
+				int t[3];
+				for (int d = 0; d < 3; d++) t[d] = kEdgePat[ie][d] < 0 ? mm : kEdgePat[ie][d];
+				const double sg = (flip && (mm & 1)) ? -1.0 : 1.0;
+				al_add(al, canon(SHFN_EDGE, ie, t), ce.dof[k], sg * ce.c[k * nb + mm - 2]);
+			}
+	}
+	for (int f = 0; f < 6; f++) {
+		const int64_t fid = m.elem_face[6 * e + f];
+		const FData &fn = fd[fid];
+		if (!fn.ced) {
+			if (fn.n <= 0) continue;
+			face_indices(f, m.face_orientation(e, f), fn.ox, fn.oy, idx);
+			if (fn.dof >= 0) {
+				for (int j = 0; j < fn.n; j++) al_add(al, idx[j], fn.dof + j * stride, 1.0);
+			}
+			else if (fn.has_proj) {
+				for (int j = 0; j < fn.n; j++) al_add(al, idx[j], DIRICHLET_DOF, fn.proj[j]);
+			}
+			continue;
+		}
+		const CedFace &cf = fcons.at(fid);
+		// local position of the face's axis vertices
+		int64_t qv[4];
+		int lvq[4];
+		for (int q = 0; q < 4; q++) { lvq[q] = kHexFaceVtx[f][q]; qv[q] = m.hex[8 * e + lvq[q]]; }
+		int o = 0;
+		for (int q = 1; q < 4; q++)
+			if (qv[q] < qv[o]) o = q;
+		int ih = (o + 1) % 4, iv = (o + 3) % 4;
+		if (qv[iv] < qv[ih]) std::swap(ih, iv);
+		int dh = -1, dv = -1;
+		double sh = 1.0, sv = 1.0;
+		for (int d = 0; d < 3; d++) {
+			if (kRefVtx[lvq[o]][d] != kRefVtx[lvq[ih]][d]) { dh = d; sh = kRefVtx[lvq[ih]][d] > kRefVtx[lvq[o]][d] ? 1.0 : -1.0; }
+			if (kRefVtx[lvq[o]][d] != kRefVtx[lvq[iv]][d]) { dv = d; sv = kRefVtx[lvq[iv]][d] > kRefVtx[lvq[o]][d] ? 1.0 : -1.0; }
+		}
+		const int nv_ = cf.ov - 1, nper = (cf.oh - 1) * nv_;
+		for (size_t k = 0; k < cf.dof.size(); k++)
+			for (int a = 2; a <= cf.oh; a++)
+				for (int b = 2; b <= cf.ov; b++) {
+					int t[3];
+					t[kFaceFixedDir[f]] = kFaceFixedVal[f];
+					t[dh] = a;
+					t[dv] = b;
+					const double sg = ((sh < 0 && (a & 1)) ? -1.0 : 1.0) * ((sv < 0 && (b & 1)) ? -1.0 : 1.0);
+					al_add(al, canon(SHFN_FACE, f, t), cf.dof[k], sg * cf.c[k * nper + (a - 2) * nv_ + (b - 2)]);
+				}
 	}
 	if (bd[e].n > 0) {
 		bubble_indices(&order[3 * e], idx);
@@ -609,8 +1041,10 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 	const Mesh &m = *sp.mesh;
 	const int64_t ne = scope ? (int64_t) scope->elems.size() : m.ne();
 	auto G = [&](int64_t e) -> int64_t { return scope ? scope->elems[e] : e; };   // plan element -> mesh element
+	if (m.nrefined) { err = "refined meshes take the batched path"; return -1; }
 	P = Plan();
 	P.ne = ne;
+	P.ne_ids = m.ne();
 	P.ndof = sp.ndof();
 	P.px = sp.order[0]; P.py = sp.order[1]; P.pz = sp.order[2];
 	for (int64_t e = 0; e < ne; e++)
@@ -824,19 +1258,23 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string &err, const PlanScope *scope) {
 	if (!sp.assigned) { err = "assign_dofs() has not been called"; return -1; }
 	const Mesh &m = *sp.mesh;
-	const int64_t ne = scope ? (int64_t) scope->elems.size() : m.ne();
-	auto G = [&](int64_t e) -> int64_t { return scope ? scope->elems[e] : e; };   // plan element -> mesh element
+	if (scope && m.nrefined) { err = "partitions of refined meshes are not supported"; return -1; }
+	std::vector<int64_t> act;                                  // plan element -> mesh element
+	if (scope) act = scope->elems;
+	else
+		for (int64_t e = 0; e < m.ne(); e++)
+			if (m.active(e)) act.push_back(e);
+	const int64_t ne = (int64_t) act.size();
+	auto G = [&](int64_t e) -> int64_t { return act[e]; };
 	P = Plan();
-	P.ne = ne;
 	P.ndof = sp.ndof();
+	P.ne_ids = m.ne();
 	P.mixed = true;
 	P.canon = true;
 	P.px = P.py = P.pz = -1;
 	P.nqx = P.nqy = P.nqz = -1;
 
-	// orders, rules, table sets, kernel class
-	std::vector<int64_t> eb(ne + 1, 0);
-	std::vector<std::array<int, 11>> desc(ne);
+	// table sets (p, nq) shared by all elements
 	std::vector<std::pair<int, int>> set_key;
 	std::vector<int> set_off;
 	auto table_set = [&](int p, int nq) -> int {
@@ -856,42 +1294,99 @@ int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string 
 		set_off.push_back(off);
 		return off;
 	};
+
+	// assembly lists; constrained elements in expanded form, grouped by DOF
+	struct CedTmp { int p[3]; std::vector<int32_t> udof; std::vector<std::vector<std::pair<int, double>>> col; };
+	std::vector<char> isced(ne, 0);
+	std::vector<CedTmp> ctmp(ne);
+	std::vector<std::vector<AsmEntry>> als(ne);
+	parallel_for(ne, [&](int64_t lo, int64_t hi) {
+		for (int64_t e = lo; e < hi; e++) {
+			isced[e] = sp.element_constrained(G(e));
+			sp.element_assembly_list(G(e), als[e]);
+		}
+	});
+	std::vector<std::array<int, 11>> desc(ne);
+	std::vector<int64_t> eb(ne + 1, 0);
 	for (int64_t e = 0; e < ne; e++) {
 		auto &d = desc[e];
+		int pe[3];
+		for (int r = 0; r < 3; r++) pe[r] = sp.order[3 * G(e) + r];
+		if (isced[e])
+			for (const AsmEntry &x : als[e]) {
+				const Canon c = decode_index(x.idx);
+				pe[0] = std::max(pe[0], c.a);
+				pe[1] = std::max(pe[1], c.b);
+				pe[2] = std::max(pe[2], c.c);
+			}
 		int nl = 1, pmax = 0, qmax = 0;
 		for (int r = 0; r < 3; r++) {
 			const int p = sp.order[3 * G(e) + r];
 			const int nq = p_plus ? p + qn : qn;
 			if (p < 1 || p > 10) { err = "element order out of range"; return -1; }
 			if (nq < 1 || nq > kMaxQuadPoints) { err = "Gauss points per direction must be in 1..13"; return -1; }
-			d[r] = p;
+			d[r] = pe[r];
 			d[3 + r] = nq;
-			d[6 + r] = table_set(p, nq);
-			nl *= p + 1;
-			pmax = std::max(pmax, p);
+			d[6 + r] = table_set(pe[r], nq);
+			nl *= pe[r] + 1;
+			pmax = std::max(pmax, pe[r]);
 			qmax = std::max(qmax, nq);
 		}
 		d[9] = nl;
 		int cls = -1;
-		for (int c = 0; c < Plan::kClasses && cls < 0; c++)
-			if (pmax <= Plan::kClassP[c] && qmax <= Plan::kClassQ[c]) cls = c;
-		if (cls < 0) { err = "mixed-order kernels cover orders <= 6 and <= 8 points per direction"; return -1; }
+		if (!isced[e]) {
+			for (int c = 0; c < Plan::kClasses && cls < 0; c++)
+				if (pmax <= Plan::kClassP[c] && qmax <= Plan::kClassQ[c]) cls = c;
+			if (cls < 0) { err = "mixed-order kernels cover orders <= 6 and <= 8 points per direction"; return -1; }
+			P.max_nl = std::max(P.max_nl, nl);
+		}
+		else {
+			for (int c = 0; c < Plan::kCedClasses && cls < 0; c++)
+				if (pmax <= Plan::kCedClassP[c] && qmax <= Plan::kCedClassQ[c]) cls = c;
+			if (cls < 0) { err = "constrained elements: orders <= 8 and <= 10 points per direction"; return -1; }
+			P.ce_max_nl = std::max(P.ce_max_nl, nl);
+		}
 		d[10] = cls;
-		eb[e + 1] = eb[e] + nl;
-		P.max_nl = std::max(P.max_nl, nl);
+		eb[e + 1] = eb[e] + std::max<int64_t>(nl, (int64_t) als[e].size());
 	}
 
-	// assembly lists
 	std::vector<int32_t> cnt(2 * ne), dofs(eb[ne], -1);
 	std::vector<uint16_t> ss(eb[ne], 0);
 	std::vector<double> cf(eb[ne], 0.0);
 	std::vector<int> bad(ne, 0);
 	parallel_for(ne, [&](int64_t lo, int64_t hi) {
-		std::vector<AsmEntry> al;
 		std::vector<char> seen;
 		for (int64_t e = lo; e < hi; e++) {
 			const int nl = desc[e][9], py = desc[e][1], pz = desc[e][2];
-			sp.element_assembly_list(G(e), al);
+			const std::vector<AsmEntry> &al = als[e];
+			if (isced[e]) {
+				CedTmp &t = ctmp[e];
+				std::unordered_map<int, int> col_of;
+				std::vector<std::pair<int, double>> lift;
+				for (const AsmEntry &x : al) {
+					const Canon c = decode_index(x.idx);
+					const int sidx = (c.a * (py + 1) + c.b) * (pz + 1) + c.c;
+					if (sidx < 0 || sidx >= nl) { bad[e] = 3; break; }
+					const double w = c.sign * x.coef;
+					if (x.dof < 0) { lift.push_back({ sidx, w }); continue; }
+					auto it = col_of.find(x.dof);
+					if (it == col_of.end()) {
+						it = col_of.emplace(x.dof, (int) t.udof.size()).first;
+						t.udof.push_back(x.dof);
+						t.col.emplace_back();
+					}
+					t.col[it->second].push_back({ sidx, w });
+				}
+				if (!lift.empty()) {
+					t.udof.push_back(DIRICHLET_DOF);
+					t.col.push_back(lift);
+				}
+				const int nu = (int) t.udof.size() - (lift.empty() ? 0 : 1);
+				cnt[2 * e] = nu;
+				cnt[2 * e + 1] = 0;
+				for (int k = 0; k < nu; k++) dofs[eb[e] + k] = t.udof[k];
+				continue;
+			}
 			int mcount = 0, lcount = 0;
 			for (auto &a : al) (a.dof >= 0 ? mcount : lcount)++;
 			if (mcount + lcount > nl) { bad[e] = 1; continue; }
@@ -984,39 +1479,48 @@ int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string 
 	}
 	P.ncolors = ncol;
 
-	// order: colour, class, decreasing work (nl^2 * points), element id
-	std::vector<int64_t> order_(ne);
-	for (int64_t e = 0; e < ne; e++) order_[e] = e;
+	// order: colour, class, decreasing work (nl^2 * points), element id;
+	// unconstrained and constrained elements in separate lists
+	std::vector<int64_t> order_, corder;
+	for (int64_t e = 0; e < ne; e++) (isced[e] ? corder : order_).push_back(e);
 	auto work = [&](int64_t e) { return (int64_t) desc[e][9] * desc[e][9] * desc[e][3]; };
-	std::sort(order_.begin(), order_.end(), [&](int64_t x, int64_t y) {
+	auto cmp = [&](int64_t x, int64_t y) {
 		if (color[x] != color[y]) return color[x] < color[y];
 		if (desc[x][10] != desc[y][10]) return desc[x][10] < desc[y][10];
 		int64_t wx = work(x), wy = work(y);
 		if (wx != wy) return wx > wy;
 		return x < y;
-	});
+	};
+	std::sort(order_.begin(), order_.end(), cmp);
+	std::sort(corder.begin(), corder.end(), cmp);
+	const int64_t nn = (int64_t) order_.size(), nc = (int64_t) corder.size();
+	P.ne = nn;
+	P.nce = nc;
 	P.launch_ptr.assign((size_t) ncol * Plan::kClasses + 1, 0);
-	for (int64_t e = 0; e < ne; e++) P.launch_ptr[(size_t) color[e] * Plan::kClasses + desc[e][10] + 1]++;
+	for (int64_t e : order_) P.launch_ptr[(size_t) color[e] * Plan::kClasses + desc[e][10] + 1]++;
 	for (size_t i = 0; i + 1 < P.launch_ptr.size(); i++) P.launch_ptr[i + 1] += P.launch_ptr[i];
 	P.color_ptr.assign(ncol + 1, 0);
 	for (int c = 0; c <= ncol; c++) P.color_ptr[c] = P.launch_ptr[(size_t) c * Plan::kClasses];
+	P.ce_launch_ptr.assign((size_t) ncol * Plan::kCedClasses + 1, 0);
+	for (int64_t e : corder) P.ce_launch_ptr[(size_t) color[e] * Plan::kCedClasses + desc[e][10] + 1]++;
+	for (size_t i = 0; i + 1 < P.ce_launch_ptr.size(); i++) P.ce_launch_ptr[i + 1] += P.ce_launch_ptr[i];
 
 	// per-element tables in assembly order
-	P.el_base.assign(ne + 1, 0);
-	P.el_obase.assign(ne + 1, 0);
-	for (int64_t k = 0; k < ne; k++) {
+	P.el_base.assign(nn + 1, 0);
+	P.el_obase.assign(nn + 1, 0);
+	for (int64_t k = 0; k < nn; k++) {
 		const int nl = desc[order_[k]][9];
 		P.el_base[k + 1] = P.el_base[k] + nl;
 		P.el_obase[k + 1] = P.el_obase[k] + (int64_t) nl * nl;
 	}
-	P.el_vtx.resize(8 * ne);
-	P.el_id.resize(ne);
-	P.el_cnt.resize(2 * ne);
-	P.el_desc.assign((size_t) ne * Plan::kDescInts, 0);
-	P.el_cdof.assign(P.el_base[ne], -1);
-	P.el_ccoef.assign(P.el_base[ne], 0.0);
-	P.el_offm.assign(P.el_obase[ne], 0);
-	parallel_for(ne, [&](int64_t lo, int64_t hi) {
+	P.el_vtx.resize(8 * nn);
+	P.el_id.resize(nn);
+	P.el_cnt.resize(2 * nn);
+	P.el_desc.assign((size_t) nn * Plan::kDescInts, 0);
+	P.el_cdof.assign(P.el_base[nn], -1);
+	P.el_ccoef.assign(P.el_base[nn], 0.0);
+	P.el_offm.assign(P.el_obase[nn], 0);
+	parallel_for(nn, [&](int64_t lo, int64_t hi) {
 		for (int64_t k = lo; k < hi; k++) {
 			const int64_t e = order_[k];
 			const int nl = desc[e][9];
@@ -1039,6 +1543,47 @@ int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string 
 					const int row = dofs[eb[e] + a], si = ss[eb[e] + a];
 					const int32_t *pos = std::lower_bound(c0, c1, row);
 					P.el_offm[ob + (int64_t) sj * nl + si] = (uint16_t) (pos - c0);
+				}
+			}
+		}
+	});
+
+	// constrained elements
+	P.ce_desc.assign((size_t) nc * Plan::kDescInts, 0);
+	P.ce_vtx.resize(8 * nc);
+	P.ce_id.resize(nc);
+	P.ce_ubase.assign(nc + 1, 0);
+	P.ce_obase.assign(nc + 1, 0);
+	P.ce_wptr.assign(1, 0);
+	for (int64_t k = 0; k < nc; k++) {
+		const int64_t e = corder[k];
+		const CedTmp &t = ctmp[e];
+		P.ce_id[k] = (int32_t) G(e);
+		for (int v = 0; v < 8; v++) P.ce_vtx[8 * k + v] = (int32_t) m.hex[8 * G(e) + v];
+		for (int q = 0; q < 11; q++) P.ce_desc[(size_t) k * Plan::kDescInts + q] = desc[e][q];
+		P.ce_ubase[k + 1] = P.ce_ubase[k] + (int64_t) t.udof.size();
+		const int64_t nu = cnt[2 * e];
+		P.ce_obase[k + 1] = P.ce_obase[k] + nu * nu;
+		for (size_t u = 0; u < t.udof.size(); u++) {
+			P.ce_udof.push_back(t.udof[u]);
+			for (const auto &sw : t.col[u]) {
+				P.ce_ws.push_back((uint16_t) sw.first);
+				P.ce_ww.push_back(sw.second);
+			}
+			P.ce_wptr.push_back((int64_t) P.ce_ws.size());
+		}
+	}
+	P.ce_off.assign(P.ce_obase[nc], 0);
+	parallel_for(nc, [&](int64_t lo, int64_t hi) {
+		for (int64_t k = lo; k < hi; k++) {
+			const CedTmp &t = ctmp[corder[k]];
+			const int64_t nu = P.ce_obase[k + 1] - P.ce_obase[k] == 0 ? 0 : cnt[2 * corder[k]];
+			for (int64_t v = 0; v < nu; v++) {
+				const int col = t.udof[v];
+				const int32_t *c0 = &P.Ai[P.Ap[col]], *c1 = &P.Ai[P.Ap[col + 1]];
+				for (int64_t u = 0; u < nu; u++) {
+					const int32_t *pos = std::lower_bound(c0, c1, t.udof[u]);
+					P.ce_off[P.ce_obase[k] + v * nu + u] = (uint16_t) (pos - c0);
 				}
 			}
 		}

@@ -10,6 +10,7 @@
 
 #include <array>
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -60,10 +61,29 @@ struct Mesh {
 	std::vector<int> edge_bnd;
 	bool finalized = false;
 
+	// refinement tree (Mesh::refine_element with REFT_HEX_XYZ, src/mesh.cc:1262-1633):
+	// children get the next element ids, new vertices the next vertex ids
+	std::vector<int64_t> parent;             // ne: parent element, -1 for a base element
+	std::vector<int64_t> sons;               // ne x 8: child elements (-1: none, element active)
+	std::map<std::pair<int64_t, int64_t>, int64_t> midpoints;   // vertex pair (ascending) -> midpoint vertex
+	int64_t nrefined = 0;
+
+	// derived by finalize() when elements are refined: hanging nodes
+	// (Space::fc_element, src/space.cc:598-736).  A face of an inactive element
+	// whose neighbour across it is active is a constraining face: the nodes its
+	// refinement created (edge midpoints, face midpoint, half edges, mid edges,
+	// quarter faces) are constrained.
+	std::vector<char> vertex_ced, edge_ced, facet_ced;
+	struct Interface { int64_t small_parent; int face; int64_t big; int big_face; };
+	std::vector<Interface> interfaces;
+	std::vector<std::pair<int64_t, int64_t>> edge_vtx;   // nedges: the two vertices (ascending)
+
 	int64_t nv() const { return (int64_t) xyz.size() / 3; }
 	int64_t ne() const { return (int64_t) hex.size() / 8; }
+	bool active(int64_t e) const { return sons.empty() || sons[8 * e] < 0; }
 
 	int finalize(std::string &err);
+	int refine_xyz(int64_t e, std::string &err);
 	int edge_orientation(int64_t e, int iedge) const;
 	int face_orientation(int64_t e, int iface) const;
 };
@@ -78,6 +98,14 @@ struct AsmEntry {
 	double coef;     // 1.0, or the Dirichlet lifting coefficient
 };
 
+// Restriction of global basis functions to a constrained node, in the node's
+// own parametrisation (edge: from its lower to its higher vertex id; face: see
+// ced_face_axes).  Entry k holds a global function (DOF, or DIRICHLET_DOF with
+// the lifting value folded in) and the coefficients of the node's functions.
+struct CedVertex { std::vector<int> dof; std::vector<double> val; };
+struct CedEdge { int order = 1; std::vector<int> dof; std::vector<double> c; };              // c: n x (order - 1), m = 2..order
+struct CedFace { int oh = 1, ov = 1; std::vector<int> dof; std::vector<double> c; };         // c: n x (oh - 1)(ov - 1)
+
 struct Space {
 	const Mesh *mesh = nullptr;
 	std::vector<int> order;                  // ne x 3 element orders
@@ -87,9 +115,9 @@ struct Space {
 	void *bc_value_ctx = nullptr;
 
 	// node data (src/space.h:110-300)
-	struct VData { int bc = BC_NONE, marker = MARKER_UNDEFINED, dof = -2; double proj = 0.0; };
-	struct EData { int bc = BC_NONE, marker = MARKER_UNDEFINED, order = -1, dof = -2, n = -1; std::vector<double> proj; bool has_proj = false; };
-	struct FData { int bc = BC_NONE, marker = MARKER_UNDEFINED, ox = -1, oy = -1, dof = -2, n = -1; std::vector<double> proj; bool has_proj = false; };
+	struct VData { int bc = BC_NONE, marker = MARKER_UNDEFINED, dof = -2; double proj = 0.0; bool ced = false; };
+	struct EData { int bc = BC_NONE, marker = MARKER_UNDEFINED, order = -1, dof = -2, n = -1; std::vector<double> proj; bool has_proj = false; bool ced = false; };
+	struct FData { int bc = BC_NONE, marker = MARKER_UNDEFINED, ox = -1, oy = -1, dof = -2, n = -1; std::vector<double> proj; bool has_proj = false; bool ced = false; };
 	struct BData { int dof = -2, n = -1; };
 	std::vector<VData> vd;
 	std::vector<EData> ed;
@@ -97,14 +125,27 @@ struct Space {
 	std::vector<BData> bd;
 	int first_dof = 0, next_dof = 0, stride = 1;
 	bool assigned = false;
+	// constraints of the hanging nodes (empty without refinement)
+	std::map<int64_t, CedVertex> vcons;
+	std::map<int64_t, CedEdge> econs;
+	std::map<int64_t, CedFace> fcons;
 
 	int ndof() const { return (next_dof - first_dof) / stride; }
+	bool constrained() const { return !vcons.empty() || !econs.empty() || !fcons.empty(); }
 	int assign_dofs(int first, int stride, std::string &err);
+	// For an element with constrained nodes the list is in expanded form: one
+	// entry per (canonical function, global function), idx = the canonical
+	// function with orientation 0, coef = the restriction coefficient (sign
+	// included).  A constrained function of the reference's list
+	// (src/space.cc:296-450, negative CED indices) is the sum of its entries.
 	void element_assembly_list(int64_t e, std::vector<AsmEntry> &al) const;
+	bool element_constrained(int64_t e) const;
 
 private:
 	void lift_edge(int64_t e, int iedge);
 	void lift_face(int64_t e, int iface);
+	int build_constraints(std::string &err);
+	void constrained_assembly_list(int64_t e, std::vector<AsmEntry> &al) const;
 };
 
 // ---------------------------------------------------------------- assembly plan
@@ -158,6 +199,29 @@ struct Plan {
 	std::vector<double> mixed_tables;        // per (p, nq) set: V[(p+1) nq], D[(p+1) nq], q[nq], w[nq]
 	std::vector<int64_t> launch_ptr;         // ncolors * kClasses + 1: (colour, class) ranges, assembly order
 	int max_nl = 0;
+	int64_t ne_ids = 0;                      // element ids of the mesh (coefficient arrays are indexed by them)
+
+	// elements with constrained nodes (hanging nodes): the element matrix is
+	// computed in the element's canonical basis, with the orders raised to
+	// those of the constraining functions, and mapped onto the global
+	// functions by W: column u of element k lists (canonical function, weight)
+	// pairs; a global DOF has one column, the Dirichlet lifting one more (DOF -1,
+	// always last).  K_uv = sum_a sum_b w_a w_b K[s_b][s_a].
+	static constexpr int kCedClasses = 3;
+	static constexpr int kCedClassP[kCedClasses] = { 4, 6, 8 };
+	static constexpr int kCedClassQ[kCedClasses] = { 6, 8, 10 };
+	int64_t nce = 0;
+	int ce_max_nl = 0;
+	std::vector<int32_t> ce_desc;            // nce x kDescInts (as el_desc, orders raised)
+	std::vector<int32_t> ce_vtx, ce_id;      // nce x 8, nce
+	std::vector<int64_t> ce_ubase;           // nce + 1: the element's columns
+	std::vector<int32_t> ce_udof;            // per column: DOF or -1
+	std::vector<int64_t> ce_wptr;            // columns + 1
+	std::vector<uint16_t> ce_ws;             // canonical function
+	std::vector<double> ce_ww;               // weight
+	std::vector<int64_t> ce_obase;           // nce + 1
+	std::vector<uint16_t> ce_off;            // per element [v][u] (DOF columns): row position of DOF u in column DOF v
+	std::vector<int64_t> ce_launch_ptr;      // ncolors * kCedClasses + 1
 };
 
 // One part of a z-slab partition of the mesh (multi-GPU sharding without

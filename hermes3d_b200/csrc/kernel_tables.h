@@ -14,6 +14,7 @@
 #include "kernels/asm_fp64_ho.cuh"
 #include "kernels/adjoint.cuh"
 #include "kernels/asm_fp64_mixed.cuh"
+#include "kernels/asm_fp64_ced.cuh"
 
 namespace h3dg_tables {
 
@@ -74,5 +75,20 @@ cudaError_t build_offt(const uint16_t *offc, const int32_t *cdof, const int64_t 
 std::vector<MixSpec> &mix_table();
 // adjoint (element sensitivity) kernels
 std::vector<AdjSpec> &adj_table();
+
+using CedFn = void (*)(h3dg::KArgsCed, int64_t, int64_t, int);
+
+struct CedSpec {
+	int cls;                      // Plan::kCedClassP / kCedClassQ
+	int nlm;                      // largest canonical basis of the class
+	CedFn fn;
+	int threads;
+	size_t (*smem)(int table_bytes);
+	bool configured;
+	size_t configured_smem;
+};
+
+// elements with constrained (hanging) nodes, one kernel per class
+std::vector<CedSpec> &ced_table();
 
 } // namespace h3dg_tables

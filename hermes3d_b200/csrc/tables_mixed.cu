@@ -18,4 +18,16 @@ std::vector<MixSpec> &mix_table() {
 	return t;
 }
 
+template <int CLS, int PM, int QM, int NT>
+static CedSpec ced_spec() {
+	return CedSpec { CLS, (PM + 1) * (PM + 1) * (PM + 1), &h3dg::k_assemble_fp64_ced<PM, QM, NT>, NT,
+	                 &h3dg::CedShape<PM, QM>::smem_bytes, false, 0 };
+}
+
+// classes: (orders <= 4, <= 6 points), (<= 6, <= 8), (<= 8, <= 10)
+std::vector<CedSpec> &ced_table() {
+	static std::vector<CedSpec> t = { ced_spec<0, 4, 6, 256>(), ced_spec<1, 6, 8, 256>(), ced_spec<2, 8, 10, 256>() };
+	return t;
+}
+
 } // namespace h3dg_tables

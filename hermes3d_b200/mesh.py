@@ -30,6 +30,9 @@ class Mesh:
         self.hexes = None
         self.bquads = None
         self.bmarkers = None
+        self.parent = None
+        self.refinements = []
+        self._base = None
 
     # --- reference-style incremental calls
     def add_vertex(self, x, y, z):
@@ -67,9 +70,37 @@ class Mesh:
         capi.call("h3dg_mesh_add_quad_boundaries", h, capi.ptr(self.bquads, C.c_int64),
                   capi.ptr(self.bmarkers, C.c_int32), len(self.bquads))
         capi.call("h3dg_mesh_finalize", h)
+        self._base = (self.xyz, self.hexes)
+        self.parent = np.zeros(len(self.hexes), np.int64)
         return self
 
     finalize = ugh
+
+    REFT_HEX_XYZ = 7
+
+    def refine_element(self, elem_id, refinement=REFT_HEX_XYZ):
+        """Mesh::refine_element (src/mesh.cc:1262-1279), REFT_HEX_XYZ of an active base
+        element; children get the next element ids, new vertices the next vertex ids."""
+        if self.handle is None:
+            self.ugh()
+        capi.call("h3dg_mesh_refine_element", self.handle, int(elem_id), int(refinement))
+        self.refinements.append((int(elem_id), int(refinement)))
+        nv, ne, _, _ = self.counts()
+        xyz = np.zeros((nv, 3), np.float64)
+        hexes = np.zeros((ne, 8), np.int64)
+        parent = np.zeros(ne, np.int64)
+        capi.call("h3dg_mesh_get_arrays", self.handle, capi.ptr(xyz, C.c_double), capi.ptr(hexes, C.c_int64),
+                  capi.ptr(parent, C.c_int64))
+        self.xyz, self.hexes, self.parent = xyz, hexes, parent
+        return True
+
+    @property
+    def active(self):
+        """Boolean mask over element ids 1..ne (index id - 1): not refined."""
+        act = np.ones(len(self.hexes), bool)
+        if self.parent is not None:
+            act[self.parent[self.parent > 0] - 1] = False
+        return act
 
     @property
     def num_elements(self):
@@ -91,13 +122,15 @@ class Mesh:
 
     # --- file formats
     def save_bin(self, path):
-        """Binary mesh file read by the oracle driver ("H3DMESH1")."""
+        """Binary mesh file read by the oracle driver ("H3DMESH1"): the base mesh
+        (refinements are passed to the driver separately)."""
+        xyz, hexes = self._base if self._base is not None else (self.xyz, self.hexes)
         with open(path, "wb") as f:
             f.write(b"H3DMESH1")
-            f.write(struct.pack("<q", len(self.xyz)))
-            f.write(self.xyz.tobytes())
-            f.write(struct.pack("<q", len(self.hexes)))
-            f.write(self.hexes.tobytes())
+            f.write(struct.pack("<q", len(xyz)))
+            f.write(xyz.tobytes())
+            f.write(struct.pack("<q", len(hexes)))
+            f.write(hexes.tobytes())
             bq = np.concatenate([self.bquads, self.bmarkers.astype(np.int64)[:, None]], axis=1)
             f.write(struct.pack("<q", len(bq)))
             f.write(np.ascontiguousarray(bq).tobytes())

@@ -97,6 +97,14 @@ h3dg_status h3dg_mesh_add_quad_boundaries(h3dg_mesh *mesh, const int64_t *vtx, c
 h3dg_status h3dg_mesh_finalize(h3dg_mesh *mesh);
 /* sizes: vertices, elements, facets, edges */
 h3dg_status h3dg_mesh_counts(const h3dg_mesh *mesh, int64_t *nv, int64_t *ne, int64_t *nfacets, int64_t *nedges);
+/* Mesh::refine_element (src/mesh.cc:1262-1279) with refinement REFT_HEX_XYZ (7,
+ * src/mesh.h:97) of an active base element (one refinement level): the 8 children
+ * get the next element ids, the new vertices the next vertex ids (refine_hex_8,
+ * src/mesh.cc:1555-1633).  Other refinement types return H3DG_ERR_MESH. */
+h3dg_status h3dg_mesh_refine_element(h3dg_mesh *mesh, int64_t elem_id, int reft);
+/* Current arrays (sizes from h3dg_mesh_counts): xyz nv x 3, hex ne x 8 (1-based
+ * vertex ids), parent ne (1-based parent id, 0 for base elements); any may be NULL */
+h3dg_status h3dg_mesh_get_arrays(const h3dg_mesh *mesh, double *xyz, int64_t *hex, int64_t *parent);
 
 /* ---------------------------------------------------------------- space */
 /* H1Space(mesh, H1ShapesetLobattoHex) (src/space/h1.cc:33-37) */

@@ -59,6 +59,8 @@ def run(mesh, p=2, orders=None, qmode="pplus:2", mass=False, gradcoef=None, sour
                 f.write(struct.pack("<q", len(c)))
                 f.write(c.tobytes())
             cmd += ["--gradcoef", fn]
+        if refine is None and getattr(mesh, "refinements", None):
+            refine = mesh.refinements
         if refine is not None:
             r = np.ascontiguousarray(refine, dtype=np.int64).reshape(-1, 2)
             fn = os.path.join(td, "ref.bin")

@@ -91,3 +91,35 @@ def nq_of(g):
 def rel_err(a, b):
     s = max(float(np.max(np.abs(b))) if len(b) else 0.0, 1e-300)
     return float(np.max(np.abs(a - b))) / s if len(a) else 0.0
+
+
+REFINED = os.path.join(GOLDEN, "refined")
+
+
+def refined_names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(REFINED, "*.npz")))
+
+
+def load_refined(name):
+    z = np.load(os.path.join(REFINED, name + ".npz"), allow_pickle=False)
+    d = {k: z[k] for k in z.files}
+    d["params"] = ast.literal_eval(str(d["params"]))
+    return d
+
+
+def refined_space_of(g):
+    """Base mesh of a refined fixture, its refinements (REFT_HEX_XYZ) and the space."""
+    p = g["params"]
+    mesh = mesh_of(g)
+    mesh.ugh()
+    for e in g["refine"]:
+        mesh.refine_element(int(e))
+    sp = h.H1Space(mesh)
+    bc = p.get("bc", "dirichlet0")
+    if bc == "natural":
+        sp.set_bc_types(lambda m: h.BC_NATURAL)
+    if bc == "dirichlet_poly":
+        sp.set_bc_values(lambda m, x, y, z: x * x + y * y + z * z)
+    sp.set_element_orders(g["orders"])
+    sp.assign_dofs()
+    return mesh, sp
