@@ -41,10 +41,12 @@ WORKLOADS = {
                     "f=sin(pi x)sin(pi y)sin(pi z), full CSC+RHS"),
     "c1": dict(side=8, jitter=0.0, p=3, nq=5, mass=False, lf=1.0, coef=None,
                desc="C1: 8^3 unit cube, p=3, 5^3 Gauss points, homogeneous Dirichlet, grad.grad, f=1"),
-    "c3": dict(side=32, jitter=0.0, p=(1, 6), nq=None, qplus=2, mass=False, lf=1.0, coef=None,
-               desc="C3 (unrefined): 32^3 hexahedra, anisotropic orders p_d ~ U{1..6} per element and direction "
+    "c3": dict(side=32, jitter=0.0, p=(1, 6), nq=None, qplus=2, mass=False, lf=1.0, coef=None, refine=0.10,
+               desc="C3: 32^3 hexahedra, 10% of them (3277, seeded) refined by REFT_HEX_XYZ -> 55707 active "
+                    "elements with hanging nodes, anisotropic orders p_d ~ U{1..6} per element and direction "
                     "(seeded), p_d+2 Gauss points per direction, grad.grad, f=1, homogeneous Dirichlet; "
-                    "mixed-order batched path (kernel classes, persistent CTAs, CUDA graph)"),
+                    "mixed-order batched path (kernel classes, constrained-element kernel, persistent CTAs, "
+                    "CUDA graph)"),
     "c4": dict(side=16, jitter=0.2, p=8, nq=10, mass=False, lf=None, coef=(0.5, 2.0),
                desc="C4: 16^3 jittered hexahedra, p=8, 10^3 Gauss points, a_e grad.grad, a_e ~ U[0.5,2]"),
     "c5": dict(side=32, jitter=0.2, p=3, nq=5, mass=False, lf=1.0, coef="lognormal",
@@ -158,6 +160,10 @@ def build_problem(h, seed, device, side=None, workload="c2", partition=None):
     side = w["side"] if side is None else side
     mesh = h.unit_cube(side, w["jitter"], seed)
     mesh.ugh()
+    if w.get("refine"):
+        nb = mesh.num_elements
+        ids = np.sort(np.random.default_rng(2000 + seed).choice(nb, int(round(w["refine"] * nb)), replace=False) + 1)
+        mesh.refine_elements(ids)
     sp = h.H1Space(mesh)
     if isinstance(w["p"], tuple):
         lo, hi = w["p"]
@@ -199,6 +205,32 @@ def dense_flops_per_element(workload="c2"):
     nl = (w["p"] + 1) ** 3
     nq = w["nq"] ** 3
     return 2 * nl * nl * 3 * nq + (2 * nl * nl * nq if w["mass"] else 0) + (2 * nl * nq if w["lf"] is not None else 0)
+
+
+C3_SAMPLE_SIDE = 8
+
+
+def cpu_baseline_c3(repeat=1):
+    """C3 on a bounded sample: the reference on one host core, 8^3 base
+    elements with 10 % refined and orders drawn as in the GPU run."""
+    import numpy as np
+    from hermes3d_b200.mesh import unit_cube
+    from oracle import ref_driver
+    if not ref_driver.available():
+        return None
+    n = C3_SAMPLE_SIDE
+    w = WORKLOADS["c3"]
+    mesh = unit_cube(n)
+    refs = np.sort(np.random.default_rng(2000).choice(n ** 3, int(round(w["refine"] * n ** 3)), replace=False) + 1)
+    ids = n ** 3 + 8 * len(refs)
+    orders = np.random.default_rng(1000).integers(w["p"][0], w["p"][1] + 1, size=(ids, 3)).astype(np.int32)
+    r = ref_driver.run(mesh, orders=orders, qmode="pplus:%d" % w["qplus"], source="one", bc="dirichlet0",
+                       refine=[(int(e), 7) for e in refs], repeat=repeat)
+    nact = n ** 3 + 7 * len(refs)
+    t = r["timing"]["t_assemble_median"]
+    return {"value": nact / t, "unit": "elements/s", "cores": 1, "kind": "reference",
+            "sample": "%d^3 base elements, %d refined (REFT_HEX_XYZ) -> %d active, orders U{1..6}, p+2 points, "
+                      "Discretization::assemble, median of %d" % (n, len(refs), nact, repeat)}
 
 
 def cpu_baseline(repeat=3):
@@ -459,7 +491,7 @@ def main():
     mesh, sp, d = build_problem(h, seed=0 if part else rank, device=local, side=args.side, workload=args.workload,
                                 partition=part)
     t_setup = time.time() - t_setup
-    ne, ndof, nnz, nv = mesh.num_elements, d.ndof, d.nnz, mesh.num_vertices
+    ne, ndof, nnz, nv = mesh.num_active_elements, d.ndof, d.nnz, mesh.num_vertices
     elems_here, nnz_job = ne, world * nnz
     if part:
         pinfo = d.partition()
@@ -604,9 +636,9 @@ def main():
         }
         if split_error is not None:
             out["split_error"] = split_error
-        if not args.no_cpu_baseline and world == 1 and args.workload == "c2":
+        if not args.no_cpu_baseline and world == 1 and args.workload in ("c2", "c3") and args.side is None:
             try:
-                out["cpu_baseline"] = cpu_baseline()
+                out["cpu_baseline"] = cpu_baseline() if args.workload == "c2" else cpu_baseline_c3()
             except Exception as ex:  # report, do not fail the GPU number
                 out["cpu_baseline"] = {"error": str(ex)[:200]}
         print(json.dumps(out))

@@ -51,6 +51,7 @@ SIGNATURES = {
     "h3dg_mesh_finalize": [_p],
     "h3dg_mesh_counts": [_p, _pi64, _pi64, _pi64, _pi64],
     "h3dg_mesh_refine_element": [_p, _i64, C.c_int],
+    "h3dg_mesh_refine_elements": [_p, _pi64, _i64, C.c_int],
     "h3dg_mesh_get_arrays": [_p, _pd, _pi64, _pi64],
     "h3dg_space_create": [_p, C.POINTER(_p)],
     "h3dg_space_destroy": [_p],

@@ -107,10 +107,10 @@ struct h3dg_disc {
 	DBuf<uint16_t> el_offm;
 	DBuf<unsigned> mx_counters;
 	// elements with constrained nodes: W columns, slot map, per-CTA scratch
-	DBuf<int32_t> ce_desc, ce_vtx, ce_id, ce_udof;
-	DBuf<int64_t> ce_ubase, ce_wptr, ce_obase;
+	DBuf<int32_t> ce_desc, ce_vtx, ce_id, ce_udof, ce_order;
+	DBuf<int64_t> ce_ubase, ce_wptr, ce_obase, ce_ebase;
 	DBuf<uint16_t> ce_ws, ce_off;
-	DBuf<double> ce_ww, ce_scratch;
+	DBuf<double> ce_ww, ce_scratch, ce_out;
 	int64_t ce_stride = 0;
 	int ce_per_sm[h3dg::Plan::kCedClasses] = { 1, 1, 1 };
 	int mx_variant[h3dg::Plan::kClasses] = { -1, -1, -1 };
@@ -118,8 +118,8 @@ struct h3dg_disc {
 	double *mx_ax = nullptr, *mx_rhs = nullptr;
 	const double *mx_coef = nullptr;   // coefficient array the graph was captured with
 	int32_t mx_launches = 0;
-	cudaStream_t mx_s[2] = { nullptr, nullptr };
-	cudaEvent_t mx_ev[3] = { nullptr, nullptr, nullptr };
+	cudaStream_t mx_s[3] = { nullptr, nullptr, nullptr };
+	cudaEvent_t mx_ev[5] = { nullptr, nullptr, nullptr, nullptr, nullptr };
 	void reset_mixed() {
 		if (mx_exec) cudaGraphExecDestroy(mx_exec);
 		mx_exec = nullptr;
@@ -208,6 +208,24 @@ h3dg_status h3dg_mesh_refine_element(h3dg_mesh *mesh, int64_t elem_id, int reft)
 	if (elem_id < 1 || elem_id > mesh->m.ne()) return fail(H3DG_ERR_INVALID_ARG, "refine_element: element id out of range");
 	std::string err;
 	if (mesh->m.refine_xyz(elem_id - 1, err) != 0) return fail(H3DG_ERR_MESH, err);
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_mesh_refine_elements(h3dg_mesh *mesh, const int64_t *elem_ids, int64_t n, int reft) {
+	if (!mesh || (n > 0 && !elem_ids) || n < 0) return fail(H3DG_ERR_INVALID_ARG, "refine_elements: bad arguments");
+	if (!mesh->m.finalized) return fail(H3DG_ERR_STATE, "refine_elements: mesh not finalized");
+	if (reft != 7) return fail(H3DG_ERR_MESH, "refine_elements: only REFT_HEX_XYZ (7) is supported");
+	std::string err;
+	for (int64_t i = 0; i < n; i++) {
+		if (elem_ids[i] < 1 || elem_ids[i] > mesh->m.ne()) err = "refine_elements: element id out of range";
+		else if (mesh->m.refine_xyz(elem_ids[i] - 1, err, false) != 0) {}
+		if (!err.empty()) {
+			std::string e2;
+			mesh->m.finalize(e2);
+			return fail(H3DG_ERR_MESH, err);
+		}
+	}
+	if (mesh->m.finalize(err) != 0) return fail(H3DG_ERR_MESH, err);
 	return H3DG_OK;
 }
 
@@ -471,6 +489,9 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 			H3DG_CUDA_TRY(disc->ce_ws.upload(P.ce_ws));
 			H3DG_CUDA_TRY(disc->ce_off.upload(P.ce_off));
 			H3DG_CUDA_TRY(disc->ce_ww.upload(P.ce_ww));
+			H3DG_CUDA_TRY(disc->ce_order.upload(P.ce_order));
+			H3DG_CUDA_TRY(disc->ce_ebase.upload(P.ce_ebase));
+			H3DG_CUDA_TRY(disc->ce_out.alloc((size_t) P.ce_ebase.back()));
 			// per-CTA scratch (element matrix + load vector) for every resident CTA
 			int nsm = 148;
 			cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
@@ -489,7 +510,7 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 				disc->ce_per_sm[cls] = per_sm < 1 ? 1 : per_sm;
 				blocks = std::max<int64_t>(blocks, (int64_t) nsm * disc->ce_per_sm[cls]);
 			}
-			disc->ce_stride = ((int64_t) P.ce_max_nl * P.ce_max_nl + P.ce_max_nl + 1) / 2 * 2;
+			disc->ce_stride = (P.ce_scratch + 1) / 2 * 2;
 			H3DG_CUDA_TRY(disc->ce_scratch.alloc((size_t) (disc->ce_stride * blocks)));
 		}
 		disc->el_offc.release();
@@ -743,15 +764,27 @@ static h3dg_status assemble_mixed(h3dg_disc *disc, double *d_Ax, double *d_rhs, 
 		ca.counters = disc->mx_counters.p + (size_t) P.ncolors * NC;
 		ca.scratch = disc->ce_scratch.p;
 		ca.scratch_stride = disc->ce_stride;
+		ca.order = disc->ce_order.p;
+		ca.ebase = disc->ce_ebase.p;
+		ca.out = disc->ce_out.p;
 		for (int cls = 0; cls < NCE; cls++) ce_per_sm[cls] = disc->ce_per_sm[cls];
 	}
-	auto launch_ced = [&](int c, int cls, cudaStream_t s) -> bool {
-		const int li = c * NCE + cls;
-		const int64_t kb = P.ce_launch_ptr[li], ke = P.ce_launch_ptr[li + 1];
+	// constrained elements: every element's entries in one launch per class
+	// (no colouring, it writes only its own output slice), then per colour a
+	// scatter of those entries after all colours of the other elements
+	auto launch_ced_compute = [&](int cls, cudaStream_t s) -> bool {
+		const int64_t kb = P.ce_class_ptr[cls], ke = P.ce_class_ptr[cls + 1];
 		if (ke <= kb) return false;
 		CedSpec &k = ced_table()[cls];
 		const int64_t grid = std::min<int64_t>(ke - kb, (int64_t) nsm * ce_per_sm[cls]);
-		k.fn<<<(unsigned) grid, k.threads, k.smem(disc->table_bytes), s>>>(ca, kb, ke, li);
+		k.fn<<<(unsigned) grid, k.threads, k.smem(disc->table_bytes), s>>>(ca, kb, ke, cls);
+		return true;
+	};
+	auto launch_ced_scatter = [&](int c, cudaStream_t s) -> bool {
+		const int64_t kb = P.ce_color_ptr[c], ke = P.ce_color_ptr[c + 1];
+		if (ke <= kb) return false;
+		const int64_t grid = std::min<int64_t>(ke - kb, (int64_t) nsm * 8);
+		ced_scatter_fn()<<<(unsigned) grid, kCedScatterThreads, 0, s>>>(ca, kb, ke);
 		return true;
 	};
 	// variants: time each class's launches once per plan, keep the fastest
@@ -796,6 +829,16 @@ static h3dg_status assemble_mixed(h3dg_disc *disc, double *d_Ax, double *d_rhs, 
 		if (d_Ax) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, s0));
 		if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, s0));
 		H3DG_CUDA_TRY(cudaMemsetAsync(disc->mx_counters.p, 0, ncnt, s0));
+		cudaStream_t s3 = fork ? disc->mx_s[2] : s0;
+		if (P.nce > 0) {
+			if (fork) {
+				H3DG_CUDA_TRY(cudaEventRecord(disc->mx_ev[3], s0));
+				H3DG_CUDA_TRY(cudaStreamWaitEvent(s3, disc->mx_ev[3], 0));
+			}
+			for (int cls = 0; cls < NCE; cls++)
+				if (launch_ced_compute(cls, s3)) n++;
+			if (fork) H3DG_CUDA_TRY(cudaEventRecord(disc->mx_ev[4], s3));
+		}
 		for (int c = 0; c < P.ncolors; c++) {
 			if (fork) {
 				H3DG_CUDA_TRY(cudaEventRecord(disc->mx_ev[0], s0));
@@ -805,15 +848,18 @@ static h3dg_status assemble_mixed(h3dg_disc *disc, double *d_Ax, double *d_rhs, 
 			cudaStream_t ss[NC] = { s0, s1, s2 };
 			for (int cls = 0; cls < NC; cls++)
 				if (launch(mix_table()[disc->mx_variant[cls]], per_sm[cls], c, cls, ss[cls])) n++;
-			if (P.nce > 0)
-				for (int cls = 0; cls < NCE; cls++)
-					if (launch_ced(c, cls, s0)) n++;
+
 			if (fork) {
 				H3DG_CUDA_TRY(cudaEventRecord(disc->mx_ev[1], s1));
 				H3DG_CUDA_TRY(cudaEventRecord(disc->mx_ev[2], s2));
 				H3DG_CUDA_TRY(cudaStreamWaitEvent(s0, disc->mx_ev[1], 0));
 				H3DG_CUDA_TRY(cudaStreamWaitEvent(s0, disc->mx_ev[2], 0));
 			}
+		}
+		if (P.nce > 0) {
+			if (fork) H3DG_CUDA_TRY(cudaStreamWaitEvent(s0, disc->mx_ev[4], 0));
+			for (int c = 0; c < P.ncolors; c++)
+				if (launch_ced_scatter(c, s0)) n++;
 		}
 		H3DG_CUDA_TRY(cudaGetLastError());
 		disc->mx_launches = n;

@@ -233,8 +233,8 @@ int Mesh::finalize(std::string &err) {
 // corner i; its vertex j is the point halfway between the parent's corners i
 // and j in the reference domain (corner, edge midpoint, face midpoint or
 // centre).  Only base elements are refined (one level).
-int Mesh::refine_xyz(int64_t e, std::string &err) {
-	if (!finalized) { err = "refine: mesh not finalized"; return -1; }
+int Mesh::refine_xyz(int64_t e, std::string &err, bool refinalize) {
+	if (!finalized && nrefined == 0) { err = "refine: mesh not finalized"; return -1; }
 	if (e < 0 || e >= ne()) { err = "refine: element id out of range"; return -1; }
 	if (parent.empty()) {
 		parent.assign(ne(), -1);
@@ -285,7 +285,7 @@ int Mesh::refine_xyz(int64_t e, std::string &err) {
 	}
 	nrefined++;
 	finalized = false;
-	return finalize(err);
+	return refinalize ? finalize(err) : 0;
 }
 
 // Hex::get_edge_orientation (src/mesh.cc:274-284)
@@ -1562,6 +1562,8 @@ int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string 
 		for (int v = 0; v < 8; v++) P.ce_vtx[8 * k + v] = (int32_t) m.hex[8 * G(e) + v];
 		for (int q = 0; q < 11; q++) P.ce_desc[(size_t) k * Plan::kDescInts + q] = desc[e][q];
 		P.ce_ubase[k + 1] = P.ce_ubase[k] + (int64_t) t.udof.size();
+		const int64_t nlk = desc[e][9];
+		P.ce_scratch = std::max<int64_t>(P.ce_scratch, nlk * nlk + nlk + (int64_t) t.udof.size() * nlk);
 		const int64_t nu = cnt[2 * e];
 		P.ce_obase[k + 1] = P.ce_obase[k] + nu * nu;
 		for (size_t u = 0; u < t.udof.size(); u++) {
@@ -1573,6 +1575,25 @@ int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string 
 			P.ce_wptr.push_back((int64_t) P.ce_ws.size());
 		}
 	}
+	P.ce_color_ptr.assign(ncol + 1, 0);
+	for (int c = 0; c <= ncol; c++) P.ce_color_ptr[c] = P.ce_launch_ptr[(size_t) c * Plan::kCedClasses];
+	P.ce_ebase.assign(nc + 1, 0);
+	for (int64_t k = 0; k < nc; k++) {
+		const int64_t nu = cnt[2 * corder[k]];
+		P.ce_ebase[k + 1] = P.ce_ebase[k] + nu * nu + nu;
+	}
+	P.ce_order.resize(nc);
+	for (int64_t k = 0; k < nc; k++) P.ce_order[k] = (int32_t) k;
+	std::sort(P.ce_order.begin(), P.ce_order.end(), [&](int32_t x, int32_t y) {
+		const int64_t ex = corder[x], ey = corder[y];
+		if (desc[ex][10] != desc[ey][10]) return desc[ex][10] < desc[ey][10];
+		const int64_t wx = work(ex), wy = work(ey);
+		if (wx != wy) return wx > wy;
+		return x < y;
+	});
+	P.ce_class_ptr.assign(Plan::kCedClasses + 1, 0);
+	for (int64_t k = 0; k < nc; k++) P.ce_class_ptr[desc[corder[k]][10] + 1]++;
+	for (int c = 0; c < Plan::kCedClasses; c++) P.ce_class_ptr[c + 1] += P.ce_class_ptr[c];
 	P.ce_off.assign(P.ce_obase[nc], 0);
 	parallel_for(nc, [&](int64_t lo, int64_t hi) {
 		for (int64_t k = lo; k < hi; k++) {

@@ -83,7 +83,7 @@ struct Mesh {
 	bool active(int64_t e) const { return sons.empty() || sons[8 * e] < 0; }
 
 	int finalize(std::string &err);
-	int refine_xyz(int64_t e, std::string &err);
+	int refine_xyz(int64_t e, std::string &err, bool refinalize = true);
 	int edge_orientation(int64_t e, int iedge) const;
 	int face_orientation(int64_t e, int iface) const;
 };
@@ -212,6 +212,7 @@ struct Plan {
 	static constexpr int kCedClassQ[kCedClasses] = { 6, 8, 10 };
 	int64_t nce = 0;
 	int ce_max_nl = 0;
+	int64_t ce_scratch = 0;                  // doubles of per-CTA scratch: max nl^2 + nl + columns x nl
 	std::vector<int32_t> ce_desc;            // nce x kDescInts (as el_desc, orders raised)
 	std::vector<int32_t> ce_vtx, ce_id;      // nce x 8, nce
 	std::vector<int64_t> ce_ubase;           // nce + 1: the element's columns
@@ -222,6 +223,10 @@ struct Plan {
 	std::vector<int64_t> ce_obase;           // nce + 1
 	std::vector<uint16_t> ce_off;            // per element [v][u] (DOF columns): row position of DOF u in column DOF v
 	std::vector<int64_t> ce_launch_ptr;      // ncolors * kCedClasses + 1
+	std::vector<int64_t> ce_color_ptr;       // ncolors + 1: the colour's elements (scatter launches)
+	std::vector<int32_t> ce_order;           // compute order: by class, then decreasing work
+	std::vector<int64_t> ce_class_ptr;       // kCedClasses + 1: ranges of ce_order
+	std::vector<int64_t> ce_ebase;           // nce + 1: output slice (nu x nu entries, then nu rhs values)
 };
 
 // One part of a z-slab partition of the mesh (multi-GPU sharding without

@@ -88,7 +88,11 @@ struct CedSpec {
 	size_t configured_smem;
 };
 
-// elements with constrained (hanging) nodes, one kernel per class
+// elements with constrained (hanging) nodes, one kernel per class, and the
+// scatter of their entries
 std::vector<CedSpec> &ced_table();
+using CedScatterFn = void (*)(h3dg::KArgsCed, int64_t, int64_t);
+CedScatterFn ced_scatter_fn();
+constexpr int kCedScatterThreads = 256;
 
 } // namespace h3dg_tables

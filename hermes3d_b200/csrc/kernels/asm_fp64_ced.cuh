@@ -5,16 +5,22 @@
 // src/space.cc:296-450 with the CED combinations of
 // src/shapeset/h1lobattohex.cc:428-719): column u of the element's W lists
 // (canonical function s, weight w) pairs for one global DOF, and one extra
-// column holds the Dirichlet lifting.  The kernel computes the element
-// matrix K and the load vector F in the element's canonical basis (orders
-// raised to those of the constraining functions, rule of the element's own
-// orders; the same sum-factorised stages as the mixed-order kernel) into a
-// per-CTA scratch block in global memory, then
-//   Ax[slot(u, v)] += sum_{a in u} sum_{b in v} w_a w_b K[s_b][s_a]
-//   rhs[u]         += sum_{a in u} w_a F[s_a] - sum_{a in u} sum_{b in lift} w_a w_b K[s_b][s_a]
-// once per (u, v) pair: the reference posts every pair of its assembly list
-// (src/discretization.cc:293-342), whose sum this is.  Elements of one
-// colour share no DOF, so each entry receives at most one add per launch.
+// column holds the Dirichlet lifting.
+//
+// Two kernels.  k_assemble_fp64_ced computes, for every constrained element
+// in one persistent launch (no colouring: it writes only its own output),
+// the element matrix K and load vector F in the element's canonical basis
+// (orders raised to those of the constraining functions, rule of the
+// element's own orders; the sum-factorised stages of the mixed-order kernel)
+// into a per-CTA scratch block, then the element's entries in the global
+// functions
+//   E[v][u] = sum_{a in u} w_a sum_{b in v} w_b K[s_b][s_a]
+//   r[u]    = sum_{a in u} w_a (F[s_a] - sum_{b in lift} w_b K[s_b][s_a])
+// into its slice of an output buffer: the reference posts every pair of its
+// assembly list (src/discretization.cc:293-342), whose sums these are.
+// k_scatter_ced then posts E and r for the elements of one colour; elements
+// of a colour share no DOF, so each entry receives at most one add per
+// launch and the result is bitwise reproducible.
 #pragma once
 
 #include "common.cuh"
@@ -42,8 +48,11 @@ struct KArgsCed {
 	double *Ax, *rhs;
 	int *status;
 	unsigned int *counters;
-	double *scratch;           // per CTA: K (nl x nl, [j][i]) then F (nl)
+	double *scratch;           // per CTA: K (nl x nl, [j][i]), F (nl), Y (columns x nl)
 	int64_t scratch_stride;    // doubles per CTA
+	const int32_t *order;      // compute order (class, decreasing work) -> element
+	const int64_t *ebase;      // nce + 1: the element's slice of out: E (nu x nu, [v][u]) then r (nu)
+	double *out;
 };
 
 template <int PM, int QM>
@@ -83,7 +92,8 @@ __global__ void __launch_bounds__(NT, 1) k_assemble_fp64_ced(KArgsCed args, int6
 		__syncthreads();
 		const int64_t k = s_k;
 		if (k >= kend) break;                                   // block-uniform
-		const int32_t *dsc = args.el_desc + k * 12;
+		const int64_t el = args.order[k];
+		const int32_t *dsc = args.el_desc + el * 12;
 		const int px = dsc[0], py = dsc[1], pz = dsc[2];
 		const int nqx = dsc[3], nqy = dsc[4], nqz = dsc[5];
 		const int NX = px + 1, NY = py + 1, NZ = pz + 1, NL = NX * NY * NZ;
@@ -92,14 +102,14 @@ __global__ void __launch_bounds__(NT, 1) k_assemble_fp64_ced(KArgsCed args, int6
 		const double *Vy = tab + dsc[7], *Dy = Vy + NY * nqy, *Qy = Dy + NY * nqy, *Wy = Qy + nqy;
 		const double *Vz = tab + dsc[8], *Dz = Vz + NZ * nqz, *Qz = Dz + NZ * nqz, *Wz = Qz + nqz;
 		double *Fs = Ks + (int64_t) NL * NL;
-		const int64_t u0 = args.ubase[k], u1 = args.ubase[k + 1];
+		const int64_t u0 = args.ubase[el], u1 = args.ubase[el + 1];
 		const bool has_lift = u1 > u0 && args.udof[u1 - 1] < 0;
 		const int nu = (int) (u1 - u0) - (has_lift ? 1 : 0);
 		const bool do_rhs = args.rhs && (args.lf || has_lift);
 		const bool need_k = args.Ax || (args.rhs && has_lift);
 
 		// ---- set-up: vertices, monomial coefficients of the trilinear map
-		if (tid < 24) X[tid] = args.xyz[3 * (int64_t) args.el_vtx[8 * k + tid / 3] + tid % 3];
+		if (tid < 24) X[tid] = args.xyz[3 * (int64_t) args.el_vtx[8 * el + tid / 3] + tid % 3];
 		__syncthreads();
 		for (int i = tid; i < 24; i += NT) {
 			const int mo = i / 3, r = i % 3;
@@ -115,7 +125,7 @@ __global__ void __launch_bounds__(NT, 1) k_assemble_fp64_ced(KArgsCed args, int6
 			}
 			Mo[i] = 0.125 * c;
 		}
-		const double cgrad = args.ecoef ? args.ecoef[args.el_id[k]] : 1.0;
+		const double cgrad = args.ecoef ? args.ecoef[args.el_id[el]] : 1.0;
 		__syncthreads();
 
 		// ---- geometry (FP64): w J^-1 J^-T |J| (x coefficient), mass and source weights
@@ -271,45 +281,72 @@ __global__ void __launch_bounds__(NT, 1) k_assemble_fp64_ced(KArgsCed args, int6
 			}
 		}
 
-		// ---- map onto the global functions and post
+		// ---- entries in the global functions, into the element's output slice:
+		// Y[v][i] = sum_{b in v} w_b K[s_b][i] (coalesced over the rows i), then
+		// E[v][u] = sum_{a in u} w_a Y[v][s_a]; the lifting column last
+		double *E = args.out + args.ebase[el];
+		double *Y = Fs + NL;
+		const int nv = (int) (u1 - u0);
+		if (need_k) {
+			const int vb = args.Ax ? 0 : nu;                 // without Ax only the lifting column
+			for (int p = tid; p < (nv - vb) * NL; p += NT) {
+				const int v = vb + p / NL, i = p % NL;
+				const int64_t b0 = args.wptr[u0 + v], b1 = args.wptr[u0 + v + 1];
+				double s = 0.0;
+				for (int64_t bi = b0; bi < b1; bi++) s += args.ww[bi] * Ks[(int64_t) args.ws[bi] * NL + i];
+				Y[(int64_t) v * NL + i] = s;
+			}
+			__syncthreads();
+		}
 		if (args.Ax) {
-			const uint16_t *offe = args.off + args.obase[k];
 			for (int p = tid; p < nu * nu; p += NT) {
 				const int v = p / nu, u = p % nu;
 				const int64_t a0 = args.wptr[u0 + u], a1 = args.wptr[u0 + u + 1];
-				const int64_t b0 = args.wptr[u0 + v], b1 = args.wptr[u0 + v + 1];
+				const double *yv = Y + (int64_t) v * NL;
 				double s = 0.0;
-				for (int64_t bi = b0; bi < b1; bi++) {
-					const double *kc = Ks + (int64_t) args.ws[bi] * NL;
-					double t = 0.0;
-					for (int64_t ai = a0; ai < a1; ai++) t += args.ww[ai] * kc[args.ws[ai]];
-					s += args.ww[bi] * t;
-				}
-				const int dv = args.udof[u0 + v];
-				const int64_t c0 = args.Ap[dv], c1 = args.Ap[dv + 1];
-				const int64_t pos = c0 + offe[(int64_t) v * nu + u];
-				if (pos < c1) posted_add(args.Ax + pos, s);
-				else if (c1 > c0) atomicOr(args.status, kErrBounds);
+				for (int64_t ai = a0; ai < a1; ai++) s += args.ww[ai] * yv[args.ws[ai]];
+				E[p] = s;
 			}
 		}
 		if (do_rhs) {
-			const int64_t l0 = has_lift ? args.wptr[u1 - 1] : 0, l1 = has_lift ? args.wptr[u1] : 0;
+			const double *yl = Y + (int64_t) nu * NL;
 			for (int u = tid; u < nu; u += NT) {
 				const int64_t a0 = args.wptr[u0 + u], a1 = args.wptr[u0 + u + 1];
 				double s = 0.0;
 				if (args.lf)
 					for (int64_t ai = a0; ai < a1; ai++) s += args.ww[ai] * Fs[args.ws[ai]];
-				double l = 0.0;
-				for (int64_t bi = l0; bi < l1; bi++) {
-					const double *kc = Ks + (int64_t) args.ws[bi] * NL;
-					double t = 0.0;
-					for (int64_t ai = a0; ai < a1; ai++) t += args.ww[ai] * kc[args.ws[ai]];
-					l += args.ww[bi] * t;
-				}
-				posted_add(args.rhs + args.udof[u0 + u], s - l);
+				if (has_lift)
+					for (int64_t ai = a0; ai < a1; ai++) s -= args.ww[ai] * yl[args.ws[ai]];
+				E[(int64_t) nu * nu + u] = s;
 			}
 		}
 		__syncthreads();
+	}
+}
+
+// posts the entries of the constrained elements kbeg..kend-1 (one colour):
+// one CTA per element at a time
+template <int NT>
+__global__ void __launch_bounds__(NT) k_scatter_ced(KArgsCed args, int64_t kbeg, int64_t kend) {
+	for (int64_t k = kbeg + blockIdx.x; k < kend; k += gridDim.x) {
+		const int64_t u0 = args.ubase[k], u1 = args.ubase[k + 1];
+		const bool has_lift = u1 > u0 && args.udof[u1 - 1] < 0;
+		const int nu = (int) (u1 - u0) - (has_lift ? 1 : 0);
+		const double *E = args.out + args.ebase[k];
+		if (args.Ax) {
+			const uint16_t *offe = args.off + args.obase[k];
+			for (int p = threadIdx.x; p < nu * nu; p += NT) {
+				const int v = p / nu, u = p % nu;
+				const int dv = args.udof[u0 + v];
+				const int64_t c0 = args.Ap[dv], c1 = args.Ap[dv + 1];
+				const int64_t pos = c0 + offe[p];
+				if (pos < c1) posted_add(args.Ax + pos, E[p]);
+				else if (c1 > c0) atomicOr(args.status, kErrBounds);
+				(void) u;
+			}
+		}
+		if (args.rhs && (args.lf || has_lift))
+			for (int u = threadIdx.x; u < nu; u += NT) posted_add(args.rhs + args.udof[u0 + u], E[(int64_t) nu * nu + u]);
 	}
 }
 

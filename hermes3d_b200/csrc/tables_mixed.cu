@@ -30,4 +30,6 @@ std::vector<CedSpec> &ced_table() {
 	return t;
 }
 
+CedScatterFn ced_scatter_fn() { return &h3dg::k_scatter_ced<kCedScatterThreads>; }
+
 } // namespace h3dg_tables

@@ -85,6 +85,20 @@ class Mesh:
             self.ugh()
         capi.call("h3dg_mesh_refine_element", self.handle, int(elem_id), int(refinement))
         self.refinements.append((int(elem_id), int(refinement)))
+        self._read_back()
+        return True
+
+    def refine_elements(self, elem_ids, refinement=REFT_HEX_XYZ):
+        """refine_element for each id in order, rebuilding the topology once."""
+        if self.handle is None:
+            self.ugh()
+        ids = np.ascontiguousarray(elem_ids, dtype=np.int64)
+        capi.call("h3dg_mesh_refine_elements", self.handle, capi.ptr(ids, C.c_int64), len(ids), int(refinement))
+        self.refinements += [(int(e), int(refinement)) for e in ids]
+        self._read_back()
+        return True
+
+    def _read_back(self):
         nv, ne, _, _ = self.counts()
         xyz = np.zeros((nv, 3), np.float64)
         hexes = np.zeros((ne, 8), np.int64)
@@ -92,7 +106,10 @@ class Mesh:
         capi.call("h3dg_mesh_get_arrays", self.handle, capi.ptr(xyz, C.c_double), capi.ptr(hexes, C.c_int64),
                   capi.ptr(parent, C.c_int64))
         self.xyz, self.hexes, self.parent = xyz, hexes, parent
-        return True
+
+    @property
+    def num_active_elements(self):
+        return int(self.active.sum())
 
     @property
     def active(self):

@@ -102,6 +102,8 @@ h3dg_status h3dg_mesh_counts(const h3dg_mesh *mesh, int64_t *nv, int64_t *ne, in
  * get the next element ids, the new vertices the next vertex ids (refine_hex_8,
  * src/mesh.cc:1555-1633).  Other refinement types return H3DG_ERR_MESH. */
 h3dg_status h3dg_mesh_refine_element(h3dg_mesh *mesh, int64_t elem_id, int reft);
+/* The same for n elements (1-based ids, in order), rebuilding the topology once */
+h3dg_status h3dg_mesh_refine_elements(h3dg_mesh *mesh, const int64_t *elem_ids, int64_t n, int reft);
 /* Current arrays (sizes from h3dg_mesh_counts): xyz nv x 3, hex ne x 8 (1-based
  * vertex ids), parent ne (1-based parent id, 0 for base elements); any may be NULL */
 h3dg_status h3dg_mesh_get_arrays(const h3dg_mesh *mesh, double *xyz, int64_t *hex, int64_t *parent);
