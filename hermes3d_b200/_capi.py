@@ -22,6 +22,7 @@ STATUS = {
 BC_ESSENTIAL, BC_NATURAL, BC_NONE = 0, 1, 2
 BF_GRAD_GRAD, BF_GRAD_GRAD_MASS = 1, 2
 LF_NONE, LF_CONST, LF_SIN = 0, 1, 2
+SBF_U_V, SLF_G_V = 1, 1
 QUAD_FIXED, QUAD_P_PLUS = 0, 1
 PREC_FP64 = 0
 PREC_TF32X3 = 1
@@ -51,6 +52,7 @@ SIGNATURES = {
     "h3dg_mesh_finalize": [_p],
     "h3dg_mesh_counts": [_p, _pi64, _pi64, _pi64, _pi64],
     "h3dg_mesh_refine_element": [_p, _i64, C.c_int],
+    "h3dg_disc_set_surface_forms": [_p, C.c_int, C.c_int, _pd, C.c_int],
     "h3dg_mesh_refine_elements": [_p, _pi64, _i64, C.c_int],
     "h3dg_mesh_get_arrays": [_p, _pd, _pi64, _pi64],
     "h3dg_space_create": [_p, C.POINTER(_p)],

@@ -74,6 +74,14 @@ struct h3dg_disc {
 	int lf = H3DG_LF_NONE;
 	double lf_value = 0.0;
 	int qmode = H3DG_QUAD_FIXED, qn = 0;
+	// surface forms (natural boundary faces)
+	int sbf = 0, slf = 0;
+	double sg[h3dg::kSurfMarkers] = {};
+	DBuf<int32_t> sf_desc, sf_vtx, sf_dof;
+	DBuf<int64_t> sf_base, sf_obase;
+	DBuf<double> sf_coef, sf_tables;
+	DBuf<int16_t> sf_ab;
+	DBuf<uint16_t> sf_off;
 	bool have_plan = false;
 	bool on_device = false;
 	int nparts = 1, part = 0;  // z-slab partition of the next plan (1: whole mesh)
@@ -376,6 +384,18 @@ h3dg_status h3dg_disc_set_linear_form(h3dg_disc *disc, int form, double value) {
 	return H3DG_OK;
 }
 
+h3dg_status h3dg_disc_set_surface_forms(h3dg_disc *disc, int bilinear, int linear, const double *g, int ng) {
+	if (!disc) return fail(H3DG_ERR_INVALID_ARG, "set_surface_forms: null disc");
+	if ((bilinear != H3DG_SBF_NONE && bilinear != H3DG_SBF_U_V) || (linear != H3DG_SLF_NONE && linear != H3DG_SLF_G_V))
+		return fail(H3DG_ERR_UNSUPPORTED_FORM, "set_surface_forms: unknown surface form");
+	if (ng < 0 || ng > h3dg::kSurfMarkers || (ng > 0 && !g))
+		return fail(H3DG_ERR_INVALID_ARG, "set_surface_forms: g needs 0..16 values (markers 0..15)");
+	disc->sbf = bilinear;
+	disc->slf = linear;
+	for (int m = 0; m < h3dg::kSurfMarkers; m++) disc->sg[m] = m < ng ? g[m] : 0.0;
+	return H3DG_OK;
+}
+
 h3dg_status h3dg_disc_set_quadrature(h3dg_disc *disc, int mode, int n) {
 	if (!disc || (mode != H3DG_QUAD_FIXED && mode != H3DG_QUAD_P_PLUS) || n < 0 || n > h3dg::kMaxQuadPoints)
 		return fail(H3DG_ERR_INVALID_ARG, "set_quadrature: bad arguments");
@@ -447,6 +467,9 @@ h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nn
 			return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
 	}
 	else if (h3dg::build_plan(sp, nq[0], nq[1], nq[2], disc->plan, err, canon, scope) != 0)
+		return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
+	if ((disc->sbf || disc->slf) &&
+	    h3dg::build_surface_plan(sp, disc->qmode == H3DG_QUAD_P_PLUS, disc->qn, disc->plan, err) != 0)
 		return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
 	const h3dg::Plan &P = disc->plan;
 	disc->on_device = false;
@@ -527,6 +550,17 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 		H3DG_CUDA_TRY(disc->el_dof.upload(P.el_dof));
 		H3DG_CUDA_TRY(disc->el_coef.upload(P.el_coef));
 		H3DG_CUDA_TRY(disc->el_off.upload(P.el_off));
+	}
+	if (P.nsf > 0) {
+		H3DG_CUDA_TRY(disc->sf_desc.upload(P.sf_desc));
+		H3DG_CUDA_TRY(disc->sf_vtx.upload(P.sf_vtx));
+		H3DG_CUDA_TRY(disc->sf_dof.upload(P.sf_dof));
+		H3DG_CUDA_TRY(disc->sf_base.upload(P.sf_base));
+		H3DG_CUDA_TRY(disc->sf_obase.upload(P.sf_obase));
+		H3DG_CUDA_TRY(disc->sf_coef.upload(P.sf_coef));
+		H3DG_CUDA_TRY(disc->sf_tables.upload(P.sf_tables));
+		H3DG_CUDA_TRY(disc->sf_ab.upload(P.sf_ab));
+		H3DG_CUDA_TRY(disc->sf_off.upload(P.sf_off));
 	}
 	std::vector<double> blob;
 	if (P.mixed) blob = P.mixed_tables;
@@ -912,7 +946,57 @@ static h3dg_status assemble_mixed(h3dg_disc *disc, double *d_Ax, double *d_rhs, 
 	return H3DG_OK;
 }
 
+static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream);
+
+// surface forms, after the volume assembly on the same stream, face colours in order
+static h3dg_status assemble_surface(h3dg_disc *disc, double *d_Ax, double *d_rhs, cudaStream_t st) {
+	const h3dg::Plan &P = disc->plan;
+	if (P.nsf == 0 || !d_Ax || !(disc->sbf || disc->slf)) return H3DG_OK;
+	h3dg::KArgsSurf a;
+	a.xyz = disc->xyz.p;
+	a.desc = disc->sf_desc.p;
+	a.vtx = disc->sf_vtx.p;
+	a.base = disc->sf_base.p;
+	a.obase = disc->sf_obase.p;
+	a.dof = disc->sf_dof.p;
+	a.coef = disc->sf_coef.p;
+	a.ab = disc->sf_ab.p;
+	a.off = disc->sf_off.p;
+	a.Ap = disc->Ap.p;
+	a.tables = disc->sf_tables.p;
+	a.bf = disc->sbf;
+	a.lf = disc->slf;
+	for (int m = 0; m < h3dg::kSurfMarkers; m++) a.g[m] = disc->sg[m];
+	a.Ax = d_Ax;
+	a.rhs = d_rhs;
+	a.status = disc->status.p;
+	int nqmax = 0;
+	for (int64_t k = 0; k < P.nsf; k++) nqmax = std::max(nqmax, P.sf_desc[k * h3dg::Plan::kSfDescInts + 4] * P.sf_desc[k * h3dg::Plan::kSfDescInts + 5]);
+	const size_t smem = sizeof(double) * (size_t) nqmax * (P.sf_max_n + 1);
+	SurfFn fn = surf_fn();
+	if (smem > 48 * 1024) H3DG_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+	int nsm = 148;
+	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
+	int32_t n = 0;
+	for (size_t c = 0; c + 1 < P.sf_color_ptr.size(); c++) {
+		const int64_t kb = P.sf_color_ptr[c], ke = P.sf_color_ptr[c + 1];
+		if (ke <= kb) continue;
+		const int64_t grid = std::min<int64_t>(ke - kb, (int64_t) nsm * 4);
+		fn<<<(unsigned) grid, kSurfThreads, smem, st>>>(a, kb, ke);
+		n++;
+	}
+	H3DG_CUDA_TRY(cudaGetLastError());
+	disc->last_launches += n;
+	return H3DG_OK;
+}
+
 h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream) {
+	h3dg_status s = assemble_volume(disc, precision, d_Ax, d_rhs, stream);
+	if (s != H3DG_OK) return s;
+	return assemble_surface(disc, d_Ax, d_rhs, (cudaStream_t) stream);
+}
+
+static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream) {
 	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "assemble: create_pattern() first");
 	if (precision != H3DG_PREC_FP64 && precision != H3DG_PREC_TF32X3 && precision != H3DG_PREC_OZAKI)
 		return fail(H3DG_ERR_INVALID_ARG, "assemble: unknown precision");

@@ -1612,4 +1612,133 @@ int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string 
 	return 0;
 }
 
+// ---------------------------------------------------------------- surface forms
+
+// Discretization::assemble's surface loop (src/discretization.cc:345-412):
+// every outer face of an active element whose marker's BC type is natural,
+// with the boundary assembly list (H1Space::get_boundary_assembly_list,
+// src/space/h1.cc:139-147: the face's vertex, edge and face functions, i.e.
+// the functions whose trace on the face is not zero).
+int build_surface_plan(const Space &sp, bool p_plus, int qn, Plan &P, std::string &err) {
+	const Mesh &m = *sp.mesh;
+	if (m.nrefined) { err = "surface forms on refined meshes are not supported"; return -1; }
+	P.nsf = 0;
+	P.sf_max_n = 0;
+	P.sf_desc.clear(); P.sf_vtx.clear(); P.sf_base.assign(1, 0); P.sf_dof.clear(); P.sf_coef.clear(); P.sf_ab.clear();
+	P.sf_obase.assign(1, 0); P.sf_off.clear(); P.sf_color_ptr.clear(); P.sf_tables.clear();
+	std::vector<std::pair<int, int>> set_key;
+	std::vector<int> set_off;
+	auto table_set = [&](int p, int nq) -> int {
+		for (size_t t = 0; t < set_key.size(); t++)
+			if (set_key[t].first == p && set_key[t].second == nq) return set_off[t];
+		int off = (int) P.sf_tables.size();
+		std::vector<double> q, w;
+		gauss_legendre(nq, q, w);
+		P.sf_tables.insert(P.sf_tables.end(), q.begin(), q.end());
+		P.sf_tables.insert(P.sf_tables.end(), w.begin(), w.end());
+		for (int k = 0; k <= p; k++)
+			for (int i = 0; i < nq; i++) P.sf_tables.push_back(lobatto_value(k, q[i]));
+		set_key.push_back({ p, nq });
+		set_off.push_back(off);
+		return off;
+	};
+	std::vector<AsmEntry> al;
+	std::vector<std::vector<int32_t>> face_dofs;
+	for (int64_t e = 0; e < m.ne(); e++) {
+		if (!m.active(e)) continue;
+		for (int f = 0; f < 6; f++) {
+			const int64_t fid = m.elem_face[6 * e + f];
+			if (!m.facet_outer[fid]) continue;
+			const int marker = m.facet_marker[fid];
+			const int bc = sp.bc_type_fn ? sp.bc_type_fn(marker, sp.bc_type_ctx) : BC_ESSENTIAL;
+			if (bc != BC_NATURAL) continue;
+			sp.element_assembly_list(e, al);
+			const int dn = kFaceFixedDir[f], side = kFaceFixedVal[f];
+			const int d1 = kFaceDirs[f][0], d2 = kFaceDirs[f][1];
+			std::vector<int32_t> fd_;
+			int n = 0;
+			for (const AsmEntry &x : al) {
+				const Canon c = decode_index(x.idx);
+				const int ind[3] = { c.a, c.b, c.c };
+				if (ind[dn] != side) continue;
+				P.sf_dof.push_back(x.dof);
+				P.sf_coef.push_back(c.sign * x.coef);
+				P.sf_ab.push_back((int16_t) ind[d1]);
+				P.sf_ab.push_back((int16_t) ind[d2]);
+				if (x.dof >= 0) fd_.push_back(x.dof);
+				n++;
+			}
+			const int p1 = sp.order[3 * e + d1], p2 = sp.order[3 * e + d2];
+			const int nq1 = p_plus ? p1 + qn : qn, nq2 = p_plus ? p2 + qn : qn;
+			if (nq1 < 1 || nq1 > kMaxQuadPoints || nq2 < 1 || nq2 > kMaxQuadPoints) { err = "surface rule out of range"; return -1; }
+			int32_t d[Plan::kSfDescInts] = { (int32_t) e, f, marker, n, nq1, nq2, table_set(p1, nq1), table_set(p2, nq2) };
+			P.sf_desc.insert(P.sf_desc.end(), d, d + Plan::kSfDescInts);
+			for (int v = 0; v < 8; v++) P.sf_vtx.push_back((int32_t) m.hex[8 * e + v]);
+			P.sf_base.push_back((int64_t) P.sf_dof.size());
+			P.sf_obase.push_back(P.sf_obase.back() + (int64_t) n * n);
+			P.sf_max_n = std::max(P.sf_max_n, n);
+			face_dofs.push_back(fd_);
+			P.nsf++;
+		}
+	}
+	// offsets into the volume pattern
+	P.sf_off.assign(P.sf_obase.back(), 0);
+	for (int64_t k = 0; k < P.nsf; k++) {
+		const int64_t b = P.sf_base[k], n = P.sf_base[k + 1] - b, ob = P.sf_obase[k];
+		for (int64_t j = 0; j < n; j++) {
+			const int dj = P.sf_dof[b + j];
+			if (dj < 0) continue;
+			const int32_t *c0 = &P.Ai[P.Ap[dj]], *c1 = &P.Ai[P.Ap[dj + 1]];
+			for (int64_t i = 0; i < n; i++) {
+				const int di = P.sf_dof[b + i];
+				if (di < 0) continue;
+				const int32_t *pos = std::lower_bound(c0, c1, di);
+				if (pos == c1 || *pos != di) { err = "surface entry outside the volume pattern"; return -1; }
+				P.sf_off[ob + j * n + i] = (uint16_t) (pos - c0);
+			}
+		}
+	}
+	// greedy colouring of the faces by shared DOFs, faces reordered by colour
+	std::unordered_map<int32_t, std::vector<int64_t>> dof_faces;
+	std::vector<int> col(P.nsf, -1);
+	int ncol = 0;
+	for (int64_t k = 0; k < P.nsf; k++) {
+		std::vector<char> used(ncol + 1, 0);
+		for (int32_t d : face_dofs[k]) {
+			auto it = dof_faces.find(d);
+			if (it == dof_faces.end()) continue;
+			for (int64_t o : it->second) used[col[o]] = 1;
+		}
+		int c = 0;
+		while (used[c]) c++;
+		col[k] = c;
+		ncol = std::max(ncol, c + 1);
+		for (int32_t d : face_dofs[k]) dof_faces[d].push_back(k);
+	}
+	std::vector<int64_t> ord(P.nsf);
+	for (int64_t k = 0; k < P.nsf; k++) ord[k] = k;
+	std::stable_sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) { return col[a] < col[b]; });
+	Plan Q;
+	Q.sf_base.assign(1, 0);
+	Q.sf_obase.assign(1, 0);
+	for (int64_t k : ord) {
+		const int64_t b = P.sf_base[k], n = P.sf_base[k + 1] - b, ob = P.sf_obase[k];
+		Q.sf_desc.insert(Q.sf_desc.end(), &P.sf_desc[k * Plan::kSfDescInts], &P.sf_desc[(k + 1) * Plan::kSfDescInts]);
+		Q.sf_vtx.insert(Q.sf_vtx.end(), &P.sf_vtx[8 * k], &P.sf_vtx[8 * k + 8]);
+		Q.sf_dof.insert(Q.sf_dof.end(), P.sf_dof.begin() + b, P.sf_dof.begin() + b + n);
+		Q.sf_coef.insert(Q.sf_coef.end(), P.sf_coef.begin() + b, P.sf_coef.begin() + b + n);
+		Q.sf_ab.insert(Q.sf_ab.end(), P.sf_ab.begin() + 2 * b, P.sf_ab.begin() + 2 * (b + n));
+		Q.sf_off.insert(Q.sf_off.end(), P.sf_off.begin() + ob, P.sf_off.begin() + ob + n * n);
+		Q.sf_base.push_back((int64_t) Q.sf_dof.size());
+		Q.sf_obase.push_back((int64_t) Q.sf_off.size());
+	}
+	P.sf_desc.swap(Q.sf_desc); P.sf_vtx.swap(Q.sf_vtx); P.sf_dof.swap(Q.sf_dof); P.sf_coef.swap(Q.sf_coef);
+	P.sf_ab.swap(Q.sf_ab); P.sf_off.swap(Q.sf_off); P.sf_base.swap(Q.sf_base); P.sf_obase.swap(Q.sf_obase);
+	P.sf_color_ptr.assign(ncol + 1, 0);
+	for (int64_t k = 0; k < P.nsf; k++) P.sf_color_ptr[col[k] + 1]++;
+	for (int c = 0; c < ncol; c++) P.sf_color_ptr[c + 1] += P.sf_color_ptr[c];
+	if (P.sf_tables.empty()) P.sf_tables.push_back(0.0);
+	return 0;
+}
+
 } // namespace h3dg

@@ -227,7 +227,29 @@ struct Plan {
 	std::vector<int32_t> ce_order;           // compute order: by class, then decreasing work
 	std::vector<int64_t> ce_class_ptr;       // kCedClasses + 1: ranges of ce_order
 	std::vector<int64_t> ce_ebase;           // nce + 1: output slice (nu x nu entries, then nu rhs values)
+
+	// surface forms on the outer faces of active elements whose marker is
+	// natural (src/discretization.cc:345-412): per face the trace functions of
+	// the element's assembly list (canonical index on the face's normal equal
+	// to the face's side), the element's rule on the face's two directions
+	static constexpr int kSfDescInts = 8;    // element (mesh index), face, marker, n, nq1, nq2, t1, t2
+	int64_t nsf = 0;
+	int sf_max_n = 0;
+	std::vector<int32_t> sf_desc;            // nsf x kSfDescInts; t1, t2: offsets of the direction tables
+	std::vector<int32_t> sf_vtx;             // nsf x 8
+	std::vector<int64_t> sf_base;            // nsf + 1: trace functions
+	std::vector<int32_t> sf_dof;             // DOF or -1
+	std::vector<double> sf_coef;             // sign x assembly-list coefficient
+	std::vector<int16_t> sf_ab;              // 2 per trace function: Lobatto index along the two face directions
+	std::vector<int64_t> sf_obase;           // nsf + 1
+	std::vector<uint16_t> sf_off;            // [j][i]: row position of dof_i in column dof_j (both >= 0)
+	std::vector<int64_t> sf_color_ptr;       // colours of faces (no two faces of a colour share a DOF)
+	std::vector<double> sf_tables;           // per (order, points) set: q[nq], w[nq], V[(p+1) nq]
 };
+
+// surface-form plan of the outer faces whose marker is natural (needs the
+// volume plan's pattern); nq per direction p_d + qn (p_plus) or qn
+int build_surface_plan(const Space &sp, bool p_plus, int qn, Plan &P, std::string &err);
 
 // One part of a z-slab partition of the mesh (multi-GPU sharding without
 // communication): the part's slab of elements plus the one-element halo that

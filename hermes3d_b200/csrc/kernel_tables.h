@@ -15,6 +15,7 @@
 #include "kernels/adjoint.cuh"
 #include "kernels/asm_fp64_mixed.cuh"
 #include "kernels/asm_fp64_ced.cuh"
+#include "kernels/asm_surface.cuh"
 
 namespace h3dg_tables {
 
@@ -94,5 +95,10 @@ std::vector<CedSpec> &ced_table();
 using CedScatterFn = void (*)(h3dg::KArgsCed, int64_t, int64_t);
 CedScatterFn ced_scatter_fn();
 constexpr int kCedScatterThreads = 256;
+
+// surface forms on natural boundary faces
+using SurfFn = void (*)(h3dg::KArgsSurf, int64_t, int64_t);
+SurfFn surf_fn();
+constexpr int kSurfThreads = 128;
 
 } // namespace h3dg_tables

@@ -506,7 +506,7 @@ __global__ void __launch_bounds__(NT, MINB) k_assemble_fp64(KArgs args, int64_t 
 				const int sa = ei[NL + a];
 				const double ca = Eb[S::E_C + a];
 				double lr = 0.0;
-				for (int j = s_m[e]; j < s_m[e] + s_l[e]; j++) {
+				for (int j = s_m[e]; j < s_m[e] + (args.Ax ? s_l[e] : 0); j++) {      // lifting only with the matrix (src/discretization.cc:296-317)
 					const int sj = ei[NL + j];
 					lr -= ca * Eb[S::E_C + j] * (A[sa * NL + sj] + A[sj * NL + sa]);
 				}

@@ -105,8 +105,8 @@ __global__ void __launch_bounds__(NT, 1) k_assemble_fp64_ced(KArgsCed args, int6
 		const int64_t u0 = args.ubase[el], u1 = args.ubase[el + 1];
 		const bool has_lift = u1 > u0 && args.udof[u1 - 1] < 0;
 		const int nu = (int) (u1 - u0) - (has_lift ? 1 : 0);
-		const bool do_rhs = args.rhs && (args.lf || has_lift);
-		const bool need_k = args.Ax || (args.rhs && has_lift);
+		const bool do_rhs = args.rhs && args.lf;      // no linear form: no rhs update at all (src/discretization.cc:328-338)
+		const bool need_k = args.Ax != nullptr;          // the lifting enters only with the matrix (src/discretization.cc:296-317)
 
 		// ---- set-up: vertices, monomial coefficients of the trilinear map
 		if (tid < 24) X[tid] = args.xyz[3 * (int64_t) args.el_vtx[8 * el + tid / 3] + tid % 3];
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(NT, 1) k_assemble_fp64_ced(KArgsCed args, int6
 				double s = 0.0;
 				if (args.lf)
 					for (int64_t ai = a0; ai < a1; ai++) s += args.ww[ai] * Fs[args.ws[ai]];
-				if (has_lift)
+				if (has_lift && args.Ax)
 					for (int64_t ai = a0; ai < a1; ai++) s -= args.ww[ai] * yl[args.ws[ai]];
 				E[(int64_t) nu * nu + u] = s;
 			}
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(NT) k_scatter_ced(KArgsCed args, int64_t kbeg,
 				(void) u;
 			}
 		}
-		if (args.rhs && (args.lf || has_lift))
+		if (args.rhs && args.lf)
 			for (int u = threadIdx.x; u < nu; u += NT) posted_add(args.rhs + args.udof[u0 + u], E[(int64_t) nu * nu + u]);
 	}
 }

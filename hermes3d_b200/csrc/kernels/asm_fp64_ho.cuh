@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(NT, 1) k_assemble_fp64_ho(KArgsHO args, int64_
 	for (int64_t k = kbeg + blockIdx.x; k < kend; k += gridDim.x) {
 		const double cgrad = ho_element_setup<S, NT>(args, k, X, Mo, cc, cd, cs, ce, &s_nlift);
 		ho_geometry<S, NT>(args, tab, Mo, cgrad, G);
-		if (do_rhs) ho_rhs<S, NT>(args, tab, G, U, cd, cc, s_nlift > 0);
+		if (do_rhs) ho_rhs<S, NT>(args, tab, G, U, cd, cc, s_nlift > 0 && args.Ax);
 
 		// ---- matrix: chunks of the test z index c
 		if (args.Ax) {

@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(NT, MINB) k_assemble_fp64_mixed(KArgsMixed arg
 			double *Pw = U + 4 * NQ;                       // P: [3][NX][nqy][nqz]
 			double *Qw = Pw + 3 * NX * nqy * nqz;          // Q: [2][NX][NY][nqz]
 			const int PS = NX * nqy * nqz, QS = NX * NY * nqz;
-			if (s_nlift > 0) {
+			if (s_nlift > 0 && args.Ax) {          // lifting only with the matrix (src/discretization.cc:296-317)
 				for (int i = tid; i < QS; i += NT) {
 					const int ab = i / nqz, q3 = i % nqz;
 					double s0 = 0.0, s1 = 0.0;

@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(32 * W, MINB) k_assemble_fp64_warp(KArgs args,
 				const int sa = ei[NL + a];
 				const double ca = Eb[S::E_C + a];
 				double lr = 0.0;
-				for (int j = s_m[e]; j < s_m[e] + s_l[e]; j++) {
+				for (int j = s_m[e]; j < s_m[e] + (args.Ax ? s_l[e] : 0); j++) {      // lifting only with the matrix (src/discretization.cc:296-317)
 					const int sj = ei[NL + j];
 					lr -= ca * Eb[S::E_C + j] * (A[sa * NL + sj] + A[sj * NL + sa]);
 				}

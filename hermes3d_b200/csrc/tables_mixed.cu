@@ -32,4 +32,6 @@ std::vector<CedSpec> &ced_table() {
 
 CedScatterFn ced_scatter_fn() { return &h3dg::k_scatter_ced<kCedScatterThreads>; }
 
+SurfFn surf_fn() { return &h3dg::k_assemble_surface<kSurfThreads>; }
+
 } // namespace h3dg_tables

@@ -114,6 +114,40 @@ int_grad_u_grad_v = BilinearForm(capi.BF_GRAD_GRAD, "int_grad_u_grad_v")
 int_grad_u_grad_v_plus_u_v = BilinearForm(capi.BF_GRAD_GRAD_MASS, "int_grad_u_grad_v + int_u_v")
 
 
+@dataclass(frozen=True)
+class SurfaceBilinearForm:
+    kind: int
+    name: str
+
+
+@dataclass(frozen=True)
+class SurfaceLinearForm:
+    kind: int
+    g: tuple
+    name: str
+
+
+surf_int_u_v = SurfaceBilinearForm(capi.SBF_U_V, "surf_int_u_v")
+
+
+def surf_int_G_v(g):
+    """Surface linear form int G v on natural boundary faces, G constant per boundary
+    marker: a dict {marker: value} or a sequence indexed by marker (markers 0..15)."""
+    if isinstance(g, dict):
+        vals = [0.0] * 16
+        for m, v in g.items():
+            if not 0 <= int(m) < 16:
+                raise capi.H3dgError(1, "surface markers must be 0..15")
+            vals[int(m)] = float(v)
+    elif np.isscalar(g):
+        vals = [float(g)] * 16
+    else:
+        vals = [float(v) for v in g]
+        if len(vals) > 16:
+            raise capi.H3dgError(1, "surface markers must be 0..15")
+    return SurfaceLinearForm(capi.SLF_G_V, tuple(vals), "surf_int_G_v")
+
+
 def int_F_v(F):
     """Linear form int F v for a constant F or F = "sin" (sin(pi x) sin(pi y) sin(pi z))."""
     if isinstance(F, str) and F == "sin":
@@ -169,21 +203,37 @@ class Discretization:
     def set_pss(self, *args):
         pass  # the precalculated shapeset is the device's 1D tables
 
-    def set_bilinear_form(self, form, coef=None):
+    def set_bilinear_form(self, form, coef=None, surf=None):
+        """set_bilinear_form(0, 0, unsym, sym, surf): ``surf`` = surf_int_u_v or None."""
         if not isinstance(form, BilinearForm):
             raise UnsupportedForm(4, "bilinear form %r is not one of the device forms" % (form,))
+        if surf is not None and not isinstance(surf, SurfaceBilinearForm):
+            raise UnsupportedForm(4, "surface form %r is not one of the device forms" % (surf,))
         c = None if coef is None else np.ascontiguousarray(coef, dtype=np.float64)
         capi.call("h3dg_disc_set_bilinear_form", self.handle, form.kind,
                   capi.ptr(c, C.c_double), 0 if c is None else len(c))
         self._coef = c
+        self._sbf = surf
+        self._set_surface()
 
-    def set_linear_form(self, form):
+    def set_linear_form(self, form, surf=None):
+        """set_linear_form(0, lf, surf): ``surf`` = surf_int_G_v(g) or None."""
+        if surf is not None and not isinstance(surf, SurfaceLinearForm):
+            raise UnsupportedForm(4, "surface form %r is not one of the device forms" % (surf,))
+        self._slf = surf
+        self._set_surface()
         if form is None:
             capi.call("h3dg_disc_set_linear_form", self.handle, capi.LF_NONE, 0.0)
             return
         if not isinstance(form, LinearForm):
             raise UnsupportedForm(4, "linear form %r is not one of the device forms" % (form,))
         capi.call("h3dg_disc_set_linear_form", self.handle, form.kind, form.value)
+
+    def _set_surface(self):
+        sbf, slf = getattr(self, "_sbf", None), getattr(self, "_slf", None)
+        g = np.ascontiguousarray(slf.g if slf is not None else [], dtype=np.float64)
+        capi.call("h3dg_disc_set_surface_forms", self.handle, capi.SBF_U_V if sbf is not None else 0,
+                  capi.SLF_G_V if slf is not None else 0, capi.ptr(g, C.c_double) if len(g) else None, len(g))
 
     def set_quadrature(self, points=None, p_plus=None):
         """Fixed Gauss points per direction, or p_d + p_plus per direction."""

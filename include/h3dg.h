@@ -47,6 +47,12 @@ typedef int h3dg_status;
 #define H3DG_BF_GRAD_GRAD       1   /* int_grad_u_grad_v, optionally times a per-element coefficient */
 #define H3DG_BF_GRAD_GRAD_MASS  2   /* int_grad_u_grad_v + int_u_v */
 
+/* surface forms (src/integrals/h1.h:184-242) */
+#define H3DG_SBF_NONE 0
+#define H3DG_SBF_U_V  1   /* surf_int_u_v */
+#define H3DG_SLF_NONE 0
+#define H3DG_SLF_G_V  1   /* surf_int_G_v, g constant per boundary marker */
+
 /* linear forms (int_F_v, src/integrals/h1.h:136-152) */
 #define H3DG_LF_NONE   0
 #define H3DG_LF_CONST  1   /* F(x,y,z) = c */
@@ -137,6 +143,15 @@ h3dg_status h3dg_disc_set_space(h3dg_disc *disc, h3dg_space *space);
 h3dg_status h3dg_disc_set_bilinear_form(h3dg_disc *disc, int form, const double *elem_coef, int64_t ne);
 /* set_linear_form(0, lf) (src/discretization.cc:151-161); value is the constant for H3DG_LF_CONST */
 h3dg_status h3dg_disc_set_linear_form(h3dg_disc *disc, int form, double value);
+/* surface forms on the outer faces whose marker is natural (set_bilinear_form's
+ * and set_linear_form's surf arguments, src/discretization.cc:136-161, assembled as
+ * src/discretization.cc:345-412): bilinear H3DG_SBF_U_V = surf_int_u_v, linear
+ * H3DG_SLF_G_V = surf_int_G_v with g constant per boundary marker (g[marker], ng values,
+ * markers 0..15; src/integrals/h1.h:200-242), each integrated with the element's rule on
+ * the face's two directions.  As in the reference, the surface pass runs only when the
+ * matrix is assembled, and its Dirichlet lifting reaches the RHS only with a surface
+ * linear form.  Set before create_pattern; not supported on refined meshes. */
+h3dg_status h3dg_disc_set_surface_forms(h3dg_disc *disc, int bilinear, int linear, const double *g, int ng);
 /* quadrature of the forms: mode H3DG_QUAD_FIXED (n points per direction) or
  * H3DG_QUAD_P_PLUS (p_d + n points per direction); the reference's forms fix the
  * order inside the form (tests/integrals/hex-h1-real/h1-hex-real.cc:55-103) */

@@ -25,6 +25,7 @@
 //       [--qmode fixed:N | pplus:K | ref] [--mass] [--gradcoef COEF.bin]
 //       [--source none|one|sin|poly] [--bc dirichlet0|dirichlet_poly|natural]
 //       [--refine REF.bin] [--repeat R] [--no-asm] [--elem-dump]
+//       [--surf-uv] [--surf-g g1,...,g6] [--natural-markers m1,m2,...]
 //
 // Output (little-endian binary, all counts int64):
 //   "H3DOUT01" ndof nnz Ap[ndof+1](i32) Ai[nnz](i32) Ax[nnz](f64) rhs[ndof](f64)
@@ -141,10 +142,44 @@ static scalar bf_ref(RealFunction *fu, RealFunction *fv, RefMap *ru, RefMap *rv)
 
 static scalar lf_ref(RealFunction *fv, RefMap *rv) { return int_F_v(source_fn, fv, rv); }
 
+// --- surface forms with an explicit order (pattern of surf_int_u_v /
+// surf_int_G_v, src/integrals/h1.h:184-242): the face rule is the element's
+// rule restricted to the face
+static double g_surf_g[7] = { 0, 0, 0, 0, 0, 0, 0 };   // g per boundary marker 1..6
+
+static scalar sbf_uv(RealFunction *fu, RealFunction *fv, RefMap *ru, RefMap *rv, FacePos *fp) {
+	Quad3D *quad = fu->get_quad();
+	order3_t o = elem_qorder(ru);
+	order2_t face_order = o.get_face_order(fp->face);
+	qorder_t qord = FACE_QORDER(fp->face, face_order);
+	fu->set_quad_order(qord, FN_VAL);
+	fv->set_quad_order(qord, FN_VAL);
+	double *uval = fu->get_fn_values();
+	double *vval = fv->get_fn_values();
+	H1_INTEGRATE_SURF_EXPRESSION(uval[i] * vval[i]);
+	return result;
+}
+
+static scalar slf_gv(RealFunction *fv, RefMap *rv, FacePos *fp) {
+	Quad3D *quad = fv->get_quad();
+	order3_t o = elem_qorder(rv);
+	order2_t face_order = o.get_face_order(fp->face);
+	qorder_t qord = FACE_QORDER(fp->face, face_order);
+	fv->set_quad_order(qord, FN_VAL);
+	double *vval = fv->get_fn_values();
+	double g = (fp->marker >= 1 && fp->marker <= 6) ? g_surf_g[fp->marker] : 0.0;
+	H1_INTEGRATE_SURF_EXPRESSION(vval[i] * g);
+	return result;
+}
+
 // --- boundary conditions
 static int g_bc = 0;   // 0 homogeneous Dirichlet, 1 Dirichlet x^2+y^2+z^2, 2 natural
+static int g_natural_mask = 0;   // markers (bit m) that are natural whatever g_bc says
 
-static EBCType bc_types(int marker) { return g_bc == 2 ? BC_NATURAL : BC_ESSENTIAL; }
+static EBCType bc_types(int marker) {
+	if (marker >= 0 && marker < 31 && (g_natural_mask >> marker) & 1) return BC_NATURAL;
+	return g_bc == 2 ? BC_NATURAL : BC_ESSENTIAL;
+}
 
 static scalar bc_values(int marker, double x, double y, double z) {
 	return g_bc == 1 ? x * x + y * y + z * z : 0.0;
@@ -194,7 +229,7 @@ static double now() {
 int main(int argc, char **argv) {
 	const char *mesh_fn = NULL, *out_fn = NULL, *orders_fn = NULL, *coef_fn = NULL, *refine_fn = NULL;
 	int p = 2, repeat = 1;
-	bool qref = false, do_asm = true, elem_dump = false;
+	bool qref = false, do_asm = true, elem_dump = false, surf_uv = false, surf_g = false;
 	for (int i = 1; i < argc; i++) {
 		std::string a = argv[i];
 		const char *v = i + 1 < argc ? argv[i + 1] : "";
@@ -219,6 +254,28 @@ int main(int argc, char **argv) {
 			std::string s = v; i++;
 			g_source = s == "none" ? 0 : s == "one" ? 1 : s == "sin" ? 2 : s == "poly" ? 3 : -1;
 			if (g_source < 0) { fprintf(stderr, "bad --source\n"); return 2; }
+		}
+		else if (a == "--surf-uv") surf_uv = true;
+		else if (a == "--surf-g") {
+			surf_g = true;
+			std::string t = v; i++;
+			size_t pos = 0;
+			for (int m = 1; m <= 6 && pos <= t.size(); m++) {
+				size_t c = t.find(',', pos);
+				g_surf_g[m] = atof(t.substr(pos, c == std::string::npos ? std::string::npos : c - pos).c_str());
+				if (c == std::string::npos) break;
+				pos = c + 1;
+			}
+		}
+		else if (a == "--natural-markers") {
+			std::string t = v; i++;
+			size_t pos = 0;
+			while (pos < t.size()) {
+				size_t c = t.find(',', pos);
+				g_natural_mask |= 1 << atoi(t.substr(pos, c == std::string::npos ? std::string::npos : c - pos).c_str());
+				if (c == std::string::npos) break;
+				pos = c + 1;
+			}
 		}
 		else if (a == "--bc") {
 			std::string s = v; i++;
@@ -323,9 +380,9 @@ int main(int argc, char **argv) {
 	d.set_num_equations(1);
 	d.set_spaces(1, &space);
 	d.set_pss(1, &pss);
-	if (qref) d.set_bilinear_form(0, 0, bf_ref);
-	else d.set_bilinear_form(0, 0, bf_fixed);
-	if (g_source != 0) d.set_linear_form(0, qref ? lf_ref : lf_fixed);
+	if (qref) d.set_bilinear_form(0, 0, bf_ref, NULL, surf_uv ? sbf_uv : NULL);
+	else d.set_bilinear_form(0, 0, bf_fixed, NULL, surf_uv ? sbf_uv : NULL);
+	if (g_source != 0 || surf_g) d.set_linear_form(0, g_source == 0 ? NULL : (qref ? lf_ref : lf_fixed), surf_g ? slf_gv : NULL);
 
 	DumpMatrix mat;
 	DumpVector rhs;

@@ -31,7 +31,8 @@ def build(ref="/root/reference"):
 
 
 def run(mesh, p=2, orders=None, qmode="pplus:2", mass=False, gradcoef=None, source="one", bc="dirichlet0",
-        repeat=1, elem_dump=False, assemble=True, refine=None, timeout=3600):
+        repeat=1, elem_dump=False, assemble=True, refine=None, surf_uv=False, surf_g=None, natural_markers=None,
+        timeout=3600):
     """Assemble ``mesh`` (hermes3d_b200.Mesh with arrays) with the reference.
 
     Returns dict(ndof, nnz, Ap, Ai, Ax, rhs, asm=[(id, idx, dof, coef)...],
@@ -70,6 +71,12 @@ def run(mesh, p=2, orders=None, qmode="pplus:2", mass=False, gradcoef=None, sour
             cmd += ["--refine", fn]
         if mass:
             cmd.append("--mass")
+        if surf_uv:
+            cmd.append("--surf-uv")
+        if surf_g is not None:
+            cmd += ["--surf-g", ",".join(repr(float(x)) for x in surf_g)]
+        if natural_markers:
+            cmd += ["--natural-markers", ",".join(str(int(m)) for m in natural_markers)]
         if elem_dump:
             cmd.append("--elem-dump")
         if not assemble:

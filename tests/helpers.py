@@ -123,3 +123,47 @@ def refined_space_of(g):
     sp.set_element_orders(g["orders"])
     sp.assign_dofs()
     return mesh, sp
+
+
+SURFACE = os.path.join(GOLDEN, "surface")
+
+
+def surface_names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(SURFACE, "*.npz")))
+
+
+def load_surface(name):
+    z = np.load(os.path.join(SURFACE, name + ".npz"), allow_pickle=False)
+    d = {k: z[k] for k in z.files}
+    d["params"] = ast.literal_eval(str(d["params"]))
+    return d
+
+
+def surface_problem(g, device=0):
+    """Space and discretization of a surface-form fixture: BC types per marker,
+    surf_int_u_v and / or surf_int_G_v with the fixture's g per marker 1..6."""
+    p = g["params"]
+    mesh = mesh_of(g)
+    mesh.ugh()
+    sp = h.H1Space(mesh)
+    nat = set(p.get("natural_markers") or [])
+    all_nat = p.get("bc") == "natural"
+    sp.set_bc_types(lambda m: h.BC_NATURAL if (all_nat or m in nat) else h.BC_ESSENTIAL)
+    if p.get("bc") == "dirichlet_poly":
+        sp.set_bc_values(lambda m, x, y, z: x * x + y * y + z * z)
+    if len(g["orders"]):
+        sp.set_element_orders(g["orders"])
+    else:
+        sp.set_uniform_order(p["p"])
+    sp.assign_dofs()
+    d = h.Discretization(device)
+    d.set_spaces(sp)
+    d.set_bilinear_form(h.int_grad_u_grad_v_plus_u_v if p.get("mass") else h.int_grad_u_grad_v,
+                        surf=h.surf_int_u_v if p.get("surf_uv") else None)
+    src = p.get("source", "one")
+    lf = {"one": h.int_F_v(1.0), "sin": h.int_F_v("sin"), "poly": h.int_F_v(-6.0)}[src]
+    sg = p.get("surf_g")
+    d.set_linear_form(lf, surf=h.surf_int_G_v([0.0] + list(sg)) if sg is not None else None)
+    kind, n = quad_of(g)
+    d.set_quadrature(p_plus=n) if kind == "pplus" else d.set_quadrature(points=n)
+    return mesh, sp, d
