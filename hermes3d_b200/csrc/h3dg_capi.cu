@@ -98,6 +98,7 @@ struct h3dg_disc {
 	DBuf<int32_t> Ai, el_vtx, el_cnt, el_dof, el_id;
 	DBuf<uint16_t> el_s, el_off, el_offc;
 	DBuf<uint16_t> el_offt;    // tensor-core scatter stream (built at the first split-precision assembly)
+	bool offt_store_all = false;   // its first-touch stores cover every Ax slot
 	DBuf<double> ho_scratch;   // per-CTA global work area of the FP64-accurate split kernel
 	DBuf<int32_t> el_cdof;
 	DBuf<double> el_ccoef;
@@ -538,12 +539,14 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 		}
 		disc->el_offc.release();
 		disc->el_offt.release();
+		disc->offt_store_all = false;
 	}
 	else if (P.canon) {
 		H3DG_CUDA_TRY(disc->el_cdof.upload(P.el_cdof));
 		H3DG_CUDA_TRY(disc->el_ccoef.upload(P.el_ccoef));
 		H3DG_CUDA_TRY(disc->el_offc.upload(P.el_offc));
 		disc->el_offt.release();
+		disc->offt_store_all = false;
 	}
 	else {
 		H3DG_CUDA_TRY(disc->el_s.upload(P.el_s));
@@ -654,14 +657,18 @@ static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, dou
 		// built once per plan; the build validates every position against its
 		// column, so the split kernel posts without a per-entry bounds test
 		size_t cnt = 0;
-		H3DG_CUDA_TRY(build_offt(disc->el_offc.p, disc->el_cdof.p, disc->Ap.p, P.ne, P.px, P.nqx, &disc->el_offt.p, &cnt,
-		                         disc->status.p, st));
+		unsigned long long stores = 0;
+		H3DG_CUDA_TRY(build_offt(disc->el_offc.p, disc->el_cdof.p, disc->Ap.p, P.ne, P.px, P.nqx, P.color_ptr.data(),
+		                         P.ncolors, P.nnz, &disc->el_offt.p, &cnt, &stores, disc->status.p, st));
 		disc->el_offt.n = cnt;
+		// every slot first-touched by a store: the split kernels need no zero-fill of Ax
+		disc->offt_store_all = (int64_t) stores == P.nnz;
 		int hs = 0;
 		H3DG_CUDA_TRY(cudaMemcpyAsync(&hs, disc->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
 		H3DG_CUDA_TRY(cudaStreamSynchronize(st));
 		if (hs & h3dg::kErrBounds) {
 			disc->el_offt.release();
+			disc->offt_store_all = false;
 			cudaMemsetAsync(disc->status.p, 0, sizeof(int), st);
 			return fail(H3DG_ERR_STATE, "assemble: a scatter position falls outside its column (plan corrupt)");
 		}
@@ -676,7 +683,9 @@ static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, dou
 	a.Ax = d_Ax;
 	a.rhs = disc->lf ? d_rhs : nullptr;
 	a.status = disc->status.p;
-	if (d_Ax) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
+	// the 3xTF32 epilogue stores each slot's first contribution (no zero-fill needed)
+	if (d_Ax && !(precision == H3DG_PREC_TF32X3 && disc->offt_store_all))
+		H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
 	if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
 	int nsm = 148;
 	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);

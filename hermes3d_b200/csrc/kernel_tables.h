@@ -70,8 +70,10 @@ std::vector<HoSpec> &ho_tc_table();
 // FP64-accurate high-order kernels (int8-sliced tcgen05 stage 3)
 std::vector<HoSpec> &ho_oz_table();
 // tensor-core scatter stream from the canonical position map (async on st)
+// (colour by colour, with first-touch store flags; *stores = the number of flagged entries)
 cudaError_t build_offt(const uint16_t *offc, const int32_t *cdof, const int64_t *Ap, int64_t ne, int px, int nq,
-                       uint16_t **offt, size_t *count, int *status, cudaStream_t st);
+                       const int64_t *color_ptr, int ncolors, int64_t nnz, uint16_t **offt, size_t *count,
+                       unsigned long long *stores, int *status, cudaStream_t st);
 // mixed-order kernels, several variants per class (timed once per plan)
 std::vector<MixSpec> &mix_table();
 // adjoint (element sensitivity) kernels

@@ -368,7 +368,8 @@ __global__ void __launch_bounds__(256, MINB) k_assemble_ho_oz(KArgsHO args, int6
 								const double kv = t * rsc * fsc[n];           // exact power-of-two scalings
 								const int a2 = n / NX, a = n - a2 * NX;
 								const int i_ = (a * NY + b) * NZ + c, j_ = (a2 * NY + b2) * NZ + c2;
-								posted_add(args.Ax + cs[j_] + off, cc[i_] * cc[j_] * kv);
+								// first-touch flags ignored: measured slower here than the zero-fill
+								posted_add(args.Ax + cs[j_] + (off & kOffMask), cc[i_] * cc[j_] * kv);
 							}
 						}
 					}

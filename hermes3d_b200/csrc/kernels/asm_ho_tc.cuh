@@ -88,13 +88,26 @@ struct HoTcShape {
 // kOffSkip where either function has no matrix entry (Dirichlet) or n is
 // padding.  Records are NB * 2 bytes (a multiple of 32), so a thread reads
 // its half with 16-byte loads.
+//
+// First touch: built colour by colour (assembly order), an entry whose Ax
+// slot no earlier element wrote carries kOffStore; the epilogue stores it
+// instead of adding.  When every slot of the pattern is first-touched this
+// way the assembly needs no zero-fill of Ax (saving a write and, for each
+// first touch, the read of the posted add); 0 + v = v, so the values are
+// the same.
 constexpr uint16_t kOffSkip = 0xFFFF;
+constexpr uint16_t kOffStore = 0x8000;
+constexpr uint16_t kOffMask = 0x7FFF;
 
-static __global__ void k_build_offt(const uint16_t *offc, const int32_t *cdof, const int64_t *Ap, int64_t ne, int nx, int ny,
-                             int nz, int nb, uint16_t *offt, int *status) {
+static __global__ void k_build_offt(const uint16_t *offc, const int32_t *cdof, const int64_t *Ap, int64_t kbeg, int64_t kend,
+                                    int nx, int ny, int nz, int nb, uint16_t *offt, int *status, uint8_t *touched,
+                                    unsigned long long *stores) {
 	const int nl = nx * ny * nz, ncol = ny * ny * nz;
-	const int64_t total = ne * nz * ncol * nb;
-	for (int64_t e = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; e < total; e += (int64_t) gridDim.x * blockDim.x) {
+	const int64_t per = (int64_t) nz * ncol * nb;
+	const int64_t total = (kend - kbeg) * per;
+	unsigned long long nst = 0;
+	for (int64_t e0 = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; e0 < total; e0 += (int64_t) gridDim.x * blockDim.x) {
+		const int64_t e = kbeg * per + e0;
 		const int n = (int) (e % nb);
 		int64_t r = e / nb;
 		const int col = (int) (r % ncol);
@@ -112,14 +125,24 @@ static __global__ void k_build_offt(const uint16_t *offc, const int32_t *cdof, c
 				// every position is checked against its column once, here, so the
 				// epilogue can post without a bounds test
 				const int64_t len = Ap[dj + 1] - Ap[dj];
-				if (v == kOffSkip || (int64_t) v >= len) {
+				if (v == kOffSkip || (int64_t) v >= len || v > kOffMask - 1) {
 					if (len > 0) atomicOr(status, kErrBounds);     // an empty column is one this plan does not own
 					v = kOffSkip;
+				}
+				else if (touched) {
+					// elements of this launch (one colour) write disjoint slots
+					const int64_t slot = Ap[dj] + v;
+					if (!touched[slot]) {
+						touched[slot] = 1;
+						v |= kOffStore;
+						nst++;
+					}
 				}
 			}
 		}
 		offt[e] = v;
 	}
+	if (stores && nst) atomicAdd(stores, nst);
 }
 
 // stage 1 (FP32) for a fixed TRIAL z index c':
@@ -295,7 +318,10 @@ __device__ __forceinline__ void ho_tc_epilogue(uint32_t tacc, const uint4 *offv,
 		for (int a = 0; a < NX; a++) {
 			const int n = a2 * NX + a;
 			const uint16_t off = o16[n - E::E0];
-			if (off != kOffSkip) posted_add(Ax + csj + off, cci[a] * ccj * (double) v[n - E::CHB * 16]);
+			if (off == kOffSkip) continue;
+			const double val = cci[a] * ccj * (double) v[n - E::CHB * 16];
+			if (off & kOffStore) posted_store(Ax + csj + (off & kOffMask), val);     // first touch of the slot
+			else posted_add(Ax + csj + off, val);
 		}
 	}
 }

@@ -151,6 +151,12 @@ __device__ __forceinline__ void posted_add(double *addr, double v) {
 	asm volatile("red.global.add.f64 [%0], %1;" ::"l"(addr), "d"(v) : "memory");
 }
 
+// Plain store of an entry's first contribution (same ordering constraints
+// for the compiler as posted_add)
+__device__ __forceinline__ void posted_store(double *addr, double v) {
+	asm volatile("st.global.f64 [%0], %1;" ::"l"(addr), "d"(v) : "memory");
+}
+
 __device__ __forceinline__ double source_value(int lf, double value, const double xp[3]) {
 	if (lf == 1) return value;
 	if (lf == 2) return sinpi(xp[0]) * sinpi(xp[1]) * sinpi(xp[2]);   // sin(pi x) sin(pi y) sin(pi z)
