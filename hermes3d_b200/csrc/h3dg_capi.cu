@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <algorithm>
@@ -74,6 +75,14 @@ struct h3dg_disc {
 	int lf = H3DG_LF_NONE;
 	double lf_value = 0.0;
 	int qmode = H3DG_QUAD_FIXED, qn = 0;
+	// evaluation plan (norms), built at the first norms call after create_pattern
+	bool have_eval = false;
+	int64_t ev_ne = 0;
+	int ev_nlmax = 0, ev_amax = 0, ev_bmax = 0;
+	DBuf<int32_t> ev_desc, ev_vtx, ev_edof;
+	DBuf<int64_t> ev_gptr, ev_eptr;
+	DBuf<uint16_t> ev_gs;
+	DBuf<double> ev_ecoef, ev_tables, ev_partial, ev_out;
 	// surface forms (natural boundary faces)
 	int sbf = 0, slf = 0;
 	double sg[h3dg::kSurfMarkers] = {};
@@ -475,6 +484,7 @@ h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nn
 	const h3dg::Plan &P = disc->plan;
 	disc->on_device = false;
 	disc->have_plan = true;
+	disc->have_eval = false;
 	disc->variant = -1;
 	if (ndof) *ndof = P.ndof;
 	if (nnz) *nnz = P.nnz;
@@ -996,6 +1006,67 @@ static h3dg_status assemble_surface(h3dg_disc *disc, double *d_Ax, double *d_rhs
 	}
 	H3DG_CUDA_TRY(cudaGetLastError());
 	disc->last_launches += n;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_norms(h3dg_disc *disc, const double *d_sol, int exact, double *out, void *stream) {
+	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "norms: create_pattern() first");
+	if (!d_sol || !out || exact < H3DG_EXACT_ZERO || exact > H3DG_EXACT_SIN) return fail(H3DG_ERR_INVALID_ARG, "norms: bad arguments");
+	{ h3dg_status s0 = ensure_device(disc); if (s0 != H3DG_OK) return s0; }
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	cudaStream_t st = (cudaStream_t) stream;
+	if (!disc->have_eval) {
+		h3dg::EvalPlan E;
+		std::string err;
+		if (h3dg::build_eval_plan(disc->space->s, disc->qmode == H3DG_QUAD_P_PLUS, disc->qn, E, err) != 0)
+			return fail(H3DG_ERR_INVALID_ARG, "norms: " + err);
+		H3DG_CUDA_TRY(disc->ev_desc.upload(E.desc));
+		H3DG_CUDA_TRY(disc->ev_vtx.upload(E.vtx));
+		H3DG_CUDA_TRY(disc->ev_edof.upload(E.edof));
+		H3DG_CUDA_TRY(disc->ev_gptr.upload(E.gptr));
+		H3DG_CUDA_TRY(disc->ev_eptr.upload(E.eptr));
+		H3DG_CUDA_TRY(disc->ev_gs.upload(E.gs));
+		H3DG_CUDA_TRY(disc->ev_ecoef.upload(E.ecoef));
+		H3DG_CUDA_TRY(disc->ev_tables.upload(E.tables));
+		H3DG_CUDA_TRY(disc->ev_partial.alloc((size_t) std::max<int64_t>(1, 4 * E.ne)));
+		H3DG_CUDA_TRY(disc->ev_out.alloc(4));
+		disc->ev_ne = E.ne;
+		disc->ev_nlmax = E.nlmax;
+		disc->ev_amax = E.amax;
+		disc->ev_bmax = E.bmax;
+		disc->have_eval = true;
+	}
+	h3dg::KArgsNorm a;
+	a.xyz = disc->xyz.p;
+	a.el_vtx = disc->ev_vtx.p;
+	a.el_desc = disc->ev_desc.p;
+	a.gptr = disc->ev_gptr.p;
+	a.eptr = disc->ev_eptr.p;
+	a.gs = disc->ev_gs.p;
+	a.edof = disc->ev_edof.p;
+	a.ecoef = disc->ev_ecoef.p;
+	a.tables = disc->ev_tables.p;
+	a.sol = d_sol;
+	a.exact = exact;
+	a.partial = disc->ev_partial.p;
+	const size_t smem = sizeof(double) * ((size_t) disc->ev_nlmax + disc->ev_amax + disc->ev_bmax + 4 * kNormThreads);
+	NormFn fn = norm_fn();
+	if (smem > 48 * 1024) H3DG_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+	int nsm = 148;
+	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
+	if (disc->ev_ne > 0) {
+		const int64_t grid = std::min<int64_t>(disc->ev_ne, (int64_t) nsm * 4);
+		fn<<<(unsigned) grid, kNormThreads, smem, st>>>(a, disc->ev_ne, disc->ev_nlmax, disc->ev_amax, disc->ev_bmax);
+		norm_reduce_fn()<<<1, kNormThreads, 0, st>>>(disc->ev_partial.p, disc->ev_ne, disc->ev_out.p);
+		H3DG_CUDA_TRY(cudaGetLastError());
+	}
+	double v[4] = { 0.0, 0.0, 0.0, 0.0 };
+	if (disc->ev_ne > 0) {
+		H3DG_CUDA_TRY(cudaMemcpyAsync(v, disc->ev_out.p, sizeof(v), cudaMemcpyDeviceToHost, st));
+		H3DG_CUDA_TRY(cudaStreamSynchronize(st));
+	}
+	// calc_error / calc_norm: the square root only above 1e-14 (src/norm.cc:58,79)
+	for (int j = 0; j < 4; j++) out[j] = v[j] > 10e-15 ? std::sqrt(v[j]) : v[j];
 	return H3DG_OK;
 }
 

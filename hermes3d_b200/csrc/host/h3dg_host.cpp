@@ -1612,6 +1612,87 @@ int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string 
 	return 0;
 }
 
+// ---------------------------------------------------------------- evaluation plan
+
+int build_eval_plan(const Space &sp, bool p_plus, int qn, EvalPlan &E, std::string &err) {
+	if (!sp.assigned) { err = "assign_dofs() has not been called"; return -1; }
+	const Mesh &m = *sp.mesh;
+	E = EvalPlan();
+	E.gptr.assign(1, 0);
+	E.eptr.assign(1, 0);
+	std::vector<std::pair<int, int>> set_key;
+	std::vector<int> set_off;
+	auto table_set = [&](int p, int nq) -> int {
+		for (size_t t = 0; t < set_key.size(); t++)
+			if (set_key[t].first == p && set_key[t].second == nq) return set_off[t];
+		int off = (int) E.tables.size();
+		std::vector<double> q, w;
+		gauss_legendre(nq, q, w);
+		for (int k = 0; k <= p; k++)
+			for (int i = 0; i < nq; i++) E.tables.push_back(lobatto_value(k, q[i]));
+		for (int k = 0; k <= p; k++)
+			for (int i = 0; i < nq; i++) E.tables.push_back(lobatto_deriv(k, q[i]));
+		E.tables.insert(E.tables.end(), q.begin(), q.end());
+		E.tables.insert(E.tables.end(), w.begin(), w.end());
+		set_key.push_back({ p, nq });
+		set_off.push_back(off);
+		return off;
+	};
+	std::vector<AsmEntry> al;
+	for (int64_t e = 0; e < m.ne(); e++) {
+		if (!m.active(e)) continue;
+		sp.element_assembly_list(e, al);
+		int pe[3];
+		for (int r = 0; r < 3; r++) pe[r] = sp.order[3 * e + r];
+		struct Ent { int s; int dof; double c; size_t ord; };
+		std::vector<Ent> ents;
+		std::vector<Canon> cs;
+		for (const AsmEntry &x : al) {
+			const Canon c = decode_index(x.idx);
+			pe[0] = std::max(pe[0], c.a);
+			pe[1] = std::max(pe[1], c.b);
+			pe[2] = std::max(pe[2], c.c);
+			cs.push_back(c);
+		}
+		int32_t d[12] = { 0 };
+		int nl = 1;
+		for (int r = 0; r < 3; r++) {
+			const int p = sp.order[3 * e + r];
+			const int nq = p_plus ? p + qn : qn;
+			if (nq < 1 || nq > kMaxQuadPoints || pe[r] > kMaxOrder) { err = "evaluation: order or rule out of range"; return -1; }
+			d[r] = pe[r];
+			d[3 + r] = nq;
+			d[6 + r] = table_set(pe[r], nq);
+			nl *= pe[r] + 1;
+		}
+		d[9] = nl;
+		for (size_t i = 0; i < al.size(); i++) {
+			const Canon &c = cs[i];
+			const int s = (c.a * (pe[1] + 1) + c.b) * (pe[2] + 1) + c.c;
+			ents.push_back(Ent { s, al[i].dof, c.sign * al[i].coef, i });
+		}
+		std::stable_sort(ents.begin(), ents.end(), [](const Ent &x, const Ent &y) { return x.s < y.s; });
+		for (size_t i = 0; i < ents.size(); i++) {
+			if (i == 0 || ents[i].s != ents[i - 1].s) {
+				E.gs.push_back((uint16_t) ents[i].s);
+				if (i > 0) E.eptr.push_back((int64_t) E.edof.size());
+			}
+			E.edof.push_back(ents[i].dof);
+			E.ecoef.push_back(ents[i].c);
+		}
+		if (!ents.empty()) E.eptr.push_back((int64_t) E.edof.size());
+		E.gptr.push_back((int64_t) E.gs.size());
+		E.desc.insert(E.desc.end(), d, d + 12);
+		for (int v = 0; v < 8; v++) E.vtx.push_back((int32_t) m.hex[8 * e + v]);
+		E.nlmax = std::max(E.nlmax, nl);
+		E.amax = std::max(E.amax, 2 * (pe[0] + 1) * (pe[1] + 1) * d[5]);
+		E.bmax = std::max(E.bmax, 3 * (pe[0] + 1) * d[4] * d[5]);
+		E.ne++;
+	}
+	if (E.tables.empty()) E.tables.push_back(0.0);
+	return 0;
+}
+
 // ---------------------------------------------------------------- surface forms
 
 // Discretization::assemble's surface loop (src/discretization.cc:345-412):

@@ -247,6 +247,23 @@ struct Plan {
 	std::vector<double> sf_tables;           // per (order, points) set: q[nq], w[nq], V[(p+1) nq]
 };
 
+// Evaluation plan of a finite-element function on the active elements (norms,
+// src/norm.cc:33-180): per element its orders and rule (p_d + qn or qn points,
+// orders raised where constraints need it), and its expanded assembly list
+// grouped by canonical function (groups ascending, entries in list order).
+struct EvalPlan {
+	int64_t ne = 0;
+	int nlmax = 0, amax = 0, bmax = 0;       // largest C, A and B work arrays (doubles)
+	std::vector<int32_t> desc;               // ne x 12 (as Plan::el_desc)
+	std::vector<int32_t> vtx;                // ne x 8
+	std::vector<int64_t> gptr, eptr;         // ne + 1, groups + 1
+	std::vector<uint16_t> gs;
+	std::vector<int32_t> edof;
+	std::vector<double> ecoef;
+	std::vector<double> tables;              // per set: V, D, q, w (as Plan::mixed_tables)
+};
+int build_eval_plan(const Space &sp, bool p_plus, int qn, EvalPlan &E, std::string &err);
+
 // surface-form plan of the outer faces whose marker is natural (needs the
 // volume plan's pattern); nq per direction p_d + qn (p_plus) or qn
 int build_surface_plan(const Space &sp, bool p_plus, int qn, Plan &P, std::string &err);

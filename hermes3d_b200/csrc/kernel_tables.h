@@ -16,6 +16,7 @@
 #include "kernels/asm_fp64_mixed.cuh"
 #include "kernels/asm_fp64_ced.cuh"
 #include "kernels/asm_surface.cuh"
+#include "kernels/norms.cuh"
 
 namespace h3dg_tables {
 
@@ -102,5 +103,12 @@ constexpr int kCedScatterThreads = 256;
 using SurfFn = void (*)(h3dg::KArgsSurf, int64_t, int64_t);
 SurfFn surf_fn();
 constexpr int kSurfThreads = 128;
+
+// norms of a finite-element function (per element, then a fixed-order reduction)
+using NormFn = void (*)(h3dg::KArgsNorm, int64_t, int, int, int);
+using NormReduceFn = void (*)(const double *, int64_t, double *);
+NormFn norm_fn();
+NormReduceFn norm_reduce_fn();
+constexpr int kNormThreads = 128;
 
 } // namespace h3dg_tables

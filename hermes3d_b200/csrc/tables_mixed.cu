@@ -34,4 +34,7 @@ CedScatterFn ced_scatter_fn() { return &h3dg::k_scatter_ced<kCedScatterThreads>;
 
 SurfFn surf_fn() { return &h3dg::k_assemble_surface<kSurfThreads>; }
 
+NormFn norm_fn() { return &h3dg::k_norms<kNormThreads>; }
+NormReduceFn norm_reduce_fn() { return &h3dg::k_norms_reduce<kNormThreads>; }
+
 } // namespace h3dg_tables

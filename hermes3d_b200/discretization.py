@@ -235,6 +235,23 @@ class Discretization:
         capi.call("h3dg_disc_set_surface_forms", self.handle, capi.SBF_U_V if sbf is not None else 0,
                   capi.SLF_G_V if slf is not None else 0, capi.ptr(g, C.c_double) if len(g) else None, len(g))
 
+    def norms(self, sol, exact=None, stream=None):
+        """L2 / H1 error against an exact solution (None, "quadratic" = x^2+y^2+z^2,
+        "sin") and L2 / H1 norm of the finite-element function with coefficients
+        ``sol`` (calc_error / calc_norm, src/norm.cc:33-180), on the device."""
+        import torch
+        kinds = {None: 0, "quadratic": 1, "sin": 2}
+        if exact not in kinds:
+            raise capi.H3dgError(1, "exact solution must be None, 'quadratic' or 'sin'")
+        t = sol if isinstance(sol, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(sol, dtype=np.float64))
+        t = t.to(device="cuda:%d" % self.device, dtype=torch.float64).contiguous()
+        if stream is None:
+            stream = torch.cuda.current_stream(t.device)
+        out = np.zeros(4, np.float64)
+        capi.call("h3dg_disc_norms", self.handle, C.c_void_p(t.data_ptr()), kinds[exact], capi.ptr(out, C.c_double),
+                  C.c_void_p(stream.cuda_stream))
+        return {"l2_error": out[0], "h1_error": out[1], "l2_norm": out[2], "h1_norm": out[3]}
+
     def set_quadrature(self, points=None, p_plus=None):
         """Fixed Gauss points per direction, or p_d + p_plus per direction."""
         if points is not None:

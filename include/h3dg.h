@@ -47,6 +47,11 @@ typedef int h3dg_status;
 #define H3DG_BF_GRAD_GRAD       1   /* int_grad_u_grad_v, optionally times a per-element coefficient */
 #define H3DG_BF_GRAD_GRAD_MASS  2   /* int_grad_u_grad_v + int_u_v */
 
+/* exact solutions for h3dg_disc_norms */
+#define H3DG_EXACT_ZERO      0   /* u = 0: the errors are the norms */
+#define H3DG_EXACT_QUADRATIC 1   /* u = x^2 + y^2 + z^2 */
+#define H3DG_EXACT_SIN       2   /* u = sin(pi x) sin(pi y) sin(pi z) */
+
 /* surface forms (src/integrals/h1.h:184-242) */
 #define H3DG_SBF_NONE 0
 #define H3DG_SBF_U_V  1   /* surf_int_u_v */
@@ -143,6 +148,14 @@ h3dg_status h3dg_disc_set_space(h3dg_disc *disc, h3dg_space *space);
 h3dg_status h3dg_disc_set_bilinear_form(h3dg_disc *disc, int form, const double *elem_coef, int64_t ne);
 /* set_linear_form(0, lf) (src/discretization.cc:151-161); value is the constant for H3DG_LF_CONST */
 h3dg_status h3dg_disc_set_linear_form(h3dg_disc *disc, int form, double value);
+/* Norms of the finite-element function with coefficient vector d_sol (device,
+ * ndof doubles; Dirichlet parts from the space's lifting), as calc_error /
+ * calc_norm with the H1 and L2 functions (src/norm.cc:33-180): out[0] = L2 error,
+ * out[1] = H1 error against the exact solution `exact` (H3DG_EXACT_*), out[2] = L2
+ * norm, out[3] = H1 norm of the function itself; each integral with the rule of
+ * the assembly (set_quadrature), the square root taken above 1e-14 as in the
+ * reference.  Synchronises `stream`. */
+h3dg_status h3dg_disc_norms(h3dg_disc *disc, const double *d_sol, int exact, double *out, void *stream);
 /* surface forms on the outer faces whose marker is natural (set_bilinear_form's
  * and set_linear_form's surf arguments, src/discretization.cc:136-161, assembled as
  * src/discretization.cc:345-412): bilinear H3DG_SBF_U_V = surf_int_u_v, linear
