@@ -54,6 +54,7 @@ SIGNATURES = {
     "h3dg_mesh_refine_element": [_p, _i64, C.c_int],
     "h3dg_disc_set_surface_forms": [_p, C.c_int, C.c_int, _pd, C.c_int],
     "h3dg_disc_norms": [_p, _p, C.c_int, _pd, _p],
+    "h3dg_disc_solve_cg": [_p, _p, _p, _p, C.c_double, C.c_int, _pi32, _pd, _p],
     "h3dg_mesh_refine_elements": [_p, _pi64, _i64, C.c_int],
     "h3dg_mesh_get_arrays": [_p, _pd, _pi64, _pi64],
     "h3dg_space_create": [_p, C.POINTER(_p)],

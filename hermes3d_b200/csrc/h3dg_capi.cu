@@ -5,6 +5,7 @@
 #include "kernel_tables.h"
 #include "kernels/tc_selftest.cuh"
 #include "kernels/geom.cuh"
+#include "kernels/cg.cuh"
 
 #include <cuda_runtime.h>
 
@@ -75,6 +76,7 @@ struct h3dg_disc {
 	int lf = H3DG_LF_NONE;
 	double lf_value = 0.0;
 	int qmode = H3DG_QUAD_FIXED, qn = 0;
+	DBuf<double> cg_work;            // conjugate-gradient vectors and partial sums
 	// evaluation plan (norms), built at the first norms call after create_pattern
 	bool have_eval = false;
 	int64_t ev_ne = 0;
@@ -1006,6 +1008,57 @@ static h3dg_status assemble_surface(h3dg_disc *disc, double *d_Ax, double *d_rhs
 	}
 	H3DG_CUDA_TRY(cudaGetLastError());
 	disc->last_launches += n;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_solve_cg(h3dg_disc *disc, const double *d_Ax, const double *d_rhs, double *d_x, double rtol,
+                               int maxit, int *iters, double *relres, void *stream) {
+	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "solve_cg: create_pattern() first");
+	if (!d_Ax || !d_rhs || !d_x || !(rtol > 0.0) || maxit < 1) return fail(H3DG_ERR_INVALID_ARG, "solve_cg: bad arguments");
+	if (disc->nparts > 1) return fail(H3DG_ERR_STATE, "solve_cg: the matrix of one part is not the whole operator");
+	{ h3dg_status s0 = ensure_device(disc); if (s0 != H3DG_OK) return s0; }
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	cudaStream_t st = (cudaStream_t) stream;
+	const int64_t n = disc->plan.ndof;
+	const size_t need = 5 * (size_t) n + h3dg::kCgBlocks + 8;
+	if (disc->cg_work.n < need) H3DG_CUDA_TRY(disc->cg_work.alloc(need));
+	double *r = disc->cg_work.p, *z = r + n, *p = z + n, *q = p + n, *dinv = q + n;
+	double *partial = dinv + n, *scal = partial + h3dg::kCgBlocks;
+	const int64_t *Ap = disc->Ap.p;
+	const int32_t *Ai = disc->Ai.p;
+	const unsigned g = 148 * 8;
+	auto dot = [&](const double *a, const double *b, double &out) -> h3dg_status {
+		h3dg::k_cg_dot_partial<<<h3dg::kCgBlocks, h3dg::kCgThreads, 0, st>>>(a, b, n, partial);
+		h3dg::k_cg_dot_final<<<1, h3dg::kCgThreads, 0, st>>>(partial, h3dg::kCgBlocks, scal);
+		H3DG_CUDA_TRY(cudaMemcpyAsync(&out, scal, sizeof(double), cudaMemcpyDeviceToHost, st));
+		H3DG_CUDA_TRY(cudaStreamSynchronize(st));
+		return H3DG_OK;
+	};
+	h3dg::k_cg_invdiag<<<g, h3dg::kCgThreads, 0, st>>>(Ap, Ai, d_Ax, dinv, n);
+	h3dg::k_cg_spmv<<<g, h3dg::kCgThreads, 0, st>>>(Ap, Ai, d_Ax, d_x, q, n);
+	h3dg::k_cg_init<<<g, h3dg::kCgThreads, 0, st>>>(d_rhs, q, dinv, r, z, p, n);
+	H3DG_CUDA_TRY(cudaGetLastError());
+	double bb = 0.0, rz = 0.0, rr = 0.0;
+	if (dot(d_rhs, d_rhs, bb) != H3DG_OK || dot(r, z, rz) != H3DG_OK || dot(r, r, rr) != H3DG_OK) return H3DG_ERR_CUDA;
+	const double bnorm = std::sqrt(bb);
+	int it = 0;
+	while (it < maxit && std::sqrt(rr) > rtol * bnorm) {
+		h3dg::k_cg_spmv<<<g, h3dg::kCgThreads, 0, st>>>(Ap, Ai, d_Ax, p, q, n);
+		double pq = 0.0;
+		if (dot(p, q, pq) != H3DG_OK) return H3DG_ERR_CUDA;
+		if (!(pq > 0.0)) break;                           // not positive definite on this direction
+		const double alpha = rz / pq;
+		h3dg::k_cg_update_xr<<<g, h3dg::kCgThreads, 0, st>>>(d_x, r, z, p, q, dinv, alpha, n);
+		double rz1 = 0.0;
+		if (dot(r, z, rz1) != H3DG_OK || dot(r, r, rr) != H3DG_OK) return H3DG_ERR_CUDA;
+		h3dg::k_cg_update_p<<<g, h3dg::kCgThreads, 0, st>>>(p, z, rz1 / rz, n);
+		rz = rz1;
+		it++;
+	}
+	H3DG_CUDA_TRY(cudaGetLastError());
+	H3DG_CUDA_TRY(cudaStreamSynchronize(st));
+	if (iters) *iters = it;
+	if (relres) *relres = bnorm > 0.0 ? std::sqrt(rr) / bnorm : 0.0;
 	return H3DG_OK;
 }
 

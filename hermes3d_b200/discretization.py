@@ -235,6 +235,21 @@ class Discretization:
         capi.call("h3dg_disc_set_surface_forms", self.handle, capi.SBF_U_V if sbf is not None else 0,
                   capi.SLF_G_V if slf is not None else 0, capi.ptr(g, C.c_double) if len(g) else None, len(g))
 
+    def solve(self, Ax, rhs, x=None, rtol=1e-12, maxit=10000, stream=None):
+        """Jacobi-preconditioned CG on the device for the assembled system (torch CUDA
+        float64 tensors Ax, rhs in the plan's layout); returns (x, iterations, relres)."""
+        import torch
+        if x is None:
+            x = torch.zeros_like(rhs)
+        if stream is None:
+            stream = torch.cuda.current_stream(rhs.device)
+        it = C.c_int32()
+        rr = C.c_double()
+        capi.call("h3dg_disc_solve_cg", self.handle, C.c_void_p(Ax.data_ptr()), C.c_void_p(rhs.data_ptr()),
+                  C.c_void_p(x.data_ptr()), float(rtol), int(maxit), C.byref(it), C.byref(rr),
+                  C.c_void_p(stream.cuda_stream))
+        return x, it.value, rr.value
+
     def norms(self, sol, exact=None, stream=None):
         """L2 / H1 error against an exact solution (None, "quadratic" = x^2+y^2+z^2,
         "sin") and L2 / H1 norm of the finite-element function with coefficients

@@ -148,6 +148,13 @@ h3dg_status h3dg_disc_set_space(h3dg_disc *disc, h3dg_space *space);
 h3dg_status h3dg_disc_set_bilinear_form(h3dg_disc *disc, int form, const double *elem_coef, int64_t ne);
 /* set_linear_form(0, lf) (src/discretization.cc:151-161); value is the constant for H3DG_LF_CONST */
 h3dg_status h3dg_disc_set_linear_form(h3dg_disc *disc, int form, double value);
+/* No reference counterpart (the reference solves with UMFPACK,
+ * src/linsolver/umfpack.cc:280-330): Jacobi-preconditioned conjugate gradients on the
+ * assembled matrix (d_Ax in the plan's CSC pattern; the forms are symmetric) for the
+ * RHS d_rhs, starting from d_x and overwriting it, until ||r|| <= rtol ||b|| or maxit
+ * iterations; bitwise reproducible.  Synchronises `stream` every iteration. */
+h3dg_status h3dg_disc_solve_cg(h3dg_disc *disc, const double *d_Ax, const double *d_rhs, double *d_x, double rtol,
+                               int maxit, int *iters, double *relres, void *stream);
 /* Norms of the finite-element function with coefficient vector d_sol (device,
  * ndof doubles; Dirichlet parts from the space's lifting), as calc_error /
  * calc_norm with the H1 and L2 functions (src/norm.cc:33-180): out[0] = L2 error,
