@@ -975,6 +975,7 @@ static void parallel_for(int64_t n, F f) {
 int make_partition_scope(const Space &sp, int nparts, int part, PlanScope &S, std::string &err) {
 	if (!sp.assigned) { err = "assign_dofs() has not been called"; return -1; }
 	if (nparts < 1 || part < 0 || part >= nparts) { err = "partition: need 0 <= part < nparts"; return -1; }
+	if (sp.mesh->nrefined) { err = "partition: refined meshes are not supported"; return -1; }
 	const Mesh &m = *sp.mesh;
 	const int64_t ne = m.ne(), nd = sp.ndof();
 	std::vector<std::array<double, 3>> cen(ne);

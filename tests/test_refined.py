@@ -82,3 +82,18 @@ def test_refine_element_errors():
         m.refine_element(9)          # a child: one refinement level
     with pytest.raises(h.H3dgError):
         m.refine_element(2, 1)       # REFT_HEX_X is not supported
+
+
+def test_partition_of_refined_mesh_is_rejected():
+    m = h.unit_cube(3)
+    m.refine_element(14)
+    sp = h.H1Space(m)
+    sp.set_uniform_order(2)
+    sp.assign_dofs()
+    d = h.Discretization()
+    d.set_spaces(sp)
+    d.set_bilinear_form(h.int_grad_u_grad_v)
+    d.set_linear_form(h.int_F_v(1.0))
+    d.set_partition(2, 0)
+    with pytest.raises(h.H3dgError):
+        d.create(h.UMFPackMatrix(), h.UMFPackVector())
