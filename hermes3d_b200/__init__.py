@@ -7,7 +7,8 @@ the C ABI.
 from . import _capi
 from .discretization import (BC_ESSENTIAL, BC_NATURAL, BC_NONE, Discretization, H1Space, UMFPackMatrix,
                              UMFPackVector, UnsupportedForm, int_F_v, int_grad_u_grad_v,
-                             int_grad_u_grad_v_plus_u_v, surf_int_G_v, surf_int_u_v)
+                             int_grad_u_grad_v_plus_u_v, int_u_v, surf_int_G_v, surf_int_u_v,
+                             SystemDiscretization)
 from .mesh import Mesh, load_mesh3d, permute_vertices, unit_cube
 
 H3dgError = _capi.H3dgError
@@ -18,6 +19,6 @@ PREC_OZAKI = _capi.PREC_OZAKI
 __all__ = [
     "Mesh", "load_mesh3d", "unit_cube", "permute_vertices", "H1Space", "Discretization", "UMFPackMatrix",
     "UMFPackVector", "int_grad_u_grad_v", "int_grad_u_grad_v_plus_u_v", "int_F_v", "UnsupportedForm",
-    "surf_int_u_v", "surf_int_G_v",
+    "surf_int_u_v", "surf_int_G_v", "int_u_v", "SystemDiscretization",
     "BC_ESSENTIAL", "BC_NATURAL", "BC_NONE", "PREC_FP64", "PREC_TF32X3", "PREC_OZAKI", "H3dgError",
 ]

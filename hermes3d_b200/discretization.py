@@ -72,6 +72,7 @@ class H1Space:
         n = C.c_int64()
         capi.call("h3dg_space_assign_dofs", self.handle, int(first_dof), int(stride), C.byref(n))
         self.ndof = n.value
+        self.first_dof = int(first_dof)
         return n.value
 
     def get_dof_count(self):
@@ -112,6 +113,8 @@ class LinearForm:
 
 int_grad_u_grad_v = BilinearForm(capi.BF_GRAD_GRAD, "int_grad_u_grad_v")
 int_grad_u_grad_v_plus_u_v = BilinearForm(capi.BF_GRAD_GRAD_MASS, "int_grad_u_grad_v + int_u_v")
+# int_u_v alone (src/integrals/h1.h:154-177): the grad.grad + mass kernels with a zero grad.grad coefficient
+int_u_v = BilinearForm(-1, "int_u_v")
 
 
 @dataclass(frozen=True)
@@ -210,7 +213,12 @@ class Discretization:
         if surf is not None and not isinstance(surf, SurfaceBilinearForm):
             raise UnsupportedForm(4, "surface form %r is not one of the device forms" % (surf,))
         c = None if coef is None else np.ascontiguousarray(coef, dtype=np.float64)
-        capi.call("h3dg_disc_set_bilinear_form", self.handle, form.kind,
+        kind = form.kind
+        if form is int_u_v:
+            if self.space is None:
+                raise capi.H3dgError(6, "set_spaces() before set_bilinear_form(int_u_v)")
+            kind, c = capi.BF_GRAD_GRAD_MASS, np.zeros(self.space.mesh.num_elements, np.float64)
+        capi.call("h3dg_disc_set_bilinear_form", self.handle, kind,
                   capi.ptr(c, C.c_double), 0 if c is None else len(c))
         self._coef = c
         self._sbf = surf
@@ -425,3 +433,153 @@ class Discretization:
         if getattr(self, "handle", None) and capi._lib is not None:
             capi.lib().h3dg_disc_destroy(self.handle)
             self.handle = None
+
+
+class SystemDiscretization:
+    """Discretization with several equations (src/discretization.h:39-101 with
+    neq > 1; assembly src/discretization.cc:232-343) for equations whose spaces
+    are identical (same mesh, orders and boundary conditions) and numbered one
+    after another (space i assigned with first_dof = i * ndof).  Block (m, n)
+    holds the form of test space m and trial space n.  Each block is assembled
+    by the device kernels on the common single-space pattern and placed into
+    the system arrays on the device; the Dirichlet lifting of the trial space
+    goes to the rows of the test space.  As in the reference, equation m's RHS
+    is written only when it has a linear form."""
+
+    def __init__(self, device=0):
+        self.device = device
+        self.neq = 1
+        self.spaces = []
+        self.forms = {}
+        self.lforms = {}
+        self._quad = ("p_plus", 2)
+        self.ndof = None
+        self.nnz = None
+
+    def set_num_equations(self, neq):
+        if not 1 <= int(neq) <= 8:
+            raise capi.H3dgError(1, "1..8 equations")
+        self.neq = int(neq)
+
+    def set_spaces(self, *spaces):
+        if len(spaces) != self.neq:
+            raise capi.H3dgError(1, "one space per equation")
+        nd = spaces[0].ndof
+        for i, sp in enumerate(spaces):
+            if sp.ndof != nd or sp.mesh is not spaces[0].mesh or getattr(sp, "first_dof", None) != i * nd:
+                raise capi.H3dgError(1, "the spaces must be identical and numbered one after another")
+        self.spaces = list(spaces)
+
+    def set_bilinear_form(self, i, j, form, coef=None):
+        if not isinstance(form, BilinearForm):
+            raise UnsupportedForm(4, "bilinear form %r is not one of the device forms" % (form,))
+        self.forms[(int(i), int(j))] = (form, coef)
+
+    def set_linear_form(self, i, form):
+        if form is not None and not isinstance(form, LinearForm):
+            raise UnsupportedForm(4, "linear form %r is not one of the device forms" % (form,))
+        self.lforms[int(i)] = form
+
+    def set_quadrature(self, points=None, p_plus=None):
+        self._quad = ("points", int(points)) if points is not None else ("p_plus", int(p_plus))
+
+    def _base(self, form, coef, lf):
+        d = Discretization(self.device)
+        d.set_spaces(self.spaces[0])
+        d.set_bilinear_form(form, coef)
+        d.set_linear_form(lf)
+        if self._quad[0] == "points":
+            d.set_quadrature(points=self._quad[1])
+        else:
+            d.set_quadrature(p_plus=self._quad[1])
+        m = UMFPackMatrix()
+        d.create(m, UMFPackVector())
+        return d, m
+
+    def create(self, matrix=None, rhs=None):
+        """Discretization::create: the pattern of every block with a form."""
+        nd = self.spaces[0].ndof
+        self.nd1 = nd
+        # one single-space discretisation per block; the first block of row m
+        # carries F_m, the others contribute their lifting only (F = 0)
+        self._blocks = []
+        pattern = None
+        for m in range(self.neq):
+            row = [n for n in range(self.neq) if (m, n) in self.forms]
+            lf = self.lforms.get(m)
+            for k, n in enumerate(row):
+                form, coef = self.forms[(m, n)]
+                blf = (lf if k == 0 else int_F_v(0.0)) if lf is not None else None
+                d, bm = self._base(form, coef, blf)
+                self._blocks.append((m, n, d))
+                pattern = pattern or bm
+            if lf is not None and not row:
+                d, bm = self._base(int_grad_u_grad_v, None, lf)
+                self._blocks.append((m, -1, d))
+                pattern = pattern or bm
+        if pattern is None:
+            pattern = self._base(int_grad_u_grad_v, None, None)[1]
+        Ap0, Ai0 = pattern.Ap, pattern.Ai
+        counts = np.diff(Ap0)
+        # system column n * nd + j: the rows of the blocks (m, n), m ascending
+        pres = [[(m, n) in self.forms for n in range(self.neq)] for m in range(self.neq)]
+        colcnt = np.zeros(self.neq * nd, np.int64)
+        for n in range(self.neq):
+            colcnt[n * nd:(n + 1) * nd] = counts * sum(pres[m][n] for m in range(self.neq))
+        Ap = np.zeros(self.neq * nd + 1, np.int64)
+        np.cumsum(colcnt, out=Ap[1:])
+        Ai = np.zeros(Ap[-1], np.int32)
+        self._pos = {}
+        for n in range(self.neq):
+            off = np.zeros(nd, np.int64)
+            for m in range(self.neq):
+                if not pres[m][n]:
+                    continue
+                start = Ap[n * nd:(n + 1) * nd] + off
+                idx = np.repeat(start - Ap0[:-1], counts) + np.arange(Ap0[-1])
+                Ai[idx] = Ai0 + m * nd
+                self._pos[(m, n)] = idx
+                off += counts
+        self.ndof, self.nnz = self.neq * nd, int(Ap[-1])
+        self.Ap, self.Ai = Ap, Ai
+        if matrix is not None:
+            matrix.Ap, matrix.Ai = Ap.copy(), Ai.copy()
+            matrix.Ax = np.zeros(self.nnz, np.float64)
+            matrix.ndofs = self.ndof
+        if rhs is not None:
+            rhs.v = np.zeros(self.ndof, np.float64)
+
+    def assemble_device(self, Ax, rhs=None):
+        """Assemble into torch CUDA float64 tensors (system layout), block by block."""
+        import torch
+        nd = self.nd1
+        dev = Ax.device if Ax is not None else rhs.device
+        if Ax is not None:
+            Ax.zero_()
+        if rhs is not None:
+            rhs.zero_()
+        for m, n, d in self._blocks:
+            ax_b = torch.empty(d.nnz, dtype=torch.float64, device=dev) if (Ax is not None and n >= 0) else None
+            rhs_b = (torch.empty(nd, dtype=torch.float64, device=dev)
+                     if (rhs is not None and self.lforms.get(m) is not None) else None)
+            if ax_b is None and rhs_b is None:
+                continue
+            d.assemble_device(ax_b, rhs_b)
+            if ax_b is not None:
+                key = ("t", m, n)
+                if key not in self._pos:
+                    self._pos[key] = torch.as_tensor(self._pos[(m, n)], device=dev)
+                Ax.index_add_(0, self._pos[key], ax_b)     # each system entry belongs to one block
+            if rhs_b is not None:
+                rhs[m * nd:(m + 1) * nd] += rhs_b
+
+    def assemble(self, matrix=None, rhs=None):
+        import torch
+        dev = torch.device("cuda", self.device)
+        Ax = torch.empty(self.nnz, dtype=torch.float64, device=dev) if matrix is not None else None
+        r = torch.empty(self.ndof, dtype=torch.float64, device=dev) if rhs is not None else None
+        self.assemble_device(Ax, r)
+        if matrix is not None:
+            matrix.Ax = Ax.cpu().numpy()
+        if rhs is not None:
+            rhs.v = r.cpu().numpy()

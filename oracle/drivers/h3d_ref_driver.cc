@@ -26,6 +26,7 @@
 //       [--source none|one|sin|poly] [--bc dirichlet0|dirichlet_poly|natural]
 //       [--refine REF.bin] [--repeat R] [--no-asm] [--elem-dump]
 //       [--surf-uv] [--surf-g g1,...,g6] [--natural-markers m1,m2,...]
+//       [--sys k11,k12,k21,k22 (none|gg|ggm|mass) --source2 S]
 //
 // Output (little-endian binary, all counts int64):
 //   "H3DOUT01" ndof nnz Ap[ndof+1](i32) Ai[nnz](i32) Ax[nnz](f64) rhs[ndof](f64)
@@ -106,6 +107,41 @@ static scalar bf_fixed(RealFunction *fu, RealFunction *fv, RefMap *ru, RefMap *r
 	return result;
 }
 
+// block forms of a two-equation system: grad.grad (x coefficient), + mass, mass alone
+static scalar bf_block(RealFunction *fu, RealFunction *fv, RefMap *ru, RefMap *rv, bool gg, bool mass) {
+	order3_t o = elem_qorder(ru);
+	Quad3D *quad = fu->get_quad();
+	qorder_t qord = ELEM_QORDER(o);
+	fu->set_quad_order(qord);
+	fv->set_quad_order(qord);
+	double *dudx, *dudy, *dudz, *dvdx, *dvdy, *dvdz;
+	fu->get_dx_dy_dz_values(dudx, dudy, dudz);
+	fv->get_dx_dy_dz_values(dvdx, dvdy, dvdz);
+	double *uval = fu->get_fn_values();
+	double *vval = fv->get_fn_values();
+	QuadPt3D *pt = quad->get_points(o);
+	int np = quad->get_num_points(o);
+	double3x3 *mu = ru->get_inv_ref_map(o);
+	double3x3 *mv = rv->get_inv_ref_map(o);
+	double *jac = ru->get_jacobian(o);
+	double result = 0.0;
+	if (gg) {
+		for (int i = 0; i < np; i++, mu++, mv++)
+			result += pt[i].w * jac[i] * (T_DUDX * T_DVDX + T_DUDY * T_DVDY + T_DUDZ * T_DVDZ);
+		result *= elem_coef(ru);
+	}
+	if (mass) {
+		double m = 0.0;
+		for (int i = 0; i < np; i++)
+			m += pt[i].w * jac[i] * (uval[i] * vval[i]);
+		result += m;
+	}
+	return result;
+}
+static scalar bf_gg(RealFunction *fu, RealFunction *fv, RefMap *ru, RefMap *rv) { return bf_block(fu, fv, ru, rv, true, false); }
+static scalar bf_ggm(RealFunction *fu, RealFunction *fv, RefMap *ru, RefMap *rv) { return bf_block(fu, fv, ru, rv, true, true); }
+static scalar bf_m(RealFunction *fu, RealFunction *fv, RefMap *ru, RefMap *rv) { return bf_block(fu, fv, ru, rv, false, true); }
+
 static double source_fn(double x, double y, double z) {
 	switch (g_source) {
 		case 1: return 1.0;
@@ -113,6 +149,34 @@ static double source_fn(double x, double y, double z) {
 		case 3: return -6.0;
 		default: return 0.0;
 	}
+}
+
+static int g_source2 = 0;   // source of the second equation of a system
+static double source_fn2(double x, double y, double z) {
+	switch (g_source2) {
+		case 1: return 1.0;
+		case 2: return sin(M_PI * x) * sin(M_PI * y) * sin(M_PI * z);
+		case 3: return -6.0;
+		default: return 0.0;
+	}
+}
+
+static scalar lf2_fixed(RealFunction *fv, RefMap *rv) {
+	order3_t o = elem_qorder(rv);
+	Quad3D *quad = fv->get_quad();
+	qorder_t qord = ELEM_QORDER(o);
+	fv->set_quad_order(qord);
+	double *vval = fv->get_fn_values();
+	QuadPt3D *pt = quad->get_points(o);
+	int np = quad->get_num_points(o);
+	double *jac = rv->get_jacobian(o);
+	double *x = rv->get_phys_x(o);
+	double *y = rv->get_phys_y(o);
+	double *z = rv->get_phys_z(o);
+	double result = 0.0;
+	for (int i = 0; i < np; i++)
+		result += pt[i].w * jac[i] * (vval[i] * source_fn2(x[i], y[i], z[i]));
+	return result;
 }
 
 static scalar lf_fixed(RealFunction *fv, RefMap *rv) {
@@ -230,6 +294,7 @@ int main(int argc, char **argv) {
 	const char *mesh_fn = NULL, *out_fn = NULL, *orders_fn = NULL, *coef_fn = NULL, *refine_fn = NULL;
 	int p = 2, repeat = 1;
 	bool qref = false, do_asm = true, elem_dump = false, surf_uv = false, surf_g = false;
+	std::string sys_kinds;   // two-equation system: block kinds (none/gg/ggm/mass) row-major
 	for (int i = 1; i < argc; i++) {
 		std::string a = argv[i];
 		const char *v = i + 1 < argc ? argv[i + 1] : "";
@@ -254,6 +319,12 @@ int main(int argc, char **argv) {
 			std::string s = v; i++;
 			g_source = s == "none" ? 0 : s == "one" ? 1 : s == "sin" ? 2 : s == "poly" ? 3 : -1;
 			if (g_source < 0) { fprintf(stderr, "bad --source\n"); return 2; }
+		}
+		else if (a == "--sys") { sys_kinds = v; i++; }
+		else if (a == "--source2") {
+			std::string t = v; i++;
+			g_source2 = t == "none" ? 0 : t == "one" ? 1 : t == "sin" ? 2 : t == "poly" ? 3 : -1;
+			if (g_source2 < 0) { fprintf(stderr, "bad --source2\n"); return 2; }
 		}
 		else if (a == "--surf-uv") surf_uv = true;
 		else if (a == "--surf-g") {
@@ -373,16 +444,45 @@ int main(int argc, char **argv) {
 	FOR_ALL_ACTIVE_ELEMENTS(idx, &mesh)
 		space.set_element_order(idx, order3_t(g_orders[3 * (idx - 1)], g_orders[3 * (idx - 1) + 1], g_orders[3 * (idx - 1) + 2]));
 	int ndof = space.assign_dofs();
+	// second, identical space of a two-equation system, numbered after the first
+	H1Space space2(&mesh, &shapeset);
+	if (!sys_kinds.empty()) {
+		space2.set_bc_types(bc_types);
+		space2.set_bc_values(bc_values);
+		FOR_ALL_ACTIVE_ELEMENTS(idx, &mesh)
+			space2.set_element_order(idx, order3_t(g_orders[3 * (idx - 1)], g_orders[3 * (idx - 1) + 1], g_orders[3 * (idx - 1) + 2]));
+		ndof += space2.assign_dofs(ndof);
+	}
 	double t_space = now() - t0;
 
 	// ---- assembly
 	Discretization d;
-	d.set_num_equations(1);
-	d.set_spaces(1, &space);
-	d.set_pss(1, &pss);
-	if (qref) d.set_bilinear_form(0, 0, bf_ref, NULL, surf_uv ? sbf_uv : NULL);
-	else d.set_bilinear_form(0, 0, bf_fixed, NULL, surf_uv ? sbf_uv : NULL);
-	if (g_source != 0 || surf_g) d.set_linear_form(0, g_source == 0 ? NULL : (qref ? lf_ref : lf_fixed), surf_g ? slf_gv : NULL);
+	PrecalcShapeset pss2(&shapeset);
+	if (!sys_kinds.empty()) {
+		d.set_num_equations(2);
+		d.set_spaces(2, &space, &space2);
+		d.set_pss(2, &pss, &pss2);
+		size_t pos = 0;
+		for (int b = 0; b < 4; b++) {
+			size_t c = sys_kinds.find(',', pos);
+			std::string k = sys_kinds.substr(pos, c == std::string::npos ? std::string::npos : c - pos);
+			pos = c == std::string::npos ? sys_kinds.size() : c + 1;
+			if (k == "gg") d.set_bilinear_form(b / 2, b % 2, bf_gg);
+			else if (k == "ggm") d.set_bilinear_form(b / 2, b % 2, bf_ggm);
+			else if (k == "mass") d.set_bilinear_form(b / 2, b % 2, bf_m);
+			else if (k != "none") { fprintf(stderr, "bad --sys\n"); return 2; }
+		}
+		if (g_source != 0) d.set_linear_form(0, lf_fixed);
+		if (g_source2 != 0) d.set_linear_form(1, lf2_fixed);
+	}
+	else {
+		d.set_num_equations(1);
+		d.set_spaces(1, &space);
+		d.set_pss(1, &pss);
+		if (qref) d.set_bilinear_form(0, 0, bf_ref, NULL, surf_uv ? sbf_uv : NULL);
+		else d.set_bilinear_form(0, 0, bf_fixed, NULL, surf_uv ? sbf_uv : NULL);
+		if (g_source != 0 || surf_g) d.set_linear_form(0, g_source == 0 ? NULL : (qref ? lf_ref : lf_fixed), surf_g ? slf_gv : NULL);
+	}
 
 	DumpMatrix mat;
 	DumpVector rhs;

@@ -167,3 +167,47 @@ def surface_problem(g, device=0):
     kind, n = quad_of(g)
     d.set_quadrature(p_plus=n) if kind == "pplus" else d.set_quadrature(points=n)
     return mesh, sp, d
+
+
+SYSTEM = os.path.join(GOLDEN, "system")
+
+
+def system_names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(SYSTEM, "*.npz")))
+
+
+def load_system(name):
+    z = np.load(os.path.join(SYSTEM, name + ".npz"), allow_pickle=False)
+    d = {k: z[k] for k in z.files}
+    d["params"] = ast.literal_eval(str(d["params"]))
+    return d
+
+
+def system_problem(g, device=0):
+    """Two identical spaces and the block forms / sources of a system fixture."""
+    p = g["params"]
+    mesh = mesh_of(g)
+    mesh.ugh()
+    spaces = []
+    nd = 0
+    for i in range(2):
+        sp = h.H1Space(mesh)
+        if p.get("bc") == "natural":
+            sp.set_bc_types(lambda m: h.BC_NATURAL)
+        if p.get("bc") == "dirichlet_poly":
+            sp.set_bc_values(lambda m, x, y, z: x * x + y * y + z * z)
+        sp.set_uniform_order(p["p"])
+        nd += sp.assign_dofs(nd)
+        spaces.append(sp)
+    d = h.SystemDiscretization(device)
+    d.set_num_equations(2)
+    d.set_spaces(*spaces)
+    kinds = {"gg": h.int_grad_u_grad_v, "ggm": h.int_grad_u_grad_v_plus_u_v, "mass": h.int_u_v}
+    for b, k in enumerate(p["sys"]):
+        if k != "none":
+            d.set_bilinear_form(b // 2, b % 2, kinds[k])
+    src = {"one": h.int_F_v(1.0), "sin": h.int_F_v("sin"), "poly": h.int_F_v(-6.0), "none": None}
+    d.set_linear_form(0, src[p.get("source", "one")])
+    d.set_linear_form(1, src[p.get("source2", "none")])
+    d.set_quadrature(p_plus=2)
+    return mesh, spaces, d
