@@ -31,8 +31,6 @@ N_ELEM_SIDE = 64
 P_ORDER = 2
 N_POINTS = 4
 METRIC = "hp assembly elements/s (FP64, C2: 64^3 jittered, p=2, 4^3 pts, grad+mass, sin source, full CSC+RHS)"
-CPU_SAMPLE_SIDE = 16
-FP64_PEAK_TFLOPS = 37.0      # nominal B200 FP64 (vector and tensor), for the combined roofline only
 
 # the other configurations (parity cases; reported with --workload, never the headline)
 WORKLOADS = {
@@ -233,25 +231,69 @@ def cpu_baseline_c3(repeat=1):
                       "Discretization::assemble, median of %d" % (n, len(refs), nact, repeat)}
 
 
+SLAB_MARKER = 7          # the cut faces of a z-slab of the C2 mesh: natural (no Dirichlet row)
+
+
+def c2_slab(mesh, k0, k1, n=N_ELEM_SIDE):
+    """Elements k0 <= k < k1 (z layers) of the structured n^3 C2 mesh as a mesh
+    of their own, vertices renumbered.  The cube's faces keep their markers
+    (essential); the cut faces get SLAB_MARKER and are natural, so every element
+    of the slab does exactly the work it does inside the whole mesh."""
+    import numpy as np
+    from hermes3d_b200.mesh import Mesh
+    layer_v = (n + 1) ** 2
+    v0, v1 = k0 * layer_v, (k1 + 1) * layer_v
+    hexes = mesh.hexes[k0 * n * n:k1 * n * n] - v0
+    keep = np.all((mesh.bquads > v0) & (mesh.bquads <= v1), axis=1)
+    bq, bm = [mesh.bquads[keep] - v0], [mesh.bmarkers[keep]]
+    b, a = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    a, b = a.ravel(), b.ravel()
+
+    def vid(i, j, k):
+        return 1 + i + (n + 1) * (j + (n + 1) * (k - k0))
+    for kc in (k0, k1):
+        if 0 < kc < n:
+            bq.append(np.stack([vid(a, b, kc), vid(a + 1, b, kc), vid(a + 1, b + 1, kc), vid(a, b + 1, kc)], 1))
+            bm.append(np.full(len(a), SLAB_MARKER))
+    return Mesh().set_arrays(mesh.xyz[v0:v1], hexes, np.concatenate(bq), np.concatenate(bm))
+
+
+def _ref_slab_cmd(mesh_file, out_file, repeat):
+    from oracle import ref_driver
+    return [ref_driver.DRIVER, "--mesh", mesh_file, "--out", out_file, "--p", str(P_ORDER), "--qmode",
+            "fixed:%d" % N_POINTS, "--mass", "--source", "sin", "--bc", "dirichlet0", "--natural-markers",
+            str(SLAB_MARKER), "--repeat", str(repeat)]
+
+
 def cpu_baseline(repeat=3):
     """The reference (oracle/_ref, built from the reference's sources) on one
-    host core, on a bounded sample of the same workload."""
+    host core, on a bounded sample of the workload itself: two z layers
+    (8192 elements) from the middle of the seeded 64^3 C2 mesh."""
+    import tempfile
     from hermes3d_b200.mesh import unit_cube
     from oracle import ref_driver
     if not ref_driver.available():
         return None
-    n = CPU_SAMPLE_SIDE
-    r = ref_driver.run(unit_cube(n, 0.2, 0), p=P_ORDER, qmode="fixed:%d" % N_POINTS, mass=True, source="sin",
-                       repeat=repeat)
-    t = r["timing"]["t_assemble_median"]
-    return {"value": n ** 3 / t, "unit": "elements/s", "cores": 1, "kind": "reference",
-            "sample": "%d^3 jittered sub-mesh (%d elements) of the same workload, Discretization::assemble, "
-                      "median of %d" % (n, n ** 3, repeat)}
+    k0 = N_ELEM_SIDE // 2 - 1
+    with tempfile.TemporaryDirectory() as td:
+        mf = os.path.join(td, "m.bin")
+        c2_slab(unit_cube(N_ELEM_SIDE, 0.2, 0), k0, k0 + 2).save_bin(mf)
+        r = subprocess.run(_ref_slab_cmd(mf, os.path.join(td, "o.bin"), repeat), capture_output=True, text=True,
+                           check=True)
+    t = json.loads(r.stdout.strip().splitlines()[-1])["t_assemble_median"]
+    ne = 2 * N_ELEM_SIDE ** 2
+    return {"value": ne / t, "unit": "elements/s", "cores": 1, "kind": "reference",
+            "sample": "z layers %d-%d (%d elements) of the seeded 64^3 C2 mesh, cut faces natural, "
+                      "Discretization::assemble, median of %d" % (k0, k0 + 1, ne, repeat)}
 
 
 def run_reference_arm(args):
-    """--impl reference: the reference's own CPU assembly on all host cores
-    (one single-threaded process per core, each on a bounded sample)."""
+    """--impl reference: the reference's own CPU assembly of the whole seeded
+    64^3 C2 mesh on all host cores.  The mesh is cut into one z-slab per
+    process (the union is exactly C2; cut faces natural, so each element does
+    the work it does in the whole mesh); every process runs the reference's
+    single-threaded Discretization::create + assemble on its slab.  A step is
+    one assembly of every slab: its time is the slowest process's median."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -261,19 +303,21 @@ def run_reference_arm(args):
         print(json.dumps({"impl": "reference", "unavailable": "reference oracle binary oracle/_ref/h3d_ref_driver not built"}))
         return 0
     import tempfile
-    ncores = os.cpu_count() or 1
-    n = CPU_SAMPLE_SIDE
-    steps = args.warmup + args.steps
+    n = N_ELEM_SIDE
+    nproc = max(1, min(os.cpu_count() or 1, n))
+    cuts = [round(i * n / nproc) for i in range(nproc + 1)]
+    # bounded: about a minute of assembly per process at the reference's ~3.6e3 elements/s per core
+    repeat = max(1, min(args.warmup + args.steps, int(60 * 3600 * nproc / n ** 3)))
+    mesh = unit_cube(n, 0.2, 0)
     with tempfile.TemporaryDirectory() as td:
-        mf = os.path.join(td, "m.bin")
-        unit_cube(n, 0.2, 0).save_bin(mf)
         procs = []
+        for c in range(nproc):
+            mf = os.path.join(td, "m%d.bin" % c)
+            c2_slab(mesh, cuts[c], cuts[c + 1]).save_bin(mf)
         t0 = time.time()
-        for c in range(ncores):
-            procs.append(subprocess.Popen([ref_driver.DRIVER, "--mesh", mf, "--out", os.path.join(td, "o%d.bin" % c),
-                                           "--p", str(P_ORDER), "--qmode", "fixed:%d" % N_POINTS, "--mass",
-                                           "--source", "sin", "--repeat", str(steps)],
-                                          stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+        for c in range(nproc):
+            procs.append(subprocess.Popen(_ref_slab_cmd(os.path.join(td, "m%d.bin" % c), os.path.join(td, "o%d.bin" % c),
+                                                        repeat), stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
         outs = [p.communicate() for p in procs]
         wall = time.time() - t0
     times = []
@@ -281,15 +325,17 @@ def run_reference_arm(args):
         line = o.strip().splitlines()[-1] if o.strip() else "{}"
         times.append(json.loads(line).get("t_assemble_median", float("nan")))
     t_step = max(times)
-    value = ncores * n ** 3 / t_step
+    value = n ** 3 / t_step
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": "C2 sample: %d^3 jittered hexahedra per process, p=2, 4^3 Gauss points, grad+mass, "
-                               "sin source" % n, "processes": ncores},
-        "cpu_baseline": {"value": value, "unit": "elements/s", "cores": ncores, "kind": "reference",
-                         "sample": "%d processes x %d^3 elements, %d assemblies each, wall %.1fs" % (ncores, n, steps, wall)},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded jittered unit-cube mesh)", "impl": "reference",
+        "config": {"workload": WORKLOADS["c2"]["desc"], "ndof": 2048383, "nnz": 127263527,
+                   "processes": nproc, "slabs": "z layers %s" % ",".join("%d-%d" % (cuts[i], cuts[i + 1] - 1)
+                                                                         for i in range(nproc))},
+        "cpu_baseline": {"value": value, "unit": "elements/s", "cores": nproc, "kind": "reference",
+                         "sample": "the whole 64^3 C2 mesh as %d z-slabs, one reference process each, median of %d "
+                                   "assemblies per process, wall %.1fs" % (nproc, repeat, wall)},
         "e2e": {"value": value, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
     return 0
@@ -374,6 +420,55 @@ def run_adjoint(args):
     return 0
 
 
+def split_c4(args):
+    """The metric's comparison -- plain FP64 against the tensor-core split
+    precisions at their stated relative error -- on the C4 workload (16^3
+    jittered hexahedra, p = 8, 10^3 points, a_e grad.grad, a_e ~ U[0.5, 2]),
+    all three timed in this run on the device (CUDA events, inputs resident,
+    Ax 15.5 GB > L2) with the clocks sampled.  Errors of each split result
+    against the FP64 kernel's matrix on the same plan (that kernel is checked
+    against the reference's own assembly at p = 5..8 in the GPU tests)."""
+    import torch
+    import hermes3d_b200 as h
+    t0 = time.time()
+    mesh, sp, d = build_problem(h, seed=0, device=0, workload="c4")
+    setup = time.time() - t0
+    ne, nnz = mesh.num_elements, d.nnz
+    steps = max(3, min(args.steps, 10))
+    res = {"workload": WORKLOADS["c4"]["desc"], "elements": ne, "nnz": nnz, "steps": steps,
+           "warmup": max(3, args.warmup), "setup_s": round(setup, 1),
+           "against": "FP64 kernel on the same plan (pinned to the reference's assembly at p = 5..8)"}
+    stream = torch.cuda.current_stream()
+    A = {}
+    for name, prec in [("fp64", h.PREC_FP64), ("tf32x3", h.PREC_TF32X3), ("ozaki", h.PREC_OZAKI)]:
+        A[name] = torch.empty(nnz, dtype=torch.float64, device="cuda")
+        for _ in range(max(3, args.warmup)):
+            d.assemble_device(A[name], None, stream, precision=prec)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(0) as clk:
+            e0.record(stream)
+            for _ in range(steps):
+                d.assemble_device(A[name], None, stream, precision=prec)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        r = {"elements_per_s": ne / (ms * 1e-3), "ms_per_step": ms, "nnz_per_s": nnz / (ms * 1e-3),
+             "gpu_launches_per_step": d.last_launch_count(), "clocks": clk.summary()}
+        if name != "fp64":
+            diff = A[name] - A["fp64"]
+            r["err_max_abs_over_max"] = float(diff.abs().max() / A["fp64"].abs().max())
+            r["err_frobenius_rel"] = float(torch.linalg.vector_norm(diff) / torch.linalg.vector_norm(A["fp64"]))
+            r["tolerance"] = 1e-6 if prec == h.PREC_TF32X3 else 1e-12
+            r["speedup_vs_fp64"] = res["fp64"]["ms_per_step"] / ms
+            del diff, A[name]
+            torch.cuda.empty_cache()
+        res[name] = r
+    del A, d
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_sweep(args):
     """Orders p = 1..8 (p+2 points per direction, jittered cube, a_e grad.grad,
     32^3 elements for p <= 4, 16^3 above): elements/s of the FP64 path (the
@@ -450,6 +545,8 @@ def main():
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-split", action="store_true",
+                    help="leave out the C4 split-precision object of the default (C2) line")
     ap.add_argument("--side", type=int, default=None, help="elements per cube side (profiling runs only)")
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--partition", action="store_true",
@@ -619,15 +716,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind,
                          "algorithmic_bytes_per_step": B,
-                         "fp64_dense_equiv_tflops": ne * dense_flops_per_element(args.workload) / (kms * 1e-3) / 1e12,
-                         # the combined bound: the dense B^T D B contraction at the FP64 peak or the compulsory
-                         # bytes at the HBM peak, whichever takes longer, over the kernel time (sum factorisation
-                         # does less than the dense work, so this can exceed 1)
-                         "combined": None if prec != h.PREC_FP64 else {
-                             "definition": "max(dense-equivalent flops / FP64 peak, algorithmic bytes / HBM peak) / time",
-                             "fp64_peak_tflops": FP64_PEAK_TFLOPS, "fp64_peak_source": "nominal (no measured FP64 figure)",
-                             "frac": max(ne * dense_flops_per_element(args.workload) / (FP64_PEAK_TFLOPS * 1e12),
-                                         B / (hbm * 1e9)) / (kms * 1e-3)}},
+                         "fp64_dense_equiv_tflops": ne * dense_flops_per_element(args.workload) / (kms * 1e-3) / 1e12},
             "e2e": None if e2e_value is None else {
                 "value": e2e_value, "unit": "elements/s", "h2d_bytes_per_step": 24 * nv,
                 "d2h_bytes_per_step": 8 * nnz + 8 * ndof, "ms_per_step": e2e_ms},
@@ -641,6 +730,12 @@ def main():
                 out["cpu_baseline"] = cpu_baseline() if args.workload == "c2" else cpu_baseline_c3()
             except Exception as ex:  # report, do not fail the GPU number
                 out["cpu_baseline"] = {"error": str(ex)[:200]}
+    if rank == 0 and world == 1 and args.workload == "c2" and args.side is None and not args.no_split:
+        # the metric's other half: plain FP64 against the split precisions on the C4 workload
+        del Ax, rhs, d
+        torch.cuda.empty_cache()
+        out["split"] = split_c4(args)
+    if rank == 0:
         print(json.dumps(out))
     if world > 1:
         dist.barrier()

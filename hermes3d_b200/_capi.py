@@ -13,7 +13,10 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libh3dg.so"
 
 H3DG_OK = 0
 H3DG_ERR_STATE = 6
+H3DG_ERR_TIMEOUT = 7
 H3DG_ERR_TOO_LARGE = 8
+DEBUG_WAIT_GIVES_UP = 1
+DEBUG_CORRUPT_POSITION = 2
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "unsupported form",
     5: "mesh error", 6: "call out of order", 7: "device wait timed out", 8: "size limit exceeded",
@@ -90,6 +93,7 @@ SIGNATURES = {
     "h3dg_disc_enable_kernel_timing": [_p, _i32],
     "h3dg_disc_get_tuning": [_p, _pi32, _pi32, C.POINTER(C.c_float)],
     "h3dg_disc_kernel_times": [_p, C.POINTER(C.c_float), _i32, _pi32],
+    "h3dg_disc_debug_inject": [_p, C.c_int],
 }
 _RESTYPES = {"h3dg_status_string": C.c_char_p, "h3dg_last_error": C.c_char_p}
 

@@ -97,6 +97,8 @@ struct h3dg_disc {
 	bool on_device = false;
 	int nparts = 1, part = 0;  // z-slab partition of the next plan (1: whole mesh)
 	int prec_hint = H3DG_PREC_FP64;   // precision the next plan is built for
+	unsigned prepared = 0;     // bit p: an assembly with precision p completed on the current plan
+	int debug_once = 0;        // test hook for the next assembly (H3DG_DEBUG_*)
 	h3dg::PlanScope scope;     // element subset and owned DOFs of the current plan's part
 	int variant = -1;          // autotuned kernel variant (index into the kernel table)
 	float variant_ms = 0.0f;
@@ -486,6 +488,7 @@ h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nn
 	const h3dg::Plan &P = disc->plan;
 	disc->on_device = false;
 	disc->have_plan = true;
+	disc->prepared = 0;
 	disc->have_eval = false;
 	disc->variant = -1;
 	if (ndof) *ndof = P.ndof;
@@ -649,14 +652,41 @@ using namespace h3dg_tables;
 
 extern "C" {
 
-static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, cudaStream_t st) {
+// The high-order kernel of a precision for the current plan, its resident
+// CTAs per SM and the doubles of the per-CTA work area it needs (FP64-accurate
+// split only; 0 otherwise).
+static h3dg_status ho_select(h3dg_disc *disc, int precision, HoSpec **out, int *per_sm_out, size_t *scratch_need) {
 	const h3dg::Plan &P = disc->plan;
 	std::vector<HoSpec> &table = precision == H3DG_PREC_TF32X3 ? ho_tc_table()
 	                             : precision == H3DG_PREC_OZAKI ? ho_oz_table() : ho_table();
-	std::vector<int> cands;
+	HoSpec *k = nullptr;
 	for (size_t i = 0; i < table.size(); i++)
-		if (table[i].p == P.px && table[i].nq == P.nqx) cands.push_back((int) i);
-	if (cands.empty()) return fail(H3DG_ERR_INVALID_ARG, "assemble: no high-order kernel instantiated for this order / rule / precision");
+		if (table[i].p == P.px && table[i].nq == P.nqx) k = &table[i];
+	if (!k) return fail(H3DG_ERR_INVALID_ARG, "assemble: no high-order kernel instantiated for this order / rule / precision");
+	if (!k->configured) {
+		H3DG_CUDA_TRY(cudaFuncSetAttribute(k->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) k->smem));
+		k->configured = true;
+	}
+	int nsm = 148, per_sm = 1;
+	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k->fn, k->threads, k->smem);
+	if (per_sm < 1) per_sm = 1;
+	*out = k;
+	*per_sm_out = per_sm;
+	// G of every resident CTA: 8 x points doubles each (L2-resident)
+	*scratch_need = precision == H3DG_PREC_OZAKI ? (size_t) nsm * per_sm * 8 * (size_t) P.nqx * P.nqy * P.nqz : 0;
+	return H3DG_OK;
+}
+
+static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, cudaStream_t st) {
+	const h3dg::Plan &P = disc->plan;
+	HoSpec *kp = nullptr;
+	int per_sm = 1;
+	size_t scratch_need = 0;
+	{
+		h3dg_status s0 = ho_select(disc, precision, &kp, &per_sm, &scratch_need);
+		if (s0 != H3DG_OK) return s0;
+	}
 	h3dg::KArgsHO a;
 	a.xyz = disc->xyz.p;
 	a.el_vtx = disc->el_vtx.p;
@@ -701,19 +731,10 @@ static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, dou
 	if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
 	int nsm = 148;
 	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
-	HoSpec &k = table[cands.back()];
-	if (!k.configured) {
-		H3DG_CUDA_TRY(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) k.smem));
-		k.configured = true;
-	}
-	int per_sm = 1;
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, k.smem);
-	if (per_sm < 1) per_sm = 1;
+	HoSpec &k = *kp;
 	a.gscratch = nullptr;
 	if (precision == H3DG_PREC_OZAKI) {
-		// G of every resident CTA: 8 x points doubles each (L2-resident)
-		const size_t need = (size_t) nsm * per_sm * 8 * (size_t) P.nqx * P.nqy * P.nqz;
-		if (disc->ho_scratch.n < need) H3DG_CUDA_TRY(disc->ho_scratch.alloc(need));
+		if (disc->ho_scratch.n < scratch_need) H3DG_CUDA_TRY(disc->ho_scratch.alloc(scratch_need));
 		a.gscratch = disc->ho_scratch.p;
 	}
 	const bool rec = disc->tn < disc->tcap;
@@ -1126,7 +1147,11 @@ h3dg_status h3dg_disc_norms(h3dg_disc *disc, const double *d_sol, int exact, dou
 h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream) {
 	h3dg_status s = assemble_volume(disc, precision, d_Ax, d_rhs, stream);
 	if (s != H3DG_OK) return s;
-	return assemble_surface(disc, d_Ax, d_rhs, (cudaStream_t) stream);
+	s = assemble_surface(disc, d_Ax, d_rhs, (cudaStream_t) stream);
+	// the plan's lazily made device state for this precision now exists
+	// (h3dg_disc_assemble_host_noalloc requires it)
+	if (s == H3DG_OK) disc->prepared |= 1u << precision;
+	return s;
 }
 
 static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream) {
@@ -1180,6 +1205,7 @@ static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax,
 	a.Ax = d_Ax;
 	a.rhs = disc->lf ? d_rhs : nullptr;
 	a.status = disc->status.p;
+	a.wait_limit = h3dg::kWaitPolls;
 	if (d_Ax) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
 	if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
 	int nsm = 148;
@@ -1244,6 +1270,9 @@ static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax,
 	int per_sm = 1;
 	if (prepare(K, per_sm) != H3DG_OK) return H3DG_ERR_CUDA;
 	int32_t launches = 0;
+	// test hook: the table-staging wait of this assembly gives up at once
+	if (disc->debug_once == H3DG_DEBUG_WAIT_GIVES_UP) a.wait_limit = 0;
+	disc->debug_once = 0;
 	const bool rec = disc->tn < disc->tcap;
 	if (rec) H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn], st));
 	launches = sweep(K, per_sm);
@@ -1383,25 +1412,21 @@ h3dg_status h3dg_disc_assemble_host(h3dg_disc *disc, int precision, double *Ax, 
 
 } // extern "C"
 
-// Staging array of h3dg_disc_assemble_host_noalloc (16 MiB per device,
-// reserved when the module loads; no allocation at call time).
+// Staging array of h3dg_disc_assemble_host_noalloc (16 MiB on every device
+// that loads the library, held until exit; no allocation at call time).
 static __device__ __align__(256) double g_noalloc_scratch[H3DG_NOALLOC_SCRATCH_DOUBLES];
 
-static h3dg_status noalloc_scratch(int device, double **out) {
-	constexpr int kMaxDevices = 64;
-	static std::mutex mu;
-	static double *ptrs[kMaxDevices] = {};
-	if (device < 0 || device >= kMaxDevices) return fail(H3DG_ERR_INVALID_ARG, "assemble_host_noalloc: device index out of range");
-	std::lock_guard<std::mutex> lock(mu);
-	if (!ptrs[device]) {
-		// set-up once per device, with that device current
-		double *p = nullptr;
-		cudaError_t e = cudaGetSymbolAddress((void **) &p, g_noalloc_scratch);
-		if (e != cudaSuccess || !p)
-			return fail(H3DG_ERR_CUDA, std::string("assemble_host_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-		ptrs[device] = p;
-	}
-	*out = ptrs[device];
+// Device address of the staging array on the current device.  The host-side
+// name g_noalloc_scratch is only a stand-in: a kernel must be given this
+// address.  It is looked up on every call -- once the module is loaded the
+// lookup allocates nothing -- so an address never outlives a context that a
+// cudaDeviceReset destroyed.
+static h3dg_status noalloc_scratch(double **out) {
+	double *p = nullptr;
+	cudaError_t e = cudaGetSymbolAddress((void **) &p, g_noalloc_scratch);
+	if (e != cudaSuccess || !p)
+		return fail(H3DG_ERR_CUDA, std::string("assemble_host_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+	*out = p;
 	return H3DG_OK;
 }
 
@@ -1419,19 +1444,30 @@ h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, doub
 		                                    " doubles exceed the fixed staging array of " +
 		                                    std::to_string((size_t) H3DG_NOALLOC_SCRATCH_DOUBLES) +
 		                                    " (16 MiB); use h3dg_disc_assemble_host");
-	// everything h3dg_disc_assemble would allocate lazily must already exist
-	if (!disc->on_device || !disc->status.p)
-		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: device plan not uploaded; make one allocating assembly call first");
-	if (P.canon && precision == H3DG_PREC_OZAKI && Ax && !disc->ho_scratch.p && P.ne > 0)
-		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: split-precision work area not allocated; make one allocating "
-		                            "assembly call with this precision first");
+	// everything h3dg_disc_assemble would allocate lazily must already exist:
+	// an allocating assembly with this precision completed on this plan
+	if (!disc->on_device || !disc->status.p || !(disc->prepared & (1u << precision)))
+		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: make one allocating assembly call with this precision on "
+		                            "this plan first (h3dg_disc_assemble or h3dg_disc_assemble_host)");
 	if (P.canon && (precision == H3DG_PREC_TF32X3 || precision == H3DG_PREC_OZAKI) && Ax && !disc->el_offt.p && P.ne > 0)
 		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: split-precision scatter stream not built; make one allocating "
-		                            "split-precision assembly call first");
+		                            "split-precision assembly call with the matrix first");
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	if (P.canon && precision == H3DG_PREC_OZAKI && P.ne > 0) {
+		// the work area assemble_ho would (re)allocate: present and large enough
+		HoSpec *k = nullptr;
+		int per_sm = 1;
+		size_t scratch_need = 0;
+		h3dg_status s0 = ho_select(disc, precision, &k, &per_sm, &scratch_need);
+		if (s0 != H3DG_OK) return s0;
+		if (disc->ho_scratch.n < scratch_need)
+			return fail(H3DG_ERR_STATE, "assemble_host_noalloc: split-precision work area smaller than this plan needs; "
+			                            "make one allocating assembly call with this precision first");
+	}
 	if (P.mixed && disc->mx_variant[0] < 0)
 		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: kernel variants not tuned yet; make one allocating assembly "
 		                            "call first");
-	if (!P.canon && disc->variant < 0) {
+	if (!P.mixed && !P.canon && disc->variant < 0) {
 		int ncand = 0;
 		for (size_t i = 0; i < kernel_table().size(); i++)
 			if (kernel_table()[i].p == P.px && kernel_table()[i].nq == P.nqx) ncand++;
@@ -1439,9 +1475,8 @@ h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, doub
 			return fail(H3DG_ERR_STATE, "assemble_host_noalloc: kernel variant not tuned yet; make one allocating assembly "
 			                            "call first");
 	}
-	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
 	double *scratch = nullptr;
-	h3dg_status s0 = noalloc_scratch(disc->device, &scratch);
+	h3dg_status s0 = noalloc_scratch(&scratch);
 	if (s0 != H3DG_OK) return s0;
 	double *d_Ax = Ax ? scratch : nullptr;
 	double *d_rhs = rhs ? scratch + rhs_off : nullptr;
@@ -1489,6 +1524,27 @@ h3dg_status h3dg_disc_update_coefficients_device(h3dg_disc *disc, const double *
 	if (disc->coef.n != (size_t) ne) H3DG_CUDA_TRY(disc->coef.alloc(ne));
 	H3DG_CUDA_TRY(cudaMemcpyAsync(disc->coef.p, d_elem_coef, sizeof(double) * ne, cudaMemcpyDeviceToDevice, (cudaStream_t) stream));
 	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_debug_inject(h3dg_disc *disc, int what) {
+	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "debug_inject: create_pattern() first");
+	const h3dg::Plan &P = disc->plan;
+	if (what == H3DG_DEBUG_WAIT_GIVES_UP) {
+		disc->debug_once = what;
+		return H3DG_OK;
+	}
+	if (what != H3DG_DEBUG_CORRUPT_POSITION) return fail(H3DG_ERR_INVALID_ARG, "debug_inject: unknown hook");
+	if (P.mixed || P.canon) return fail(H3DG_ERR_INVALID_ARG, "debug_inject: position hook needs a low-order plan");
+	{ h3dg_status s0 = ensure_device(disc); if (s0 != H3DG_OK) return s0; }
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	// entry (a = 0, b = 0) of the first element with a matrix entry
+	for (int64_t k = 0; k < P.ne; k++)
+		if (P.el_cnt[2 * k] > 0) {
+			const uint16_t bad = 0xFFFF;
+			H3DG_CUDA_TRY(cudaMemcpy(disc->el_off.p + (size_t) k * P.nl * P.nl, &bad, sizeof(bad), cudaMemcpyHostToDevice));
+			return H3DG_OK;
+		}
+	return fail(H3DG_ERR_INVALID_ARG, "debug_inject: the plan has no matrix entry");
 }
 
 h3dg_status h3dg_disc_last_launch_count(const h3dg_disc *disc, int32_t *count) {

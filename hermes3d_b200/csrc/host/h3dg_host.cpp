@@ -362,14 +362,23 @@ static void phys_point(const Mesh &m, int64_t e, double x, double y, double z, d
 	}
 }
 
-// Cholesky solve of a symmetric positive-definite system (upper triangle given)
-static void chol_solve(std::vector<double> &a, int n, std::vector<double> &b) {
+// Cholesky solve of a symmetric positive-definite system (upper triangle
+// given): the decomposition and substitutions of Numerical Recipes (Press et
+// al., 2nd ed., section 2.9, choldc / cholsl), the published algorithm the
+// reference uses (src/matrix.cc:105-130), in the same loop order so that the
+// projection coefficients agree to rounding.  Returns -1 on a pivot that is
+// not positive (where the reference's choldc exits) and -2 on a non-finite
+// solution (boundary values that are not finite).
+static int chol_solve(std::vector<double> &a, int n, std::vector<double> &b) {
 	std::vector<double> p(n);
 	for (int i = 0; i < n; i++)
 		for (int j = i; j < n; j++) {
 			double sum = a[i * n + j];
 			for (int k = i - 1; k >= 0; k--) sum -= a[i * n + k] * a[j * n + k];
-			if (i == j) p[i] = std::sqrt(sum);
+			if (i == j) {
+				if (!(sum > 0.0)) return -1;
+				p[i] = std::sqrt(sum);
+			}
 			else a[j * n + i] = sum / p[i];
 		}
 	for (int i = 0; i < n; i++) {
@@ -382,6 +391,9 @@ static void chol_solve(std::vector<double> &a, int n, std::vector<double> &b) {
 		for (int k = i + 1; k < n; k++) sum -= a[k * n + i] * b[k];
 		b[i] = sum / p[i];
 	}
+	for (int i = 0; i < n; i++)
+		if (!std::isfinite(b[i])) return -2;
+	return 0;
 }
 
 // H1Space::calc_edge_boundary_projection (src/space/h1.cc:161-258): L2
@@ -389,12 +401,12 @@ static void chol_solve(std::vector<double> &a, int n, std::vector<double> &b) {
 // vertex interpolant onto the edge functions.  The right-hand side uses the
 // 13-point rule (the maximal edge order, 24); the mass matrix is computed
 // exactly (same rule), as the reference's per-pair rule also is.
-void Space::lift_edge(int64_t e, int iedge) {
+int Space::lift_edge(int64_t e, int iedge) {
 	int64_t eid = mesh->elem_edge[12 * e + iedge];
 	EData &en = ed[eid];
-	if (en.bc != BC_ESSENTIAL || en.has_proj) return;
+	if (en.bc != BC_ESSENTIAL || en.has_proj) return 0;
 	int nf = en.n;
-	if (nf <= 0) return;
+	if (nf <= 0) return 0;
 	std::vector<int64_t> idx;
 	edge_indices(iedge, mesh->edge_orientation(e, iedge), en.order, idx);
 	std::vector<double> q, w;
@@ -417,18 +429,20 @@ void Space::lift_edge(int64_t e, int iedge) {
 			rhs[i] += w[k] * phi[i] * g;
 		}
 	}
-	chol_solve(M, nf, rhs);
+	const int rc = chol_solve(M, nf, rhs);
+	if (rc != 0) return rc;
 	en.proj = rhs;
 	en.has_proj = true;
+	return 0;
 }
 
 // H1Space::calc_face_boundary_projection (src/space/h1.cc:260-394)
-void Space::lift_face(int64_t e, int iface) {
+int Space::lift_face(int64_t e, int iface) {
 	int64_t fid = mesh->elem_face[6 * e + iface];
 	FData &fn = fd[fid];
-	if (fn.bc != BC_ESSENTIAL || fn.has_proj) return;
+	if (fn.bc != BC_ESSENTIAL || fn.has_proj) return 0;
 	int nf = fn.n;
-	if (nf <= 0) return;
+	if (nf <= 0) return 0;
 	// vertex and edge functions of the face with their lifting coefficients
 	std::vector<int64_t> bidx;
 	std::vector<double> bcoef;
@@ -491,9 +505,11 @@ void Space::lift_face(int64_t e, int iface) {
 				rhs[i] += wt * phi[i] * g;
 			}
 		}
-	chol_solve(M, nf, rhs);
+	const int rc = chol_solve(M, nf, rhs);
+	if (rc != 0) return rc;
 	fn.proj = rhs;
 	fn.has_proj = true;
+	return 0;
 }
 
 static void set_bc_info(int &bc, int &marker, int newbc, int newmarker) {
@@ -640,18 +656,35 @@ int Space::assign_dofs(int first, int strd, std::string &err) {
 	// element id order; the constraints of the hanging nodes (computed by
 	// uc_element of the refined base element) come after every base element
 	// and before the children, whose boundary projections use them
-	auto lift_element = [&](int64_t e) {
-		for (int ie = 0; ie < 12; ie++) lift_edge(e, ie);
-		if (!mesh->active(e)) return;
+	// a projection that fails (pivot not positive, or boundary values that are
+	// not finite) is an error, as choldc's EXIT is in the reference
+	auto lift_element = [&](int64_t e) -> int {
+		for (int ie = 0; ie < 12; ie++) {
+			const int rc = lift_edge(e, ie);
+			if (rc) {
+				err = std::string("boundary projection of an edge of element ") + std::to_string(e + 1) +
+				      (rc == -1 ? ": projection matrix not positive definite" : ": Dirichlet values not finite");
+				return -1;
+			}
+		}
+		if (!mesh->active(e)) return 0;
 		for (int f = 0; f < 6; f++)
-			if (mesh->facet_outer[mesh->elem_face[6 * e + f]]) lift_face(e, f);
+			if (mesh->facet_outer[mesh->elem_face[6 * e + f]]) {
+				const int rc = lift_face(e, f);
+				if (rc) {
+					err = std::string("boundary projection of a face of element ") + std::to_string(e + 1) +
+					      (rc == -1 ? ": projection matrix not positive definite" : ": Dirichlet values not finite");
+					return -1;
+				}
+			}
+		return 0;
 	};
 	for (int64_t e = 0; e < ne; e++)
-		if (!mesh->nrefined || mesh->parent[e] < 0) lift_element(e);
+		if ((!mesh->nrefined || mesh->parent[e] < 0) && lift_element(e) != 0) return -1;
 	if (!mesh->interfaces.empty() && build_constraints(err) != 0) return -1;
 	if (mesh->nrefined)
 		for (int64_t e = 0; e < ne; e++)
-			if (mesh->parent[e] >= 0) lift_element(e);
+			if (mesh->parent[e] >= 0 && lift_element(e) != 0) return -1;
 	assigned = true;
 	return 0;
 }

@@ -142,8 +142,8 @@ struct Space {
 	bool element_constrained(int64_t e) const;
 
 private:
-	void lift_edge(int64_t e, int iedge);
-	void lift_face(int64_t e, int iface);
+	int lift_edge(int64_t e, int iedge);     // 0, or -1 / -2 when the projection fails
+	int lift_face(int64_t e, int iface);
 	int build_constraints(std::string &err);
 	void constrained_assembly_list(int64_t e, std::vector<AsmEntry> &al) const;
 };

@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(NT) k_assemble_fp64_seq(KArgs args, int64_t kb
 	double *E0 = sm + S::S_E;
 	const int tid = threadIdx.x;
 
-	if (!stage_tables(tab, args.tables, args.table_bytes, &bar, args.status)) return;
+	if (!stage_tables(tab, args.tables, args.table_bytes, &bar, args.status, args.wait_limit)) return;
 
 	// 1D product tables, once per CTA
 	for (int i = tid; i < S::WX; i += NT) {

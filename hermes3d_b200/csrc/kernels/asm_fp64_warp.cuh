@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(32 * W, MINB) k_assemble_fp64_warp(KArgs args,
 	int *s_m = s_mw + warp, *s_l = s_lw + warp;
 	double *s_cg = s_cgw + warp;
 
-	if (!stage_tables(tab, args.tables, args.table_bytes, &bar, args.status)) return;
+	if (!stage_tables(tab, args.tables, args.table_bytes, &bar, args.status, args.wait_limit)) return;
 	constexpr int NTC = 32 * W;
 	const int ctid = threadIdx.x;
 

@@ -7,6 +7,9 @@
 
 namespace h3dg {
 
+// polls of a bounded mbarrier wait before it gives up (seconds at the B200's clock)
+constexpr unsigned kWaitPolls = 1u << 24;
+
 // error bits written to the plan's device status word
 constexpr int kErrTimeout = 1;
 constexpr int kErrBounds = 2;    // a scatter target fell outside its (non-empty) CSC column (store skipped);
@@ -32,6 +35,7 @@ struct KArgs {
 	double *Ax;               // nnz (may be nullptr)
 	double *rhs;              // ndof (may be nullptr)
 	int *status;              // device status word
+	unsigned wait_limit;      // polls of the bounded waits (kWaitPolls; 0 only from the test hook)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -73,7 +77,7 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
 
 // Wait on phase `parity` of an mbarrier for at most `limit` polls.  Returns
 // false (and records kErrTimeout) if the phase did not complete.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *status, uint32_t limit = (1u << 24)) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *status, uint32_t limit = kWaitPolls) {
 	for (uint32_t it = 0; it < limit; it++)
 		if (mbar_try_wait(bar, parity)) return true;
 	if (status) atomicOr(status, kErrTimeout);
@@ -83,7 +87,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
 // Stage the 1D tables blob into shared memory with one bulk copy (thread 0
 // issues, everybody waits).  Returns false on timeout; the caller must then
 // leave after a bounded second wait so no copy is left in flight.
-__device__ __forceinline__ bool stage_tables(double *dst, const double *src, int bytes, uint64_t *bar, int *status) {
+__device__ __forceinline__ bool stage_tables(double *dst, const double *src, int bytes, uint64_t *bar, int *status,
+                                             uint32_t limit = kWaitPolls) {
 	if (threadIdx.x == 0) {
 		mbar_init(bar, 1);
 		fence_mbar_init();
@@ -93,7 +98,7 @@ __device__ __forceinline__ bool stage_tables(double *dst, const double *src, int
 		mbar_arrive_expect_tx(bar, (uint32_t) bytes);
 		bulk_g2s(dst, src, (uint32_t) bytes, bar);
 	}
-	bool ok = mbar_wait_bounded(bar, 0, status);
+	bool ok = mbar_wait_bounded(bar, 0, status, limit);
 	if (!ok) mbar_wait_bounded(bar, 0, nullptr, 1u << 26);
 	// every thread returns the same verdict, so an early exit is block-uniform
 	return __syncthreads_and(ok ? 1 : 0) != 0;

@@ -429,6 +429,14 @@ class Discretization:
         capi.call("h3dg_disc_last_launch_count", self.handle, C.byref(n))
         return n.value
 
+    def debug_inject(self, what: int):
+        """Test hook (no reference counterpart): DEBUG_WAIT_GIVES_UP makes the
+        next FP64 low-order assembly's bounded wait give up (H3dgError
+        TIMEOUT from ``assemble``); DEBUG_CORRUPT_POSITION points one position
+        of the device scatter map past its column (H3dgError STATE until
+        ``create`` rebuilds the plan).  Neither faults the device."""
+        capi.call("h3dg_disc_debug_inject", self.handle, int(what))
+
     def __del__(self):
         if getattr(self, "handle", None) and capi._lib is not None:
             capi.lib().h3dg_disc_destroy(self.handle)

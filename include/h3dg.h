@@ -216,13 +216,15 @@ h3dg_status h3dg_disc_assemble_host(h3dg_disc *disc, int precision, double *Ax, 
  * shared by Ax and rhs, the rhs part starting on a 256-byte boundary);
  * larger problems are rejected with H3DG_ERR_TOO_LARGE.  Preconditions
  * (H3DG_ERR_STATE otherwise): one allocating device call on this disc with
- * the same precision came first (h3dg_disc_assemble or
+ * the same precision came first on the current plan (h3dg_disc_assemble or
  * h3dg_disc_assemble_host), so the device plan, the autotuned variant and
- * the split-precision scatter stream exist.  The first call on a device
- * looks up the array's address (cudaGetSymbolAddress) with that device
- * current; make it outside any stream capture.  The array is zeroed by the
- * assembly itself.  Calls that overlap in time on one device share the
- * array and race: serialise them. */
+ * the split-precision scatter stream and work area exist.  Every call looks
+ * up the array's address (cudaGetSymbolAddress, which allocates nothing once
+ * the library's module is loaded) with the disc's device current, so a
+ * cudaDeviceReset between calls leaves no stale address; make the first call
+ * outside any stream capture, since it may load the module.  The array is
+ * zeroed by the assembly itself.  Calls that overlap in time on one device
+ * share the array and race: serialise them. */
 #define H3DG_NOALLOC_SCRATCH_DOUBLES (2u << 20)
 h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, double *Ax, double *rhs);
 /* replace the vertex coordinates (same topology) from host memory, nv x 3 */
@@ -268,6 +270,20 @@ h3dg_status h3dg_disc_adjoint(h3dg_disc *disc, int nfields, const double *d_logc
  * the int32 result is returned as floats), C 128 x 128; device pointers.
  * Checks the tensor-core layer the split-precision kernels use. */
 h3dg_status h3dg_tc_selftest(int kind, const float *d_A, const float *d_B, float *d_C, int device);
+
+/* Test hooks (no reference counterpart): drive the failure paths of an
+ * assembly without any device fault.
+ *   H3DG_DEBUG_WAIT_GIVES_UP: the next FP64 low-order assembly gives its
+ *     bounded table-staging wait no polls at all, so every CTA records a
+ *     timeout, drains its copy and leaves; h3dg_disc_assemble_host then
+ *     returns H3DG_ERR_TIMEOUT and the following assembly runs normally.
+ *   H3DG_DEBUG_CORRUPT_POSITION: one entry of the device position map of a
+ *     low-order plan is set past the end of its CSC column; the bounds check
+ *     skips that store and assemblies report H3DG_ERR_STATE until
+ *     h3dg_disc_create_pattern builds the plan again. */
+#define H3DG_DEBUG_WAIT_GIVES_UP    1
+#define H3DG_DEBUG_CORRUPT_POSITION 2
+h3dg_status h3dg_disc_debug_inject(h3dg_disc *disc, int what);
 
 /* RefMap (src/refmap.cc:177-231, 265-316): per element (id order) and per point of the
  * disc's volume rule, the signed Jacobian determinant (get_jacobian without the

@@ -20,7 +20,33 @@ struct JArr {
 
 struct JL : JArr {
 	std::map<Word_t, Word_t> m;
+	// maximal runs of consecutive keys, start -> last key, so that
+	// JudyLFirstEmpty answers in O(log n) as Judy's does (a linear scan made
+	// the reference's Map::set, and so mesh building, quadratic)
+	std::map<Word_t, Word_t> runs;
 	Word_t bytes() const { return m.size() * 48; }
+	void run_insert(Word_t k) {
+		std::map<Word_t, Word_t>::iterator nx = runs.upper_bound(k);
+		bool join_prev = false;
+		std::map<Word_t, Word_t>::iterator pv = nx;
+		if (pv != runs.begin()) {
+			--pv;
+			if (pv->second != ~0UL && pv->second + 1 == k) join_prev = true;
+		}
+		bool join_next = k != ~0UL && nx != runs.end() && nx->first == k + 1;
+		if (join_prev && join_next) { pv->second = nx->second; runs.erase(nx); }
+		else if (join_prev) pv->second = k;
+		else if (join_next) { Word_t last = nx->second; runs.erase(nx); runs[k] = last; }
+		else runs[k] = k;
+	}
+	void run_erase(Word_t k) {
+		std::map<Word_t, Word_t>::iterator r = runs.upper_bound(k);
+		--r;                                     // the run holding k
+		Word_t a = r->first, b = r->second;
+		runs.erase(r);
+		if (a < k) runs[a] = k - 1;
+		if (k < b) runs[k + 1] = b;
+	}
 };
 
 struct J1 : JArr {
@@ -59,13 +85,19 @@ inline PPvoid_t slot(Word_t &v) { return (PPvoid_t) &v; }
 
 PPvoid_t JudyLIns(PPvoid_t PPArray, Word_t Index, PJError_t) {
 	JL *a = get_or_make<JL>(PPArray);
-	return slot(a->m[Index]);                // value-initialised to 0 when new
+	std::map<Word_t, Word_t>::iterator it = a->m.lower_bound(Index);
+	if (it == a->m.end() || it->first != Index) {
+		it = a->m.insert(it, std::make_pair(Index, (Word_t) 0));   // value-initialised to 0 when new
+		a->run_insert(Index);
+	}
+	return slot(it->second);
 }
 
 int JudyLDel(PPvoid_t PPArray, Word_t Index, PJError_t) {
 	if (*PPArray == NULL) return 0;
 	JL *a = get<JL>(*PPArray);
 	int rc = (int) a->m.erase(Index);
+	if (rc) a->run_erase(Index);
 	if (a->m.empty()) free_any(PPArray);
 	return rc;
 }
@@ -80,6 +112,10 @@ PPvoid_t JudyLGet(Pcvoid_t PArray, Word_t Index, PJError_t) {
 Word_t JudyLCount(Pcvoid_t PArray, Word_t I1, Word_t I2, PJError_t) {
 	if (PArray == NULL || I1 > I2) return 0;
 	JL *a = get<JL>(PArray);
+	// whole-range counts (Array::count(), once per add_vertex / add_hex) in
+	// constant time, as Judy's population counters give them
+	if (a->m.empty()) return 0;
+	if (I1 <= a->m.begin()->first && I2 >= a->m.rbegin()->first) return (Word_t) a->m.size();
 	Word_t n = 0;
 	for (std::map<Word_t, Word_t>::iterator it = a->m.lower_bound(I1); it != a->m.end() && it->first <= I2; ++it) n++;
 	return n;
@@ -141,11 +177,13 @@ int JudyLFirstEmpty(Pcvoid_t PArray, Word_t *PIndex, PJError_t) {
 	Word_t i = *PIndex;
 	if (PArray == NULL) return 1;
 	JL *a = get<JL>(PArray);
-	std::map<Word_t, Word_t>::iterator it = a->m.lower_bound(i);
-	while (it != a->m.end() && it->first == i) {
-		if (i == ~0UL) return 0;
-		++i;
-		++it;
+	std::map<Word_t, Word_t>::iterator r = a->runs.upper_bound(i);
+	if (r != a->runs.begin()) {
+		--r;
+		if (r->second >= i) {                    // i is taken: the slot after its run
+			if (r->second == ~0UL) return 0;
+			i = r->second + 1;
+		}
 	}
 	*PIndex = i;
 	return 1;
@@ -172,6 +210,8 @@ int Judy1Test(Pcvoid_t PArray, Word_t Index, PJError_t) {
 Word_t Judy1Count(Pcvoid_t PArray, Word_t I1, Word_t I2, PJError_t) {
 	if (PArray == NULL || I1 > I2) return 0;
 	J1 *a = get<J1>(PArray);
+	if (a->s.empty()) return 0;
+	if (I1 <= *a->s.begin() && I2 >= *a->s.rbegin()) return (Word_t) a->s.size();
 	Word_t n = 0;
 	for (std::set<Word_t>::iterator it = a->s.lower_bound(I1); it != a->s.end() && *it <= I2; ++it) n++;
 	return n;

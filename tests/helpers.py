@@ -211,3 +211,41 @@ def system_problem(g, device=0):
     d.set_linear_form(1, src[p.get("source2", "none")])
     d.set_quadrature(p_plus=2)
     return mesh, spaces, d
+
+
+HIGHORDER = os.path.join(GOLDEN, "highorder")
+
+
+def highorder_names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(HIGHORDER, "*.npz")))
+
+
+def load_highorder(name):
+    z = np.load(os.path.join(HIGHORDER, name + ".npz"), allow_pickle=False)
+    d = {k: z[k] for k in z.files}
+    d["params"] = ast.literal_eval(str(d["params"]))
+    return d
+
+
+def highorder_problem(g, device=0):
+    """Space (BC type per marker, Dirichlet x^2+y^2+z^2) and discretization
+    (a_e grad.grad [+ mass], source) of a high-order fixture."""
+    p = g["params"]
+    mesh = mesh_of(g)
+    mesh.ugh()
+    sp = h.H1Space(mesh)
+    nat = set(p.get("natural_markers") or [])
+    all_nat = p.get("bc") == "natural"
+    sp.set_bc_types(lambda m: h.BC_NATURAL if (all_nat or m in nat) else h.BC_ESSENTIAL)
+    if p.get("bc") == "dirichlet_poly":
+        sp.set_bc_values(lambda m, x, y, z: x * x + y * y + z * z)
+    sp.set_uniform_order(p["p"])
+    sp.assign_dofs()
+    d = h.Discretization(device)
+    d.set_spaces(sp)
+    d.set_bilinear_form(h.int_grad_u_grad_v_plus_u_v if p.get("mass") else h.int_grad_u_grad_v, g["gradcoef"])
+    src = p.get("source", "one")
+    d.set_linear_form({"one": h.int_F_v(1.0), "sin": h.int_F_v("sin"), "poly": h.int_F_v(-6.0)}[src])
+    kind, n = quad_of(g)
+    d.set_quadrature(p_plus=n) if kind == "pplus" else d.set_quadrature(points=n)
+    return mesh, sp, d

@@ -109,3 +109,18 @@ def test_assembly_without_device_fails_loudly():
     with pytest.raises(capi.H3dgError) as ei:
         d.assemble(M, V)
     assert ei.value.status == 2
+
+
+def test_non_finite_dirichlet_values_are_an_error():
+    """A boundary projection that cannot be solved (here: Dirichlet values
+    that are not finite) fails assign_dofs, as choldc's exit does in the
+    reference, instead of leaving NaN lifting coefficients."""
+    mesh = h.unit_cube(2)
+    mesh.ugh()
+    sp = h.H1Space(mesh)
+    sp.set_bc_values(lambda m, x, y, z: float("nan") if m == 3 else 1.0)
+    sp.set_uniform_order(3)
+    with pytest.raises(capi.H3dgError) as e:
+        sp.assign_dofs()
+    assert e.value.status == capi.H3DG_ERR_STATE
+    assert "not finite" in str(e.value)

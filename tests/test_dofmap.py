@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import hermes3d_b200 as h
-from helpers import disc_of, golden_names, load, space_of
+from helpers import disc_of, golden_names, highorder_names, highorder_problem, load, load_highorder, space_of
 
 
 @pytest.mark.parametrize("name", golden_names())
@@ -71,3 +71,21 @@ def test_relabelling_changes_numbering_not_dof_count():
         sp.set_uniform_order(4)
         counts.append(sp.assign_dofs())
     assert len(set(counts)) == 1
+
+
+@pytest.mark.parametrize("name", highorder_names())
+def test_high_order_dof_map_and_pattern_bit_exact(name):
+    """Orders 5..8 with natural and Dirichlet faces mixed: assembly lists
+    (indices, DOFs, lifting coefficients) and the CSC pattern."""
+    g = load_highorder(name)
+    mesh, sp, d = highorder_problem(g)
+    assert sp.get_dof_count() == int(g["ndof"])
+    for e in range(1, len(g["hexes"]) + 1):
+        a, b = g["al_ptr"][e - 1], g["al_ptr"][e]
+        idx, dof, coef = sp.get_element_assembly_list(e)
+        assert np.array_equal(idx, g["al_idx"][a:b]), e
+        assert np.array_equal(dof, g["al_dof"][a:b]), e
+        assert np.allclose(coef, g["al_coef"][a:b], rtol=1e-12, atol=1e-12), e
+    M = h.UMFPackMatrix()
+    d.create(M, h.UMFPackVector())
+    assert np.array_equal(M.Ap, g["Ap"]) and np.array_equal(M.Ai, g["Ai"])

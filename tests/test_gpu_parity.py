@@ -120,6 +120,35 @@ def test_c1_full_size_against_reference(gpu):
     assert rel_err(V.v, r["rhs"]) < FP64_RTOL
 
 
+@pytest.mark.skipif(not ref_driver.available(), reason="reference oracle binary not built")
+def test_c2_full_size_against_reference(gpu):
+    """The headline workload at full size against the reference itself, run
+    live on the host (about 3 minutes on one core): 64^3 jittered (+-0.2h,
+    seed 0) hexahedra, p=2, 4^3 Gauss points, grad.grad + mass,
+    f = sin(pi x) sin(pi y) sin(pi z).  DOF count and CSC pattern bit for bit,
+    Ax and rhs within 1e-12 of the largest entry."""
+    mesh = h.unit_cube(64, 0.2, 0)
+    r = ref_driver.run(mesh, p=2, qmode="fixed:4", mass=True, source="sin", bc="dirichlet0", timeout=3000)
+    mesh.ugh()
+    sp = h.H1Space(mesh)
+    sp.set_uniform_order(2)
+    sp.assign_dofs()
+    assert sp.ndof == r["ndof"] == 2048383
+    d = h.Discretization()
+    d.set_spaces(sp)
+    d.set_bilinear_form(h.int_grad_u_grad_v_plus_u_v)
+    d.set_linear_form(h.int_F_v("sin"))
+    d.set_quadrature(points=4)
+    M, V = h.UMFPackMatrix(), h.UMFPackVector()
+    d.create(M, V)
+    assert np.array_equal(M.Ap, r["Ap"]) and np.array_equal(M.Ai, r["Ai"])
+    del r["Ai"]
+    d.assemble(M, V)
+    e_ax, e_rhs = rel_err(M.Ax, r["Ax"]), rel_err(V.v, r["rhs"])
+    print("C2 64^3 vs reference: Ax %.2e rhs %.2e" % (e_ax, e_rhs))
+    assert e_ax < FP64_RTOL and e_rhs < FP64_RTOL
+
+
 def test_c2_full_size_properties(gpu):
     """64^3 jittered, p=2, 4 points, grad+mass, sin source: the matrix is
     symmetric and positive definite on random vectors; assembled twice it is

@@ -7,7 +7,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from helpers import FP64_RTOL, golden_names, load, lf_of, nq_of, rel_err
+from helpers import FP64_RTOL, golden_names, highorder_names, lf_of, load, load_highorder, nq_of, rel_err
 from oracle import port, ref_driver
 
 REF = "/root/reference"
@@ -73,3 +73,19 @@ def test_refmap_fixture_is_consistent():
         prod = np.einsum("eqrc,eqrd->eqcd", irm, rm)      # irm^T rm = I  (irm = J^-T)
         assert np.allclose(prod, np.eye(3), atol=2e-5), name
         assert np.allclose(np.linalg.det(rm), z[name + "_jac"], atol=2e-5), name
+
+
+@pytest.mark.parametrize("name", highorder_names())
+def test_port_matches_reference_at_high_order(name):
+    """Orders 5..8 (up to 729 functions, 10^3 points) on jittered elements:
+    the restatement's pattern and values against the reference's."""
+    g = load_highorder(name)
+    p = g["params"]
+    lf, lv = lf_of(g)
+    al = (g["al_ptr"], g["al_idx"], g["al_dof"].astype(np.int32), g["al_coef"])
+    Ap, Ai = port.pattern(g["al_ptr"], g["al_dof"].astype(np.int32), int(g["ndof"]))
+    assert np.array_equal(Ap, g["Ap"]) and np.array_equal(Ai, g["Ai"])
+    Ax, rhs = port.assemble(g["xyz"], g["hexes"] - 1, nq_of(g), al, int(g["ndof"]), g["Ap"], g["Ai"],
+                            mass=p.get("mass", False), gradcoef=g["gradcoef"], lf=lf, lf_value=lv)
+    assert rel_err(Ax, g["Ax"]) < FP64_RTOL
+    assert rel_err(rhs, g["rhs"]) < FP64_RTOL
