@@ -92,6 +92,8 @@ SIGNATURES = {
     "h3dg_disc_get_partition_elements": [_p, _p, C.c_int64],
     "h3dg_disc_enable_kernel_timing": [_p, _i32],
     "h3dg_disc_get_tuning": [_p, _pi32, _pi32, C.POINTER(C.c_float)],
+    "h3dg_disc_tuned_scatter": [_p, _pi32],
+    "h3dg_disc_seg_stats": [_p, C.POINTER(C.c_int64)],
     "h3dg_disc_kernel_times": [_p, C.POINTER(C.c_float), _i32, _pi32],
     "h3dg_disc_debug_inject": [_p, C.c_int],
 }

@@ -117,6 +117,15 @@ struct h3dg_disc {
 	DBuf<double> el_ccoef;
 	DBuf<double> el_coef;
 	DBuf<int> status;
+	// segmented scatter: plan tables, the item schedule of the current launch
+	// shape, counters and the element-matrix ring
+	DBuf<int32_t> seg_kof, seg_col, seg_pe, seg_items, seg_p1n, seg_p2n;
+	DBuf<int64_t> seg_cptr;
+	DBuf<uint16_t> seg_plm, seg_off;
+	DBuf<unsigned> seg_ctr;
+	DBuf<double> seg_ring;
+	int seg_ctas = 0, seg_per_item = 0, seg_nitems = 0, seg_ring_win = 0;
+	bool seg_all_dofs = false;  // every DOF has a column (no RHS zero-fill needed)
 	int table_bytes = 0;
 	// kernel-only timing records
 	std::vector<cudaEvent_t> tev;
@@ -568,6 +577,16 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 		H3DG_CUDA_TRY(disc->el_dof.upload(P.el_dof));
 		H3DG_CUDA_TRY(disc->el_coef.upload(P.el_coef));
 		H3DG_CUDA_TRY(disc->el_off.upload(P.el_off));
+		if (P.seg) {
+			H3DG_CUDA_TRY(disc->seg_kof.upload(P.seg_kof));
+			H3DG_CUDA_TRY(disc->seg_col.upload(P.seg_col));
+			H3DG_CUDA_TRY(disc->seg_cptr.upload(P.seg_cptr));
+			H3DG_CUDA_TRY(disc->seg_pe.upload(P.seg_pe));
+			H3DG_CUDA_TRY(disc->seg_plm.upload(P.seg_plm));
+			H3DG_CUDA_TRY(disc->seg_off.upload(P.seg_off));
+			disc->seg_all_dofs = (int64_t) P.seg_col.size() == P.ndof;
+		}
+		disc->seg_ctas = 0;
 	}
 	if (P.nsf > 0) {
 		H3DG_CUDA_TRY(disc->sf_desc.upload(P.sf_desc));
@@ -1154,6 +1173,123 @@ h3dg_status h3dg_disc_assemble(h3dg_disc *disc, int precision, double *d_Ax, dou
 	return s;
 }
 
+// Low-order uniform plans: the colour-sweep kernels for (p, rule) and, where
+// the plan carries the segmented-scatter tables, the segmented kernels
+// (numbered from kSegVariant).  H3DG_SCATTER=colour or =segmented keeps one
+// family (tests compare the two bit for bit).
+static constexpr int kSegVariant = 1000;
+
+static std::vector<int> lo_candidates(const h3dg_disc *disc) {
+	const h3dg::Plan &P = disc->plan;
+	const char *only = std::getenv("H3DG_SCATTER");
+	const bool colour = !only || std::strcmp(only, "segmented") != 0;
+	const bool seg = P.seg && (!only || std::strcmp(only, "colour") != 0);
+	std::vector<int> c;
+	if (colour)
+		for (size_t i = 0; i < kernel_table().size(); i++)
+			if (kernel_table()[i].p == P.px && kernel_table()[i].nq == P.nqx) c.push_back((int) i);
+	if (seg)
+		for (size_t i = 0; i < seg_table().size(); i++)
+			if (seg_table()[i].p == P.px && seg_table()[i].nq == P.nqx) c.push_back(kSegVariant + (int) i);
+	return c;
+}
+
+static int seg_colcap(const h3dg::Plan &P) { return (std::min(P.seg_maxcol, 2048) + 1) & ~1; }
+
+// Item schedule (ticket order) and ring of a segmented launch with as many
+// CTAs as fit on the device.  The column items of ready window v follow the
+// element items of window v + lag, lag ~ the elements one round of all CTAs
+// takes, so their elements are done by the time they are taken; the ring
+// holds span + lag + 2 windows, so an element item overwrites only slots
+// whose column items precede it in ticket order (it waits for them).
+static h3dg_status seg_prepare(h3dg_disc *disc, SegSpec &k, int nsm) {
+	const h3dg::Plan &P = disc->plan;
+	const int colcap = seg_colcap(P);
+	const size_t smem = k.smem(colcap);
+	if (!k.configured || k.configured_smem < smem) {
+		H3DG_CUDA_TRY(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+		k.configured = true;
+		k.configured_smem = smem;
+	}
+	int per_sm = 1;
+	H3DG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, smem));
+	const int ctas = nsm * std::max(per_sm, 1);
+	if (disc->seg_ctas == ctas && disc->seg_per_item == k.per_item && disc->seg_items.p && !std::getenv("H3DG_SEG_LAG") &&
+	    !std::getenv("H3DG_SEG_RING"))
+		return H3DG_OK;
+	const int W = P.seg_window, nwin = P.seg_nwin;
+	// H3DG_SEG_LAG: the lag in rounds of all CTAs (default 2)
+	const double rounds = std::getenv("H3DG_SEG_LAG") ? std::atof(std::getenv("H3DG_SEG_LAG")) : 2.0;
+	const int lag = (int) std::min<int64_t>(nwin, (int64_t) std::ceil(rounds * ctas * k.per_item / W) + 2);
+	std::vector<int32_t> items, p1n(nwin, 0), p2n(nwin, 0);
+	auto columns = [&](int v) {
+		for (int64_t b = P.seg_p2ptr[v]; b < P.seg_p2ptr[v + 1]; b++) {
+			items.insert(items.end(), &P.seg_p2[4 * b], &P.seg_p2[4 * b] + 4);
+			p2n[v]++;
+		}
+	};
+	for (int w = 0; w < nwin; w++) {
+		const int64_t e1 = std::min<int64_t>((int64_t) (w + 1) * W, P.ne);
+		for (int64_t e = (int64_t) w * W; e < e1; e += k.per_item) {
+			items.insert(items.end(), { w, -1, (int32_t) e, (int32_t) std::min<int64_t>(e + k.per_item, e1) });
+			p1n[w]++;
+		}
+		if (w - lag >= 0) columns(w - lag);
+	}
+	for (int v = std::max(0, nwin - lag); v < nwin; v++) columns(v);
+	// ring: beyond span + lag, the windows the tickets in flight cover (about
+	// two per CTA), so an element item rarely finds the column items that last
+	// read its slots still running.  H3DG_SEG_RING: extra windows (profiling)
+	const int per_win = (int) std::max<int64_t>(1, (int64_t) items.size() / 4 / nwin);
+	const int front = (2 * ctas + per_win - 1) / per_win;
+	const int extra = std::getenv("H3DG_SEG_RING") ? std::atoi(std::getenv("H3DG_SEG_RING")) : front + 2;
+	const int ring_win = (int) std::min<int64_t>(nwin, (int64_t) P.seg_span + lag + std::max(2, extra));
+	const int cw = (P.nl + 2) & ~1;
+	const size_t ring = (size_t) ring_win * W * P.nl * cw;
+	H3DG_CUDA_TRY(disc->seg_items.upload(items));
+	H3DG_CUDA_TRY(disc->seg_p1n.upload(p1n));
+	H3DG_CUDA_TRY(disc->seg_p2n.upload(p2n));
+	if (disc->seg_ctr.n != (size_t) (2 + 2 * nwin + 4)) H3DG_CUDA_TRY(disc->seg_ctr.alloc(2 + 2 * nwin + 4));
+	if (disc->seg_ring.n < ring) H3DG_CUDA_TRY(disc->seg_ring.alloc(ring));
+	disc->seg_ctas = ctas;
+	disc->seg_per_item = k.per_item;
+	disc->seg_nitems = (int) (items.size() / 4);
+	disc->seg_ring_win = ring_win;
+	return H3DG_OK;
+}
+
+static h3dg_status seg_launch(h3dg_disc *disc, SegSpec &k, const h3dg::KArgs &a, double *d_Ax, double *d_rhs, cudaStream_t st) {
+	const h3dg::Plan &P = disc->plan;
+	if (!d_Ax && !(d_rhs && disc->lf)) {
+		if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
+		return H3DG_OK;
+	}
+	// DOFs without a column of this plan (another part's, or no linear form): zero
+	if (d_rhs && (!disc->lf || !disc->seg_all_dofs)) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
+	H3DG_CUDA_TRY(cudaMemsetAsync(disc->seg_ctr.p, 0, sizeof(unsigned) * disc->seg_ctr.n, st));
+	h3dg::SegArgs g;
+	g.kof = disc->seg_kof.p;
+	g.items = disc->seg_items.p;
+	g.nitems = disc->seg_nitems;
+	g.col = disc->seg_col.p;
+	g.cptr = disc->seg_cptr.p;
+	g.pe = disc->seg_pe.p;
+	g.plm = disc->seg_plm.p;
+	g.off = disc->seg_off.p;
+	g.p1n = disc->seg_p1n.p;
+	g.p2n = disc->seg_p2n.p;
+	g.ctr = disc->seg_ctr.p;
+	g.nwin = P.seg_nwin;
+	g.ring_win = disc->seg_ring_win;
+	g.span = P.seg_span;
+	g.ring_slots = disc->seg_ring_win * P.seg_window;
+	g.ring = disc->seg_ring.p;
+	g.colcap = seg_colcap(P);
+	k.fn<<<(unsigned) disc->seg_ctas, k.threads, k.smem(g.colcap), st>>>(a, g);
+	H3DG_CUDA_TRY(cudaGetLastError());
+	return H3DG_OK;
+}
+
 static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream) {
 	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "assemble: create_pattern() first");
 	if (precision != H3DG_PREC_FP64 && precision != H3DG_PREC_TF32X3 && precision != H3DG_PREC_OZAKI)
@@ -1173,11 +1309,11 @@ static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax,
 		H3DG_CUDA_TRY(cudaSetDevice(disc->device));
 		return assemble_ho(disc, precision, d_Ax, d_rhs, (cudaStream_t) stream);
 	}
-	std::vector<int> cands;
-	for (size_t i = 0; i < kernel_table().size(); i++)
-		if (kernel_table()[i].p == P.px && kernel_table()[i].nq == P.nqx) cands.push_back((int) i);
-	const KernelSpec *ks = cands.empty() ? nullptr : &kernel_table()[cands[0]];
-	if (!ks) return fail(H3DG_ERR_INVALID_ARG, "assemble: no FP64 kernel instantiated for this order / rule");
+	// candidates: colour-sweep kernels (index into kernel_table) and, where
+	// the plan has its tables, segmented-scatter kernels (kSegVariant + index
+	// into seg_table); all give the same bits
+	const std::vector<int> cands = lo_candidates(disc);
+	if (cands.empty()) return fail(H3DG_ERR_INVALID_ARG, "assemble: no FP64 kernel instantiated for this order / rule");
 	{
 		h3dg_status s0 = ensure_device(disc);
 		if (s0 != H3DG_OK) return s0;
@@ -1206,21 +1342,25 @@ static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax,
 	a.rhs = disc->lf ? d_rhs : nullptr;
 	a.status = disc->status.p;
 	a.wait_limit = h3dg::kWaitPolls;
-	if (d_Ax) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
-	if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
 	int nsm = 148;
 	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
-	auto prepare = [&](KernelSpec &k, int &grid_per_sm) -> h3dg_status {
+	// one assembly with candidate ci; returns launches, or -1 on a CUDA error
+	auto run = [&](int ci) -> int32_t {
+		if (ci >= kSegVariant) {
+			SegSpec &k = seg_table()[ci - kSegVariant];
+			if (seg_prepare(disc, k, nsm) != H3DG_OK) return -1;
+			return seg_launch(disc, k, a, d_Ax, d_rhs, st) == H3DG_OK ? 1 : -1;
+		}
+		KernelSpec &k = kernel_table()[ci];
+		if (d_Ax && cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st) != cudaSuccess) return -1;
+		if (d_rhs && cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st) != cudaSuccess) return -1;
 		if (!k.configured) {
-			H3DG_CUDA_TRY(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) k.smem));
+			if (cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) k.smem) != cudaSuccess) return -1;
 			k.configured = true;
 		}
-		grid_per_sm = 1;
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&grid_per_sm, k.fn, k.threads, k.smem);
-		if (grid_per_sm < 1) grid_per_sm = 1;
-		return H3DG_OK;
-	};
-	auto sweep = [&](const KernelSpec &k, int per_sm) -> int32_t {
+		int per_sm = 1;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, k.smem);
+		if (per_sm < 1) per_sm = 1;
 		int32_t n = 0;
 		for (int c = 0; c < P.ncolors; c++) {
 			int64_t kb = P.color_ptr[c], ke = P.color_ptr[c + 1];
@@ -1230,12 +1370,11 @@ static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax,
 			k.fn<<<(unsigned) grid, k.threads, k.smem, st>>>(a, kb, ke);
 			n++;
 		}
-		return n;
+		return cudaGetLastError() == cudaSuccess ? n : -1;
 	};
-	// autotune once per plan: time one colour sweep of every variant (results are
-	// bitwise identical across variants; the outputs are re-zeroed afterwards)
+	// autotune once per plan: time one assembly with every candidate
 	// H3DG_FP64_VARIANT=i pins candidate i (profiling runs) and skips the timing pass
-	if (disc->variant < 0 && !cands.empty() && std::getenv("H3DG_FP64_VARIANT")) {
+	if (disc->variant < 0 && std::getenv("H3DG_FP64_VARIANT")) {
 		int v = std::atoi(std::getenv("H3DG_FP64_VARIANT"));
 		disc->variant = cands[(size_t) std::max(0, std::min(v, (int) cands.size() - 1))];
 	}
@@ -1246,12 +1385,9 @@ static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax,
 		float best = 1e30f;
 		int besti = cands[0];
 		for (int ci : cands) {
-			KernelSpec &k = kernel_table()[ci];
-			int per_sm;
-			if (prepare(k, per_sm) != H3DG_OK) continue;
-			sweep(k, per_sm);
+			if (run(ci) < 0) continue;
 			H3DG_CUDA_TRY(cudaEventRecord(e0, st));
-			for (int r = 0; r < 2; r++) sweep(k, per_sm);
+			for (int r = 0; r < 2; r++) run(ci);
 			H3DG_CUDA_TRY(cudaEventRecord(e1, st));
 			H3DG_CUDA_TRY(cudaEventSynchronize(e1));
 			float ms = 0;
@@ -1262,21 +1398,18 @@ static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax,
 		cudaEventDestroy(e1);
 		disc->variant = besti;
 		disc->variant_ms = best / 2;
-		if (d_Ax) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
-		if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
 	}
-	if (disc->variant >= 0) ks = &kernel_table()[disc->variant];
-	KernelSpec &K = *const_cast<KernelSpec *>(ks);
-	int per_sm = 1;
-	if (prepare(K, per_sm) != H3DG_OK) return H3DG_ERR_CUDA;
-	int32_t launches = 0;
+	const int ci = disc->variant >= 0 ? disc->variant : cands[0];
 	// test hook: the table-staging wait of this assembly gives up at once
 	if (disc->debug_once == H3DG_DEBUG_WAIT_GIVES_UP) a.wait_limit = 0;
 	disc->debug_once = 0;
 	const bool rec = disc->tn < disc->tcap;
 	if (rec) H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn], st));
-	launches = sweep(K, per_sm);
-	H3DG_CUDA_TRY(cudaGetLastError());
+	const int32_t launches = run(ci);
+	if (launches < 0) {
+		cudaError_t e = cudaGetLastError();
+		return fail(H3DG_ERR_CUDA, std::string("assemble: launch failed: ") + cudaGetErrorString(e));
+	}
 	if (rec) {
 		H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn + 1], st));
 		disc->tn++;
@@ -1359,10 +1492,39 @@ h3dg_status h3dg_tc_selftest(int kind, const float *d_A, const float *d_B, float
 
 h3dg_status h3dg_disc_get_tuning(const h3dg_disc *disc, int32_t *threads, int32_t *elems_per_cta, float *ms) {
 	if (!disc) return fail(H3DG_ERR_INVALID_ARG, "get_tuning: null disc");
-	const KernelSpec *k = disc->variant >= 0 ? &kernel_table()[disc->variant] : nullptr;
-	if (threads) *threads = k ? k->threads : -1;
-	if (elems_per_cta) *elems_per_cta = k ? k->eb : -1;
+	int t = -1, eb = -1;
+	if (disc->variant >= kSegVariant) {
+		t = seg_table()[disc->variant - kSegVariant].threads;
+		eb = seg_table()[disc->variant - kSegVariant].eb;
+	}
+	else if (disc->variant >= 0) {
+		t = kernel_table()[disc->variant].threads;
+		eb = kernel_table()[disc->variant].eb;
+	}
+	if (threads) *threads = t;
+	if (elems_per_cta) *elems_per_cta = eb;
 	if (ms) *ms = disc->variant_ms;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_seg_stats(const h3dg_disc *disc, int64_t *out) {
+	if (!disc || !out) return fail(H3DG_ERR_INVALID_ARG, "seg_stats: bad arguments");
+	for (int i = 0; i < 8; i++) out[i] = 0;
+	if (!disc->seg_ctr.p) return H3DG_OK;
+	unsigned w[4];
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	H3DG_CUDA_TRY(cudaMemcpy(w, disc->seg_ctr.p + disc->seg_ctr.n - 4, sizeof(w), cudaMemcpyDeviceToHost));
+	for (int i = 0; i < 4; i++) out[i] = w[i];
+	out[4] = disc->seg_nitems;
+	out[5] = disc->seg_ring_win;
+	out[6] = disc->seg_ctas;
+	out[7] = disc->plan.seg_span;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_tuned_scatter(const h3dg_disc *disc, int32_t *segmented) {
+	if (!disc || !segmented) return fail(H3DG_ERR_INVALID_ARG, "tuned_scatter: bad arguments");
+	*segmented = disc->variant < 0 ? -1 : disc->variant >= kSegVariant ? 1 : 0;
 	return H3DG_OK;
 }
 
@@ -1468,10 +1630,7 @@ h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, doub
 		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: kernel variants not tuned yet; make one allocating assembly "
 		                            "call first");
 	if (!P.mixed && !P.canon && disc->variant < 0) {
-		int ncand = 0;
-		for (size_t i = 0; i < kernel_table().size(); i++)
-			if (kernel_table()[i].p == P.px && kernel_table()[i].nq == P.nqx) ncand++;
-		if (ncand > 1)
+		if (lo_candidates(disc).size() > 1)
 			return fail(H3DG_ERR_STATE, "assemble_host_noalloc: kernel variant not tuned yet; make one allocating assembly "
 			                            "call first");
 	}
@@ -1537,11 +1696,23 @@ h3dg_status h3dg_disc_debug_inject(h3dg_disc *disc, int what) {
 	if (P.mixed || P.canon) return fail(H3DG_ERR_INVALID_ARG, "debug_inject: position hook needs a low-order plan");
 	{ h3dg_status s0 = ensure_device(disc); if (s0 != H3DG_OK) return s0; }
 	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
-	// entry (a = 0, b = 0) of the first element with a matrix entry
+	// entry (a = 0, b = 0) of the first element with a matrix entry, in the
+	// colour sweeps' map and in the segmented scatter's pair of that column
 	for (int64_t k = 0; k < P.ne; k++)
 		if (P.el_cnt[2 * k] > 0) {
 			const uint16_t bad = 0xFFFF;
 			H3DG_CUDA_TRY(cudaMemcpy(disc->el_off.p + (size_t) k * P.nl * P.nl, &bad, sizeof(bad), cudaMemcpyHostToDevice));
+			if (P.seg) {
+				const int32_t d = P.el_dof[(size_t) k * P.nl];
+				int32_t e = -1;
+				for (int64_t i = 0; i < P.ne && e < 0; i++)
+					if (P.seg_kof[i] == k) e = (int32_t) i;
+				for (size_t j = 0; j < P.seg_col.size(); j++)
+					if (P.seg_col[j] == d)
+						for (int64_t t = P.seg_cptr[j]; t < P.seg_cptr[j + 1]; t++)
+							if (P.seg_pe[t] == e && (P.seg_plm[t] & 0xff) == 0)
+								H3DG_CUDA_TRY(cudaMemcpy(disc->seg_off.p + (size_t) t * P.nl, &bad, sizeof(bad), cudaMemcpyHostToDevice));
+			}
 			return H3DG_OK;
 		}
 	return fail(H3DG_ERR_INVALID_ARG, "debug_inject: the plan has no matrix entry");

@@ -1254,6 +1254,8 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 	}
 
 	// tables in assembly (colour-major) order
+	P.seg_kof.resize(ne);
+	for (int64_t k = 0; k < ne; k++) P.seg_kof[order_[k]] = (int32_t) k;
 	P.el_vtx.resize(8 * ne);
 	P.el_cnt.resize(2 * ne);
 	P.el_s.resize((size_t) ne * nl);
@@ -1283,7 +1285,117 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 			}
 		}
 	});
+	if (P.px <= kSegMaxOrder && P.py <= kSegMaxOrder && P.pz <= kSegMaxOrder) build_seg_tables(P, kSegWindow);
 	return 0;
+}
+
+// Tables of the segmented scatter (see Plan::seg).  Needs the colour-major
+// element tables and seg_kof.
+void build_seg_tables(Plan &P, int window) {
+	const int64_t ne = P.ne, nd = P.ndof;
+	const int nl = P.nl;
+	P.seg = true;
+	P.seg_window = window;
+	P.seg_nwin = (int) ((ne + window - 1) / window);
+	std::vector<int64_t> elem_of_k(ne);
+	for (int64_t e = 0; e < ne; e++) elem_of_k[P.seg_kof[e]] = e;
+	// pairs of every column in assembly order (k ascending)
+	std::vector<int64_t> nptr(nd + 1, 0);
+	for (int64_t k = 0; k < ne; k++)
+		for (int b = 0; b < P.el_cnt[2 * k]; b++) nptr[P.el_dof[(size_t) k * nl + b] + 1]++;
+	for (int64_t d = 0; d < nd; d++) nptr[d + 1] += nptr[d];
+	const int64_t npairs = nptr[nd];
+	std::vector<int64_t> pk(npairs);
+	std::vector<uint8_t> plb(npairs);
+	{
+		std::vector<int64_t> fill(nptr.begin(), nptr.end() - 1);
+		for (int64_t k = 0; k < ne; k++)
+			for (int b = 0; b < P.el_cnt[2 * k]; b++) {
+				const int64_t t = fill[P.el_dof[(size_t) k * nl + b]]++;
+				pk[t] = k;
+				plb[t] = (uint8_t) b;
+			}
+	}
+	// first and ready window of every column; processing order by ready window
+	std::vector<int32_t> first(nd, 0), ready(nd, -1);
+	int span = 0;
+	for (int64_t d = 0; d < nd; d++) {
+		if (nptr[d + 1] == nptr[d]) continue;
+		int64_t lo = ne, hi = -1;
+		for (int64_t t = nptr[d]; t < nptr[d + 1]; t++) {
+			const int64_t e = elem_of_k[pk[t]];
+			lo = std::min(lo, e);
+			hi = std::max(hi, e);
+		}
+		first[d] = (int32_t) (lo / window);
+		ready[d] = (int32_t) (hi / window);
+		span = std::max(span, ready[d] - first[d]);
+	}
+	P.seg_span = span;
+	int maxcol = 0;
+	for (int64_t d = 0; d < nd; d++) maxcol = std::max<int64_t>(maxcol, P.Ap[d + 1] - P.Ap[d]);
+	P.seg_maxcol = maxcol;
+	std::vector<int64_t> wptr(P.seg_nwin + 1, 0);
+	for (int64_t d = 0; d < nd; d++)
+		if (ready[d] >= 0) wptr[ready[d] + 1]++;
+	for (int w = 0; w < P.seg_nwin; w++) wptr[w + 1] += wptr[w];
+	const int64_t ncol = wptr[P.seg_nwin];
+	P.seg_col.resize(ncol);
+	{
+		std::vector<int64_t> fill(wptr.begin(), wptr.end() - 1);
+		for (int64_t d = 0; d < nd; d++)
+			if (ready[d] >= 0) P.seg_col[fill[ready[d]]++] = (int32_t) d;
+	}
+	P.seg_cptr.assign(ncol + 1, 0);
+	for (int64_t j = 0; j < ncol; j++) P.seg_cptr[j + 1] = P.seg_cptr[j] + (nptr[P.seg_col[j] + 1] - nptr[P.seg_col[j]]);
+	P.seg_pe.resize(npairs);
+	P.seg_plm.resize(npairs);
+	// row positions, padded at the end so a 16-byte-rounded bulk copy of the
+	// last batch stays inside the array
+	P.seg_off.assign((size_t) npairs * nl + 16, 0);
+	parallel_for(ncol, [&](int64_t lo, int64_t hi) {
+		for (int64_t j = lo; j < hi; j++) {
+			const int64_t d = P.seg_col[j];
+			for (int64_t u = 0; u < nptr[d + 1] - nptr[d]; u++) {
+				const int64_t s = nptr[d] + u, t = P.seg_cptr[j] + u;
+				const int64_t k = pk[s];
+				const int lb = plb[s], m = P.el_cnt[2 * k];
+				P.seg_pe[t] = (int32_t) elem_of_k[k];
+				P.seg_plm[t] = (uint16_t) (lb | (m << 8));
+				std::copy(&P.el_off[((size_t) k * nl + lb) * nl], &P.el_off[((size_t) k * nl + lb) * nl] + m,
+				          &P.seg_off[(size_t) t * nl]);
+			}
+		}
+	});
+	// column batches: consecutive columns of one ready window, at most
+	// kSegBatchCols columns and seg_batch_pairs(nl) pairs
+	P.seg_p2.clear();
+	P.seg_p2ptr.assign(P.seg_nwin + 1, 0);
+	for (int w = 0; w < P.seg_nwin; w++) {
+		int64_t j = wptr[w];
+		while (j < wptr[w + 1]) {
+			int64_t j1 = j + 1;
+			int lo = first[P.seg_col[j]];
+			while (j1 < wptr[w + 1] && j1 - j < kSegBatchCols &&
+			       P.seg_cptr[j1 + 1] - P.seg_cptr[j] <= seg_batch_pairs(nl)) {
+				lo = std::min(lo, first[P.seg_col[j1]]);
+				j1++;
+			}
+			P.seg_p2.insert(P.seg_p2.end(), { w, lo, (int32_t) j, (int32_t) j1 });
+			j = j1;
+		}
+		P.seg_p2ptr[w + 1] = (int64_t) P.seg_p2.size() / 4;
+	}
+	// a column whose pairs exceed one batch's staging area: colour sweeps only
+	for (int64_t j = 0; j < ncol; j++)
+		if (P.seg_cptr[j + 1] - P.seg_cptr[j] > seg_batch_pairs(nl)) {
+			P.seg = false;
+			break;
+		}
+	if (!P.seg) {
+		P.seg_col.clear(); P.seg_cptr.clear(); P.seg_pe.clear(); P.seg_plm.clear(); P.seg_off.clear();
+		P.seg_p2.clear(); P.seg_p2ptr.clear();
+	}
 }
 
 // Mixed orders.  Same pattern rule as build_plan (the CSC pattern does not

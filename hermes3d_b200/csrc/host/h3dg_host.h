@@ -180,6 +180,29 @@ struct Plan {
 	int ncolors = 0;
 	std::vector<int64_t> color_ptr;          // ncolors + 1 (ranges in assembly order)
 
+	// Segmented scatter (uniform low orders).  The element matrices are
+	// computed in element order (plan element index, ascending mesh id) into
+	// a ring of slots in global memory; every CSC column is then summed from
+	// the matrices of its elements, in assembly order (colour, then element:
+	// the order in which the colour sweeps add), and written once.  Elements
+	// are grouped in windows of seg_window; a column is "ready" in the window
+	// of its last element and is processed after that window.  Pairs (column,
+	// element) carry the element's local index of the column's DOF and the
+	// row positions of the element's DOFs inside the column.
+	bool seg = false;
+	int seg_window = 0;                      // elements per window
+	int seg_nwin = 0;                        // windows
+	int seg_span = 0;                        // max over columns: ready window - first window
+	int seg_maxcol = 0;                      // longest column (rows)
+	std::vector<int32_t> seg_kof;            // ne: plan element -> assembly index k
+	std::vector<int32_t> seg_col;            // columns in processing order: DOF
+	std::vector<int64_t> seg_cptr;           // columns + 1: pair ranges
+	std::vector<int32_t> seg_pe;             // per pair: plan element
+	std::vector<uint16_t> seg_plm;           // per pair: local index of the DOF | matrix entries << 8
+	std::vector<uint16_t> seg_off;           // per pair x nl: row position of the element's row a (a < m)
+	std::vector<int32_t> seg_p2;             // column batches, 4 ints each: ready window, first window, begin, end
+	std::vector<int64_t> seg_p2ptr;          // seg_nwin + 1: column batches per ready window
+
 	// 1D tables (b): per direction, V[k][q] and D[k][q] (k <= p, q < nq) and rule
 	std::vector<double> qx, wx, qy, wy, qz, wz;
 
@@ -281,6 +304,14 @@ struct PlanScope {
 	int64_t nslab = 0, nhalo = 0, nowned = 0;
 };
 int make_partition_scope(const Space &sp, int nparts, int part, PlanScope &scope, std::string &err);
+
+// segmented scatter: orders it is built for, elements per window, and the
+// bounds of one column batch (columns, pairs: the staging area of a batch)
+constexpr int kSegMaxOrder = 3;
+constexpr int kSegWindow = 256;
+constexpr int kSegBatchCols = 32;
+constexpr int seg_batch_pairs(int nl) { return nl <= 27 ? 128 : 64; }
+void build_seg_tables(Plan &plan, int window);
 
 int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &plan, std::string &err, bool canon = false,
                const PlanScope *scope = nullptr);

@@ -17,6 +17,7 @@
 #include "kernels/asm_fp64_ced.cuh"
 #include "kernels/asm_surface.cuh"
 #include "kernels/norms.cuh"
+#include "kernels/asm_fp64_seg.cuh"
 
 namespace h3dg_tables {
 
@@ -110,5 +111,22 @@ using NormReduceFn = void (*)(const double *, int64_t, double *);
 NormFn norm_fn();
 NormReduceFn norm_reduce_fn();
 constexpr int kNormThreads = 128;
+
+
+
+// segmented-scatter FP64 kernels (uniform orders p <= 3): one persistent
+// launch per assembly
+using SegFn = void (*)(h3dg::KArgs, h3dg::SegArgs);
+
+struct SegSpec {
+	int p, nq;
+	SegFn fn;
+	int threads, eb;
+	int per_item;                 // elements per element item
+	size_t (*smem)(int colcap);
+	bool configured;
+	size_t configured_smem;
+};
+std::vector<SegSpec> &seg_table();
 
 } // namespace h3dg_tables

@@ -46,6 +46,7 @@ struct SfShape {
 	static constexpr int NX = PX + 1, NY = PY + 1, NZ = PZ + 1;
 	static constexpr int NL = NX * NY * NZ;
 	static constexpr int NQ = NQX * NQY * NQZ;
+	static constexpr int NQ1X = NQX, NQ1Y = NQY, NQ1Z = NQZ;
 	static constexpr int NT_TERMS = 6;   // stage-1 products (zz and mass share one)
 	// 1D tables blob: Vx Dx Vy Dy Vz Dz (k-major, q fastest) then q/w per direction
 	static constexpr int OVX = 0, ODX = OVX + NX * NQX, OVY = ODX + NX * NQX, ODY = OVY + NY * NQY;
@@ -94,30 +95,17 @@ static __device__ __constant__ int kT1Flags[6][3] = {
 	{ 3, 0, 0 }, { 0, 3, 0 }, { 0, 0, 3 }, { 2, 1, 0 }, { 2, 0, 1 }, { 0, 2, 1 }
 };
 
-// PF: software prefetch.  The plan data of the CTA's next batch (position
-// map, DOFs, coefficients, shape indices, column bounds, vertex coordinates)
-// are loaded into registers while the current batch is being computed, so
-// their global-memory latency overlaps the arithmetic; the arithmetic itself
-// is unchanged (bitwise identical results).
-template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ, int NT, int EB, int MINB, bool PF = false>
-__global__ void __launch_bounds__(NT, MINB) k_assemble_fp64(KArgs args, int64_t kbeg, int64_t kend) {
-	using S = SfShape<PX, PY, PZ, NQX, NQY, NQZ, EB>;
-	constexpr int NX = S::NX, NY = S::NY, NZ = S::NZ, NL = S::NL, NQ = S::NQ;
-	constexpr int NL2 = NL * NL;
-	constexpr int COLS = S::COLS;
-	constexpr int CH = 4;   // scatter chunk per thread
-	extern __shared__ __align__(128) double sm[];
-	__shared__ uint64_t bar;
-	__shared__ int s_m[EB], s_l[EB];
-	__shared__ double s_cg[EB];
-	double *tab = sm + S::S_TAB;
-	double *Wx = sm + S::S_W, *Wy = Wx + S::WX, *Wz = Wy + S::WY;
-	double *E0 = sm + S::S_E;
+// ---- phases of the element computation, shared by the colour-sweep kernel
+// below and the segmented-scatter kernel (asm_fp64_seg.cuh).  Each works on
+// the EB element areas of a batch (layout of SfShape) with NT threads; the
+// caller puts a block barrier between consecutive phases.
+
+// 1D product tables W^f[k][k'][q], once per CTA
+template <class S, int NT>
+__device__ __forceinline__ void sf_product_tables(const double *tab, double *Wx, double *Wy, double *Wz) {
+	constexpr int NX = S::NX, NY = S::NY, NZ = S::NZ;
+	constexpr int NQX = S::NQ1X, NQY = S::NQ1Y, NQZ = S::NQ1Z;
 	const int tid = threadIdx.x;
-
-	if (!stage_tables(tab, args.tables, args.table_bytes, &bar, args.status, args.wait_limit)) return;
-
-	// 1D product tables, once per CTA
 	for (int i = tid; i < S::WX; i += NT) {
 		int q = i % NQX, kk = (i / NQX) % NX, k = (i / (NQX * NX)) % NX, f = i / (NQX * NX * NX);
 		double e0 = (f >> 1) ? tab[S::ODX + k * NQX + q] : tab[S::OVX + k * NQX + q];
@@ -136,6 +124,246 @@ __global__ void __launch_bounds__(NT, MINB) k_assemble_fp64(KArgs args, int64_t 
 		double e1 = (f & 1) ? tab[S::ODZ + kk * NQZ + q] : tab[S::OVZ + kk * NQZ + q];
 		Wz[i] = e0 * e1;
 	}
+}
+
+// trilinear map as monomials: x_r = sum_m c_m[r] mono_m(xi, eta, zeta),
+// mono = 1, xi, eta, zeta, xi eta, xi zeta, eta zeta, xi eta zeta;
+// c_m = (1/8) sum_v X_v prod_{d in m} s_d(v), s_d(v) = +-1 the vertex's
+// reference coordinate (src/refdomain.cc:96-105)
+template <class S, int NT, int EB>
+__device__ __forceinline__ void sf_monomials(double *E0) {
+	for (int i = threadIdx.x; i < EB * 24; i += NT) {
+		const int e = i / 24, mr = i % 24, mo = mr / 3, r = mr % 3;
+		double *Eb = E0 + e * S::E_SIZE;
+		const int usex = mo == 1 || mo == 4 || mo == 5 || mo == 7;
+		const int usey = mo == 2 || mo == 4 || mo == 6 || mo == 7;
+		const int usez = mo == 3 || mo == 5 || mo == 6 || mo == 7;
+		double c = 0.0;
+#pragma unroll
+		for (int v = 0; v < 8; v++) {
+			const int bx = ((v + 1) >> 1) & 1, by = (v >> 1) & 1, bz = v >> 2;
+			const int neg = (usex && !bx) ^ (usey && !by) ^ (usez && !bz);
+			const double xv = Eb[S::E_X + 3 * v + r];
+			c += neg ? -xv : xv;
+		}
+		Eb[S::E_M + mr] = 0.125 * c;
+	}
+}
+
+// geometry at the quadrature points -> term weights.  Jacobian, signed
+// determinant and inverse as in RefMap::calc_inv_ref_map
+// (src/refmap.cc:177-231); G = w det J^-1 J^-T = (w / det) adj(J) adj(J)^T.
+template <class S, int NT, int EB>
+__device__ __forceinline__ void sf_geometry(const double *tab, double *E0, const double *s_cg, int lf, double lf_value) {
+	constexpr int NQY = S::NQ1Y, NQZ = S::NQ1Z, NQ = S::NQ;
+	for (int i = threadIdx.x; i < EB * NQ; i += NT) {
+		const int e = i / NQ, q = i % NQ;
+		double *Eb = E0 + e * S::E_SIZE;
+		double *G = Eb + S::E_G;
+		const double *cm = Eb + S::E_M;
+		const int q1 = q / (NQY * NQZ), q2 = (q / NQZ) % NQY, q3 = q % NQZ;
+		const double x = tab[S::OQX + q1], y = tab[S::OQY + q2], z = tab[S::OQZ + q3];
+		const double xy = x * y, xz = x * z, yz = y * z, xyz = xy * z;
+		double m[3][3], xp[3];
+#pragma unroll
+		for (int r = 0; r < 3; r++) {
+			const double c0 = cm[r], c1 = cm[3 + r], c2 = cm[6 + r], c3 = cm[9 + r];
+			const double c4 = cm[12 + r], c5 = cm[15 + r], c6 = cm[18 + r], c7 = cm[21 + r];
+			m[r][0] = c1 + c4 * y + c5 * z + c7 * yz;
+			m[r][1] = c2 + c4 * x + c6 * z + c7 * xz;
+			m[r][2] = c3 + c5 * x + c6 * y + c7 * xy;
+			xp[r] = c0 + c1 * x + c2 * y + c3 * z + c4 * xy + c5 * xz + c6 * yz + c7 * xyz;
+		}
+		// cofactors: adj(J)[c][k] = C[k][c]; J^-1 = adj(J) / det
+		const double C00 = m[1][1] * m[2][2] - m[1][2] * m[2][1];
+		const double C01 = m[1][2] * m[2][0] - m[1][0] * m[2][2];
+		const double C02 = m[1][0] * m[2][1] - m[1][1] * m[2][0];
+		const double C10 = m[0][2] * m[2][1] - m[0][1] * m[2][2];
+		const double C11 = m[0][0] * m[2][2] - m[0][2] * m[2][0];
+		const double C12 = m[0][1] * m[2][0] - m[0][0] * m[2][1];
+		const double C20 = m[0][1] * m[1][2] - m[0][2] * m[1][1];
+		const double C21 = m[0][2] * m[1][0] - m[0][0] * m[1][2];
+		const double C22 = m[0][0] * m[1][1] - m[0][1] * m[1][0];
+		const double det = m[0][0] * C00 + m[0][1] * C01 + m[0][2] * C02;
+		const double w = tab[S::OWX + q1] * tab[S::OWY + q2] * tab[S::OWZ + q3];
+		const double wd = w * det;
+		const double s = w * s_cg[e] / det;
+		// (J^-1)[c][k] = C[k][c] / det  =>  G[c][d] = sum_k C[k][c] C[k][d] / det^2
+		G[0 * NQ + q] = 0.5 * s * (C00 * C00 + C10 * C10 + C20 * C20);
+		G[1 * NQ + q] = 0.5 * s * (C01 * C01 + C11 * C11 + C21 * C21);
+		G[2 * NQ + q] = 0.5 * s * (C02 * C02 + C12 * C12 + C22 * C22);
+		G[3 * NQ + q] = s * (C00 * C01 + C10 * C11 + C20 * C21);
+		G[4 * NQ + q] = s * (C00 * C02 + C10 * C12 + C20 * C22);
+		G[5 * NQ + q] = s * (C01 * C02 + C11 * C12 + C21 * C22);
+		G[6 * NQ + q] = 0.5 * wd;
+		G[7 * NQ + q] = wd * source_value(lf, lf_value, xp);
+	}
+}
+
+// element load vectors F_i = sum_q (w det f)(q) phi_i(q), by sum
+// factorisation: thread (e, a, b) contracts q3, then q2, then q1 for all c
+template <class S, int NT, int EB>
+__device__ __forceinline__ void sf_load_vector(const double *tab, double *E0) {
+	constexpr int NX = S::NX, NY = S::NY, NZ = S::NZ;
+	constexpr int NQX = S::NQ1X, NQY = S::NQ1Y, NQZ = S::NQ1Z, NQ = S::NQ;
+	for (int i = threadIdx.x; i < EB * NX * NY; i += NT) {
+		const int e = i / (NX * NY), ab = i % (NX * NY), a = ab / NY, b = ab % NY;
+		double *Eb = E0 + e * S::E_SIZE;
+		const double *src = Eb + S::E_G + 7 * NQ;
+		double fc[NZ];
+#pragma unroll
+		for (int c = 0; c < NZ; c++) fc[c] = 0.0;
+		for (int q1 = 0; q1 < NQX; q1++) {
+			double s1[NZ];
+#pragma unroll
+			for (int c = 0; c < NZ; c++) s1[c] = 0.0;
+			for (int q2 = 0; q2 < NQY; q2++) {
+				const double vy = tab[S::OVY + b * NQY + q2];
+#pragma unroll
+				for (int q3 = 0; q3 < NQZ; q3++) {
+					const double w = src[(q1 * NQY + q2) * NQZ + q3] * vy;
+#pragma unroll
+					for (int c = 0; c < NZ; c++) s1[c] += w * tab[S::OVZ + c * NQZ + q3];
+				}
+			}
+			const double vx = tab[S::OVX + a * NQX + q1];
+#pragma unroll
+			for (int c = 0; c < NZ; c++) fc[c] += vx * s1[c];
+		}
+#pragma unroll
+		for (int c = 0; c < NZ; c++) Eb[S::E_F + ab * NZ + c] = fc[c];
+	}
+}
+
+// stage 1: item (e, k, q1, q2) produces T1_k[q1][q2][*][*]
+//   k: 0 xx, 1 yy, 2 zz (+ mass), 3 xy, 4 xz, 5 yz
+template <class S, int NT, int EB>
+__device__ __forceinline__ void sf_stage1(double *E0, const double *Wz, int mass) {
+	constexpr int NZ = S::NZ;
+	constexpr int NQX = S::NQ1X, NQY = S::NQ1Y, NQZ = S::NQ1Z, NQ = S::NQ;
+	for (int i = threadIdx.x; i < EB * 6 * NQX * NQY; i += NT) {
+		const int e = i / (6 * NQX * NQY), r = i % (6 * NQX * NQY);
+		const int kk = r / (NQX * NQY), q12 = r % (NQX * NQY);
+		double *Eb = E0 + e * S::E_SIZE;
+		const double *gp = Eb + S::E_G + kk * NQ + q12 * NQZ;
+		const double *wz = Wz + kT1Flags[kk][2] * NZ * NZ * NQZ;
+		double g[NQZ];
+#pragma unroll
+		for (int q3 = 0; q3 < NQZ; q3++) g[q3] = gp[q3];
+		double *out = Eb + S::E_T1 + kk * S::T1N + q12 * NZ * NZ;
+		if (kk == 2 && mass) {
+			const double *gm = Eb + S::E_G + 6 * NQ + q12 * NQZ;
+			const double *wz0 = Wz;
+			double h[NQZ];
+#pragma unroll
+			for (int q3 = 0; q3 < NQZ; q3++) h[q3] = gm[q3];
+#pragma unroll
+			for (int cc = 0; cc < NZ * NZ; cc++) {
+				double s = 0.0;
+#pragma unroll
+				for (int q3 = 0; q3 < NQZ; q3++) s += g[q3] * wz[cc * NQZ + q3] + h[q3] * wz0[cc * NQZ + q3];
+				out[cc] = s;
+			}
+		}
+		else {
+#pragma unroll
+			for (int cc = 0; cc < NZ * NZ; cc++) {
+				double s = 0.0;
+#pragma unroll
+				for (int q3 = 0; q3 < NQZ; q3++) s += g[q3] * wz[cc * NQZ + q3];
+				out[cc] = s;
+			}
+		}
+	}
+}
+
+// stages 2+3: thread owns column (e, b, b', c, c'); it accumulates the
+// stage-2 values of the 3 x-classes in registers,
+//   V_f[q1] = sum_k(class f) sum_q2 Wy_k[b][b'][q2] T1_k[q1][q2][c][c'],
+// then A[(a,b,c)][(a',b',c')] = sum_f sum_q1 Wx_f[a][a'][q1] V_f[q1], which
+// overwrites the element's G / T1 area (block barrier in between).
+template <class S, int NT, int EB>
+__device__ __forceinline__ void sf_stage23(double *E0, const double *Wx, const double *Wy) {
+	constexpr int NX = S::NX, NY = S::NY, NZ = S::NZ, NL = S::NL;
+	constexpr int NQX = S::NQ1X, NQY = S::NQ1Y;
+	constexpr int COLS = S::COLS;
+	static_assert(EB * COLS <= NT, "one stage-3 column per thread");
+	const int tid = threadIdx.x;
+	const int e = tid / COLS, col = tid % COLS;
+	const bool active = tid < EB * COLS;
+	double acc[NX * NX];
+	const int bb = col / (NZ * NZ), cc = col % (NZ * NZ);
+	if (active) {
+		const double *Eb = E0 + e * S::E_SIZE;
+		double V[3][NQX];
+#pragma unroll
+		for (int f = 0; f < 3; f++)
+#pragma unroll
+			for (int q1 = 0; q1 < NQX; q1++) V[f][q1] = 0.0;
+#pragma unroll
+		for (int kk = 0; kk < 6; kk++) {
+			// compile-time after unrolling, so V stays in registers
+			constexpr int kFy[6] = { 0, 3, 0, 1, 0, 2 };
+			constexpr int kCls[6] = { 2, 0, 0, 1, 1, 0 };
+			const double *wy = Wy + kFy[kk] * NY * NY * NQY + bb * NQY;
+			const double *t1 = Eb + S::E_T1 + kk * S::T1N + cc;
+			const int f = kCls[kk];
+			double wyr[NQY];
+#pragma unroll
+			for (int q2 = 0; q2 < NQY; q2++) wyr[q2] = wy[q2];
+#pragma unroll
+			for (int q1 = 0; q1 < NQX; q1++) {
+				double s2 = V[f][q1];
+#pragma unroll
+				for (int q2 = 0; q2 < NQY; q2++) s2 += wyr[q2] * t1[(q1 * NQY + q2) * NZ * NZ];
+				V[f][q1] = s2;
+			}
+		}
+		const double *wx0 = Wx, *wx2 = Wx + 2 * NX * NX * NQX, *wx3 = Wx + 3 * NX * NX * NQX;
+#pragma unroll
+		for (int r = 0; r < NX * NX; r++) {
+			double s3 = 0.0;
+#pragma unroll
+			for (int q1 = 0; q1 < NQX; q1++)
+				s3 += wx0[r * NQX + q1] * V[0][q1] + wx2[r * NQX + q1] * V[1][q1] + wx3[r * NQX + q1] * V[2][q1];
+			acc[r] = s3;
+		}
+	}
+	__syncthreads();   // T1 fully consumed: A may overwrite it
+	if (active) {
+		const int b = bb / NY, b2 = bb % NY, c = cc / NZ, c2 = cc % NZ;
+		double *A = E0 + e * S::E_SIZE + S::E_A;
+#pragma unroll
+		for (int a = 0; a < NX; a++)
+#pragma unroll
+			for (int a2 = 0; a2 < NX; a2++)
+				A[((a * NY + b) * NZ + c) * NL + (a2 * NY + b2) * NZ + c2] = acc[a * NX + a2];
+	}
+}
+
+// PF: software prefetch.  The plan data of the CTA's next batch (position
+// map, DOFs, coefficients, shape indices, column bounds, vertex coordinates)
+// are loaded into registers while the current batch is being computed, so
+// their global-memory latency overlaps the arithmetic; the arithmetic itself
+// is unchanged (bitwise identical results).
+template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ, int NT, int EB, int MINB, bool PF = false>
+__global__ void __launch_bounds__(NT, MINB) k_assemble_fp64(KArgs args, int64_t kbeg, int64_t kend) {
+	using S = SfShape<PX, PY, PZ, NQX, NQY, NQZ, EB>;
+	constexpr int NL = S::NL;
+	constexpr int NL2 = NL * NL;
+	constexpr int CH = 4;   // scatter chunk per thread
+	extern __shared__ __align__(128) double sm[];
+	__shared__ uint64_t bar;
+	__shared__ int s_m[EB], s_l[EB];
+	__shared__ double s_cg[EB];
+	double *tab = sm + S::S_TAB;
+	double *Wx = sm + S::S_W, *Wy = Wx + S::WX, *Wz = Wy + S::WY;
+	double *E0 = sm + S::S_E;
+	const int tid = threadIdx.x;
+
+	if (!stage_tables(tab, args.tables, args.table_bytes, &bar, args.status, args.wait_limit)) return;
+
+	sf_product_tables<S, NT>(tab, Wx, Wy, Wz);
 	__syncthreads();
 
 	const bool do_rhs = args.rhs && args.lf;
@@ -262,202 +490,15 @@ __global__ void __launch_bounds__(NT, MINB) k_assemble_fp64(KArgs args, int64_t 
 		}
 		__syncthreads();
 
-		// ---- trilinear map as monomials: x_r = sum_m c_m[r] mono_m(xi, eta, zeta),
-		// mono = 1, xi, eta, zeta, xi eta, xi zeta, eta zeta, xi eta zeta;
-		// c_m = (1/8) sum_v X_v prod_{d in m} s_d(v), s_d(v) = +-1 the vertex's
-		// reference coordinate (src/refdomain.cc:96-105)
-		for (int i = tid; i < EB * 24; i += NT) {
-			const int e = i / 24, mr = i % 24, mo = mr / 3, r = mr % 3;
-			double *Eb = E0 + e * S::E_SIZE;
-			const int usex = mo == 1 || mo == 4 || mo == 5 || mo == 7;
-			const int usey = mo == 2 || mo == 4 || mo == 6 || mo == 7;
-			const int usez = mo == 3 || mo == 5 || mo == 6 || mo == 7;
-			double c = 0.0;
-#pragma unroll
-			for (int v = 0; v < 8; v++) {
-				const int bx = ((v + 1) >> 1) & 1, by = (v >> 1) & 1, bz = v >> 2;
-				const int neg = (usex && !bx) ^ (usey && !by) ^ (usez && !bz);
-				const double xv = Eb[S::E_X + 3 * v + r];
-				c += neg ? -xv : xv;
-			}
-			Eb[S::E_M + mr] = 0.125 * c;
-		}
+		sf_monomials<S, NT, EB>(E0);
 		__syncthreads();
-
-		// ---- geometry at the quadrature points -> term weights.  Jacobian,
-		// signed determinant and inverse as in RefMap::calc_inv_ref_map
-		// (src/refmap.cc:177-231); G = w det J^-1 J^-T = (w / det) adj(J) adj(J)^T.
-		for (int i = tid; i < EB * NQ; i += NT) {
-			const int e = i / NQ, q = i % NQ;
-			double *Eb = E0 + e * S::E_SIZE;
-			double *G = Eb + S::E_G;
-			const double *cm = Eb + S::E_M;
-			const int q1 = q / (NQY * NQZ), q2 = (q / NQZ) % NQY, q3 = q % NQZ;
-			const double x = tab[S::OQX + q1], y = tab[S::OQY + q2], z = tab[S::OQZ + q3];
-			const double xy = x * y, xz = x * z, yz = y * z, xyz = xy * z;
-			double m[3][3], xp[3];
-#pragma unroll
-			for (int r = 0; r < 3; r++) {
-				const double c0 = cm[r], c1 = cm[3 + r], c2 = cm[6 + r], c3 = cm[9 + r];
-				const double c4 = cm[12 + r], c5 = cm[15 + r], c6 = cm[18 + r], c7 = cm[21 + r];
-				m[r][0] = c1 + c4 * y + c5 * z + c7 * yz;
-				m[r][1] = c2 + c4 * x + c6 * z + c7 * xz;
-				m[r][2] = c3 + c5 * x + c6 * y + c7 * xy;
-				xp[r] = c0 + c1 * x + c2 * y + c3 * z + c4 * xy + c5 * xz + c6 * yz + c7 * xyz;
-			}
-			// cofactors: adj(J)[c][k] = C[k][c]; J^-1 = adj(J) / det
-			const double C00 = m[1][1] * m[2][2] - m[1][2] * m[2][1];
-			const double C01 = m[1][2] * m[2][0] - m[1][0] * m[2][2];
-			const double C02 = m[1][0] * m[2][1] - m[1][1] * m[2][0];
-			const double C10 = m[0][2] * m[2][1] - m[0][1] * m[2][2];
-			const double C11 = m[0][0] * m[2][2] - m[0][2] * m[2][0];
-			const double C12 = m[0][1] * m[2][0] - m[0][0] * m[2][1];
-			const double C20 = m[0][1] * m[1][2] - m[0][2] * m[1][1];
-			const double C21 = m[0][2] * m[1][0] - m[0][0] * m[1][2];
-			const double C22 = m[0][0] * m[1][1] - m[0][1] * m[1][0];
-			const double det = m[0][0] * C00 + m[0][1] * C01 + m[0][2] * C02;
-			const double w = tab[S::OWX + q1] * tab[S::OWY + q2] * tab[S::OWZ + q3];
-			const double wd = w * det;
-			const double s = w * s_cg[e] / det;
-			// (J^-1)[c][k] = C[k][c] / det  =>  G[c][d] = sum_k C[k][c] C[k][d] / det^2
-			G[0 * NQ + q] = 0.5 * s * (C00 * C00 + C10 * C10 + C20 * C20);
-			G[1 * NQ + q] = 0.5 * s * (C01 * C01 + C11 * C11 + C21 * C21);
-			G[2 * NQ + q] = 0.5 * s * (C02 * C02 + C12 * C12 + C22 * C22);
-			G[3 * NQ + q] = s * (C00 * C01 + C10 * C11 + C20 * C21);
-			G[4 * NQ + q] = s * (C00 * C02 + C10 * C12 + C20 * C22);
-			G[5 * NQ + q] = s * (C01 * C02 + C11 * C12 + C21 * C22);
-			G[6 * NQ + q] = 0.5 * wd;
-			G[7 * NQ + q] = wd * source_value(args.lf, args.lf_value, xp);
-		}
+		sf_geometry<S, NT, EB>(tab, E0, s_cg, args.lf, args.lf_value);
 		__syncthreads();
-
-		// ---- element load vectors F_i = sum_q (w det f)(q) phi_i(q), by sum
-		// factorisation: thread (e, a, b) contracts q3, then q2, then q1 for all c
-		if (do_rhs) {
-			for (int i = tid; i < EB * NX * NY; i += NT) {
-				const int e = i / (NX * NY), ab = i % (NX * NY), a = ab / NY, b = ab % NY;
-				double *Eb = E0 + e * S::E_SIZE;
-				const double *src = Eb + S::E_G + 7 * NQ;
-				double fc[NZ];
-#pragma unroll
-				for (int c = 0; c < NZ; c++) fc[c] = 0.0;
-				for (int q1 = 0; q1 < NQX; q1++) {
-					double s1[NZ];
-#pragma unroll
-					for (int c = 0; c < NZ; c++) s1[c] = 0.0;
-					for (int q2 = 0; q2 < NQY; q2++) {
-						const double vy = tab[S::OVY + b * NQY + q2];
-#pragma unroll
-						for (int q3 = 0; q3 < NQZ; q3++) {
-							const double w = src[(q1 * NQY + q2) * NQZ + q3] * vy;
-#pragma unroll
-							for (int c = 0; c < NZ; c++) s1[c] += w * tab[S::OVZ + c * NQZ + q3];
-						}
-					}
-					const double vx = tab[S::OVX + a * NQX + q1];
-#pragma unroll
-					for (int c = 0; c < NZ; c++) fc[c] += vx * s1[c];
-				}
-#pragma unroll
-				for (int c = 0; c < NZ; c++) Eb[S::E_F + ab * NZ + c] = fc[c];
-			}
-		}
-
-		// ---- stage 1: item (e, k, q1, q2) produces T1_k[q1][q2][*][*]
-		//   k: 0 xx, 1 yy, 2 zz (+ mass), 3 xy, 4 xz, 5 yz
-		for (int i = tid; i < EB * 6 * NQX * NQY; i += NT) {
-			const int e = i / (6 * NQX * NQY), r = i % (6 * NQX * NQY);
-			const int kk = r / (NQX * NQY), q12 = r % (NQX * NQY);
-			double *Eb = E0 + e * S::E_SIZE;
-			const double *gp = Eb + S::E_G + kk * NQ + q12 * NQZ;
-			const double *wz = Wz + kT1Flags[kk][2] * NZ * NZ * NQZ;
-			double g[NQZ];
-#pragma unroll
-			for (int q3 = 0; q3 < NQZ; q3++) g[q3] = gp[q3];
-			double *out = Eb + S::E_T1 + kk * S::T1N + q12 * NZ * NZ;
-			if (kk == 2 && args.mass) {
-				const double *gm = Eb + S::E_G + 6 * NQ + q12 * NQZ;
-				const double *wz0 = Wz;
-				double h[NQZ];
-#pragma unroll
-				for (int q3 = 0; q3 < NQZ; q3++) h[q3] = gm[q3];
-#pragma unroll
-				for (int cc = 0; cc < NZ * NZ; cc++) {
-					double s = 0.0;
-#pragma unroll
-					for (int q3 = 0; q3 < NQZ; q3++) s += g[q3] * wz[cc * NQZ + q3] + h[q3] * wz0[cc * NQZ + q3];
-					out[cc] = s;
-				}
-			}
-			else {
-#pragma unroll
-				for (int cc = 0; cc < NZ * NZ; cc++) {
-					double s = 0.0;
-#pragma unroll
-					for (int q3 = 0; q3 < NQZ; q3++) s += g[q3] * wz[cc * NQZ + q3];
-					out[cc] = s;
-				}
-			}
-		}
+		if (do_rhs) sf_load_vector<S, NT, EB>(tab, E0);
+		sf_stage1<S, NT, EB>(E0, Wz, args.mass);
 		__syncthreads();
 		if (PF && bt + gridDim.x < nbatch) prefetch2();   // the first-level loads have had stage 1 to land
-		// ---- stages 2+3: thread owns column (e, b, b', c, c'); it accumulates
-		// the stage-2 values of the 3 x-classes in registers,
-		//   V_f[q1] = sum_k(class f) sum_q2 Wy_k[b][b'][q2] T1_k[q1][q2][c][c'],
-		// then A[(a,b,c)][(a',b',c')] = sum_f sum_q1 Wx_f[a][a'][q1] V_f[q1].
-		{
-			static_assert(EB * COLS <= NT, "one stage-3 column per thread");
-			const int e = tid / COLS, col = tid % COLS;
-			const bool active = tid < EB * COLS;
-			double acc[NX * NX];
-			const int bb = col / (NZ * NZ), cc = col % (NZ * NZ);
-			if (active) {
-				const double *Eb = E0 + e * S::E_SIZE;
-				double V[3][NQX];
-#pragma unroll
-				for (int f = 0; f < 3; f++)
-#pragma unroll
-					for (int q1 = 0; q1 < NQX; q1++) V[f][q1] = 0.0;
-#pragma unroll
-				for (int kk = 0; kk < 6; kk++) {
-					// compile-time after unrolling, so V stays in registers
-					constexpr int kFy[6] = { 0, 3, 0, 1, 0, 2 };
-					constexpr int kCls[6] = { 2, 0, 0, 1, 1, 0 };
-					const double *wy = Wy + kFy[kk] * NY * NY * NQY + bb * NQY;
-					const double *t1 = Eb + S::E_T1 + kk * S::T1N + cc;
-					const int f = kCls[kk];
-					double wyr[NQY];
-#pragma unroll
-					for (int q2 = 0; q2 < NQY; q2++) wyr[q2] = wy[q2];
-#pragma unroll
-					for (int q1 = 0; q1 < NQX; q1++) {
-						double s2 = V[f][q1];
-#pragma unroll
-						for (int q2 = 0; q2 < NQY; q2++) s2 += wyr[q2] * t1[(q1 * NQY + q2) * NZ * NZ];
-						V[f][q1] = s2;
-					}
-				}
-				const double *wx0 = Wx, *wx2 = Wx + 2 * NX * NX * NQX, *wx3 = Wx + 3 * NX * NX * NQX;
-#pragma unroll
-				for (int r = 0; r < NX * NX; r++) {
-					double s3 = 0.0;
-#pragma unroll
-					for (int q1 = 0; q1 < NQX; q1++)
-						s3 += wx0[r * NQX + q1] * V[0][q1] + wx2[r * NQX + q1] * V[1][q1] + wx3[r * NQX + q1] * V[2][q1];
-					acc[r] = s3;
-				}
-			}
-			__syncthreads();   // T1 fully consumed: A may overwrite it
-			if (active) {
-				const int b = bb / NY, b2 = bb % NY, c = cc / NZ, c2 = cc % NZ;
-				double *A = E0 + e * S::E_SIZE + S::E_A;
-#pragma unroll
-				for (int a = 0; a < NX; a++)
-#pragma unroll
-					for (int a2 = 0; a2 < NX; a2++)
-						A[((a * NY + b) * NZ + c) * NL + (a2 * NY + b2) * NZ + c2] = acc[a * NX + a2];
-			}
-		}
+		sf_stage23<S, NT, EB>(E0, Wx, Wy);
 		__syncthreads();
 
 		// ---- scatter into the CSC matrix (exclusive within a colour)

@@ -422,7 +422,18 @@ class Discretization:
     def tuning(self):
         t, e, ms = C.c_int32(), C.c_int32(), C.c_float()
         capi.call("h3dg_disc_get_tuning", self.handle, C.byref(t), C.byref(e), C.byref(ms))
-        return {"threads": t.value, "elems_per_cta": e.value, "ms": ms.value}
+        sg = C.c_int32()
+        capi.call("h3dg_disc_tuned_scatter", self.handle, C.byref(sg))
+        scatter = {1: "segmented", 0: "colour sweeps"}.get(sg.value, "not tuned")
+        return {"threads": t.value, "elems_per_cta": e.value, "ms": ms.value, "scatter": scatter}
+
+    def seg_stats(self):
+        """Wait statistics of the last segmented assembly (measurement hook)."""
+        out = (C.c_int64 * 8)()
+        capi.call("h3dg_disc_seg_stats", self.handle, out)
+        keys = ("element_items_waited", "element_polls", "column_items_waited", "column_polls", "items",
+                "ring_windows", "ctas", "span_windows")
+        return dict(zip(keys, list(out)))
 
     def last_launch_count(self):
         n = C.c_int32()

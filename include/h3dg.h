@@ -242,6 +242,16 @@ h3dg_status h3dg_disc_last_launch_count(const h3dg_disc *disc, int32_t *count);
  * assembly with it in milliseconds (all -1 / 0 before the first assembly).
  * No reference counterpart. */
 h3dg_status h3dg_disc_get_tuning(const h3dg_disc *disc, int32_t *threads, int32_t *elems_per_cta, float *ms);
+/* which scatter the picked low-order variant uses: 1 segmented (element
+ * matrices into an L2-resident ring, every CSC column summed in assembly
+ * order and written once), 0 colour sweeps, -1 not tuned.  Both give the
+ * same bits.  No reference counterpart. */
+h3dg_status h3dg_disc_tuned_scatter(const h3dg_disc *disc, int32_t *segmented);
+/* statistics of the last segmented assembly (a measurement hook, no
+ * reference counterpart): out[0..3] element items that waited and their
+ * polls, column items that waited and their polls; out[4..7] items, ring
+ * windows, CTAs, column span in windows. */
+h3dg_status h3dg_disc_seg_stats(const h3dg_disc *disc, int64_t *out);
 
 /* Kernel-only timing (no reference counterpart; a measurement hook): when
  * enabled with capacity n, each assemble call records a CUDA event pair on its
