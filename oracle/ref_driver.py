@@ -22,8 +22,11 @@ def available():
     return os.path.exists(DRIVER)
 
 
-def build(ref="/root/reference"):
-    """Compile the reference + shim + driver (needs the reference sources)."""
+def build(ref=None):
+    """Compile the reference + shim + driver (needs the reference sources;
+    their location: HERMES3D_REF, see oracle.REFERENCE_DIR)."""
+    if ref is None:
+        from oracle import REFERENCE_DIR as ref
     if not os.path.isdir(ref):
         return available()
     subprocess.run(["make", "-C", HERE, "-j8", "REF=" + ref, "all"], check=True, capture_output=True)

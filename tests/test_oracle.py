@@ -8,9 +8,8 @@ import numpy as np
 import pytest
 
 from helpers import FP64_RTOL, golden_names, highorder_names, lf_of, load, load_highorder, nq_of, rel_err
+from oracle import REFERENCE_DIR as REF
 from oracle import port, ref_driver
-
-REF = "/root/reference"
 
 
 @pytest.mark.parametrize("name", golden_names())
