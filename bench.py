@@ -473,8 +473,9 @@ def run_sweep(args):
     """Orders p = 1..8 (p+2 points per direction, jittered cube, a_e grad.grad,
     32^3 elements for p <= 4, 16^3 above): elements/s of the FP64 path (the
     kernel the library picks: low-order kernels up to p = 4, the high-order
-    kernel above) against the two tensor-core split precisions (forced onto
-    the high-order path at every order), with each split result's error
+    kernel above) against the two tensor-core split precisions (3xTF32: the
+    batched low-order kernel at p <= 2, the high-order path above; Ozaki: the
+    high-order path at every order), with each split result's error
     against the FP64 matrix.  One JSON line; not the headline."""
     import numpy as np
     import torch
@@ -485,7 +486,9 @@ def run_sweep(args):
         side = args.side or (32 if p <= 4 else 16)
         rec = {"p": p, "elements": side ** 3}
         ref = None
-        for name, prec, force in [("fp64", h.PREC_FP64, False), ("tf32x3", h.PREC_TF32X3, True),
+        # 3xTF32 at p <= 2: the batched low-order tensor-core kernel (elements
+        # stacked in the MMA tile); above, the high-order tensor-core kernel
+        for name, prec, force in [("fp64", h.PREC_FP64, False), ("tf32x3", h.PREC_TF32X3, p > 2),
                                   ("ozaki", h.PREC_OZAKI, True)]:
             if force:
                 os.environ["H3DG_FORCE_HIGH_ORDER"] = "1"

@@ -1290,38 +1290,8 @@ static h3dg_status seg_launch(h3dg_disc *disc, SegSpec &k, const h3dg::KArgs &a,
 	return H3DG_OK;
 }
 
-static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream) {
-	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "assemble: create_pattern() first");
-	if (precision != H3DG_PREC_FP64 && precision != H3DG_PREC_TF32X3 && precision != H3DG_PREC_OZAKI)
-		return fail(H3DG_ERR_INVALID_ARG, "assemble: unknown precision");
-	const h3dg::Plan &P = disc->plan;
-	if (P.mixed) {
-		h3dg_status s0 = ensure_device(disc);
-		if (s0 != H3DG_OK) return s0;
-		H3DG_CUDA_TRY(cudaSetDevice(disc->device));
-		return assemble_mixed(disc, d_Ax, d_rhs, (cudaStream_t) stream);
-	}
-	if (P.px != P.py || P.px != P.pz || P.nqx != P.nqy || P.nqx != P.nqz)
-		return fail(H3DG_ERR_INVALID_ARG, "assemble: anisotropic orders need the batched path");
-	if (P.canon) {
-		h3dg_status s0 = ensure_device(disc);
-		if (s0 != H3DG_OK) return s0;
-		H3DG_CUDA_TRY(cudaSetDevice(disc->device));
-		return assemble_ho(disc, precision, d_Ax, d_rhs, (cudaStream_t) stream);
-	}
-	// candidates: colour-sweep kernels (index into kernel_table) and, where
-	// the plan has its tables, segmented-scatter kernels (kSegVariant + index
-	// into seg_table); all give the same bits
-	const std::vector<int> cands = lo_candidates(disc);
-	if (cands.empty()) return fail(H3DG_ERR_INVALID_ARG, "assemble: no FP64 kernel instantiated for this order / rule");
-	{
-		h3dg_status s0 = ensure_device(disc);
-		if (s0 != H3DG_OK) return s0;
-	}
-	if (!disc->xyz.p || !disc->el_vtx.p || !disc->el_off.p || !disc->Ap.p || !disc->tables.p || !disc->status.p || !disc->el_s.p)
-		return fail(H3DG_ERR_STATE, "assemble: device plan missing");
-	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
-	cudaStream_t st = (cudaStream_t) stream;
+// KArgs of the low-order kernels for the current plan and outputs
+static h3dg::KArgs lo_args(h3dg_disc *disc, double *d_Ax, double *d_rhs) {
 	h3dg::KArgs a;
 	a.xyz = disc->xyz.p;
 	a.el_vtx = disc->el_vtx.p;
@@ -1342,6 +1312,90 @@ static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax,
 	a.rhs = disc->lf ? d_rhs : nullptr;
 	a.status = disc->status.p;
 	a.wait_limit = h3dg::kWaitPolls;
+	return a;
+}
+
+// Split precision at low orders: one launch per colour of the batched
+// tensor-core kernel (one CTA per SM), outputs zeroed first.
+static h3dg_status assemble_lo_tc(h3dg_disc *disc, KernelSpec &k, double *d_Ax, double *d_rhs, cudaStream_t st) {
+	const h3dg::Plan &P = disc->plan;
+	{
+		h3dg_status s0 = ensure_device(disc);
+		if (s0 != H3DG_OK) return s0;
+	}
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	if (!k.configured) {
+		H3DG_CUDA_TRY(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) k.smem));
+		k.configured = true;
+	}
+	h3dg::KArgs a = lo_args(disc, d_Ax, d_rhs);
+	if (disc->debug_once == H3DG_DEBUG_WAIT_GIVES_UP) a.wait_limit = 0;
+	disc->debug_once = 0;
+	int nsm = 148;
+	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
+	const bool rec = disc->tn < disc->tcap;
+	if (rec) H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn], st));
+	if (d_Ax) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
+	if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
+	int32_t n = 0;
+	for (int c = 0; c < P.ncolors; c++) {
+		const int64_t kb = P.color_ptr[c], ke = P.color_ptr[c + 1];
+		if (ke <= kb) continue;
+		const int64_t nb = (ke - kb + k.eb - 1) / k.eb;
+		k.fn<<<(unsigned) std::min<int64_t>(nb, nsm), k.threads, k.smem, st>>>(a, kb, ke);
+		n++;
+	}
+	H3DG_CUDA_TRY(cudaGetLastError());
+	if (rec) {
+		H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn + 1], st));
+		disc->tn++;
+	}
+	disc->last_launches = n;
+	return H3DG_OK;
+}
+
+static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream) {
+	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "assemble: create_pattern() first");
+	if (precision != H3DG_PREC_FP64 && precision != H3DG_PREC_TF32X3 && precision != H3DG_PREC_OZAKI)
+		return fail(H3DG_ERR_INVALID_ARG, "assemble: unknown precision");
+	const h3dg::Plan &P = disc->plan;
+	if (P.mixed) {
+		h3dg_status s0 = ensure_device(disc);
+		if (s0 != H3DG_OK) return s0;
+		H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+		return assemble_mixed(disc, d_Ax, d_rhs, (cudaStream_t) stream);
+	}
+	if (P.px != P.py || P.px != P.pz || P.nqx != P.nqy || P.nqx != P.nqz)
+		return fail(H3DG_ERR_INVALID_ARG, "assemble: anisotropic orders need the batched path");
+	if (P.canon) {
+		h3dg_status s0 = ensure_device(disc);
+		if (s0 != H3DG_OK) return s0;
+		H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+		return assemble_ho(disc, precision, d_Ax, d_rhs, (cudaStream_t) stream);
+	}
+	// split precision at low orders: the batched tensor-core kernel, where one
+	// is instantiated for (p, rule); otherwise FP64 (the split kernels of the
+	// high-order path need create() with the precision hint)
+	if (precision == H3DG_PREC_TF32X3) {
+		KernelSpec *lt = nullptr;
+		for (auto &k : lo_tc_table())
+			if (k.p == P.px && k.nq == P.nqx) lt = &k;
+		if (lt) return assemble_lo_tc(disc, *lt, d_Ax, d_rhs, (cudaStream_t) stream);
+	}
+	// candidates: colour-sweep kernels (index into kernel_table) and, where
+	// the plan has its tables, segmented-scatter kernels (kSegVariant + index
+	// into seg_table); all give the same bits
+	const std::vector<int> cands = lo_candidates(disc);
+	if (cands.empty()) return fail(H3DG_ERR_INVALID_ARG, "assemble: no FP64 kernel instantiated for this order / rule");
+	{
+		h3dg_status s0 = ensure_device(disc);
+		if (s0 != H3DG_OK) return s0;
+	}
+	if (!disc->xyz.p || !disc->el_vtx.p || !disc->el_off.p || !disc->Ap.p || !disc->tables.p || !disc->status.p || !disc->el_s.p)
+		return fail(H3DG_ERR_STATE, "assemble: device plan missing");
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	cudaStream_t st = (cudaStream_t) stream;
+	h3dg::KArgs a = lo_args(disc, d_Ax, d_rhs);
 	int nsm = 148;
 	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
 	// one assembly with candidate ci; returns launches, or -1 on a CUDA error

@@ -129,4 +129,8 @@ struct SegSpec {
 };
 std::vector<SegSpec> &seg_table();
 
+// split-precision (3xTF32) low-order kernels, elements batched on the tensor
+// cores (one launch per colour, one CTA per SM; KernelSpec::eb = elements per batch)
+std::vector<KernelSpec> &lo_tc_table();
+
 } // namespace h3dg_tables

@@ -150,88 +150,103 @@ __device__ __forceinline__ void sf_monomials(double *E0) {
 	}
 }
 
-// geometry at the quadrature points -> term weights.  Jacobian, signed
-// determinant and inverse as in RefMap::calc_inv_ref_map
-// (src/refmap.cc:177-231); G = w det J^-1 J^-T = (w / det) adj(J) adj(J)^T.
+// geometry at one quadrature point -> the 8 term weights (xx yy zz xy xz yz
+// mass source).  Jacobian, signed determinant and inverse as in
+// RefMap::calc_inv_ref_map (src/refmap.cc:177-231);
+// G = w det J^-1 J^-T = (w / det) adj(J) adj(J)^T.  cm: the 24 monomial
+// coefficients of the element's map, (x, y, z) the point, w its weight.
+__device__ __forceinline__ void sf_point_terms(const double *cm, double x, double y, double z, double w, double cg, int lf,
+                                               double lf_value, double t[8]) {
+	const double xy = x * y, xz = x * z, yz = y * z, xyz = xy * z;
+	double m[3][3], xp[3];
+#pragma unroll
+	for (int r = 0; r < 3; r++) {
+		const double c0 = cm[r], c1 = cm[3 + r], c2 = cm[6 + r], c3 = cm[9 + r];
+		const double c4 = cm[12 + r], c5 = cm[15 + r], c6 = cm[18 + r], c7 = cm[21 + r];
+		m[r][0] = c1 + c4 * y + c5 * z + c7 * yz;
+		m[r][1] = c2 + c4 * x + c6 * z + c7 * xz;
+		m[r][2] = c3 + c5 * x + c6 * y + c7 * xy;
+		xp[r] = c0 + c1 * x + c2 * y + c3 * z + c4 * xy + c5 * xz + c6 * yz + c7 * xyz;
+	}
+	// cofactors: adj(J)[c][k] = C[k][c]; J^-1 = adj(J) / det
+	const double C00 = m[1][1] * m[2][2] - m[1][2] * m[2][1];
+	const double C01 = m[1][2] * m[2][0] - m[1][0] * m[2][2];
+	const double C02 = m[1][0] * m[2][1] - m[1][1] * m[2][0];
+	const double C10 = m[0][2] * m[2][1] - m[0][1] * m[2][2];
+	const double C11 = m[0][0] * m[2][2] - m[0][2] * m[2][0];
+	const double C12 = m[0][1] * m[2][0] - m[0][0] * m[2][1];
+	const double C20 = m[0][1] * m[1][2] - m[0][2] * m[1][1];
+	const double C21 = m[0][2] * m[1][0] - m[0][0] * m[1][2];
+	const double C22 = m[0][0] * m[1][1] - m[0][1] * m[1][0];
+	const double det = m[0][0] * C00 + m[0][1] * C01 + m[0][2] * C02;
+	const double wd = w * det;
+	const double s = w * cg / det;
+	// (J^-1)[c][k] = C[k][c] / det  =>  G[c][d] = sum_k C[k][c] C[k][d] / det^2
+	t[0] = 0.5 * s * (C00 * C00 + C10 * C10 + C20 * C20);
+	t[1] = 0.5 * s * (C01 * C01 + C11 * C11 + C21 * C21);
+	t[2] = 0.5 * s * (C02 * C02 + C12 * C12 + C22 * C22);
+	t[3] = s * (C00 * C01 + C10 * C11 + C20 * C21);
+	t[4] = s * (C00 * C02 + C10 * C12 + C20 * C22);
+	t[5] = s * (C01 * C02 + C11 * C12 + C21 * C22);
+	t[6] = 0.5 * wd;
+	t[7] = wd * source_value(lf, lf_value, xp);
+}
+
+// geometry at the quadrature points of the batch -> term weights G
 template <class S, int NT, int EB>
 __device__ __forceinline__ void sf_geometry(const double *tab, double *E0, const double *s_cg, int lf, double lf_value) {
 	constexpr int NQY = S::NQ1Y, NQZ = S::NQ1Z, NQ = S::NQ;
 	for (int i = threadIdx.x; i < EB * NQ; i += NT) {
 		const int e = i / NQ, q = i % NQ;
 		double *Eb = E0 + e * S::E_SIZE;
-		double *G = Eb + S::E_G;
-		const double *cm = Eb + S::E_M;
 		const int q1 = q / (NQY * NQZ), q2 = (q / NQZ) % NQY, q3 = q % NQZ;
-		const double x = tab[S::OQX + q1], y = tab[S::OQY + q2], z = tab[S::OQZ + q3];
-		const double xy = x * y, xz = x * z, yz = y * z, xyz = xy * z;
-		double m[3][3], xp[3];
-#pragma unroll
-		for (int r = 0; r < 3; r++) {
-			const double c0 = cm[r], c1 = cm[3 + r], c2 = cm[6 + r], c3 = cm[9 + r];
-			const double c4 = cm[12 + r], c5 = cm[15 + r], c6 = cm[18 + r], c7 = cm[21 + r];
-			m[r][0] = c1 + c4 * y + c5 * z + c7 * yz;
-			m[r][1] = c2 + c4 * x + c6 * z + c7 * xz;
-			m[r][2] = c3 + c5 * x + c6 * y + c7 * xy;
-			xp[r] = c0 + c1 * x + c2 * y + c3 * z + c4 * xy + c5 * xz + c6 * yz + c7 * xyz;
-		}
-		// cofactors: adj(J)[c][k] = C[k][c]; J^-1 = adj(J) / det
-		const double C00 = m[1][1] * m[2][2] - m[1][2] * m[2][1];
-		const double C01 = m[1][2] * m[2][0] - m[1][0] * m[2][2];
-		const double C02 = m[1][0] * m[2][1] - m[1][1] * m[2][0];
-		const double C10 = m[0][2] * m[2][1] - m[0][1] * m[2][2];
-		const double C11 = m[0][0] * m[2][2] - m[0][2] * m[2][0];
-		const double C12 = m[0][1] * m[2][0] - m[0][0] * m[2][1];
-		const double C20 = m[0][1] * m[1][2] - m[0][2] * m[1][1];
-		const double C21 = m[0][2] * m[1][0] - m[0][0] * m[1][2];
-		const double C22 = m[0][0] * m[1][1] - m[0][1] * m[1][0];
-		const double det = m[0][0] * C00 + m[0][1] * C01 + m[0][2] * C02;
 		const double w = tab[S::OWX + q1] * tab[S::OWY + q2] * tab[S::OWZ + q3];
-		const double wd = w * det;
-		const double s = w * s_cg[e] / det;
-		// (J^-1)[c][k] = C[k][c] / det  =>  G[c][d] = sum_k C[k][c] C[k][d] / det^2
-		G[0 * NQ + q] = 0.5 * s * (C00 * C00 + C10 * C10 + C20 * C20);
-		G[1 * NQ + q] = 0.5 * s * (C01 * C01 + C11 * C11 + C21 * C21);
-		G[2 * NQ + q] = 0.5 * s * (C02 * C02 + C12 * C12 + C22 * C22);
-		G[3 * NQ + q] = s * (C00 * C01 + C10 * C11 + C20 * C21);
-		G[4 * NQ + q] = s * (C00 * C02 + C10 * C12 + C20 * C22);
-		G[5 * NQ + q] = s * (C01 * C02 + C11 * C12 + C21 * C22);
-		G[6 * NQ + q] = 0.5 * wd;
-		G[7 * NQ + q] = wd * source_value(lf, lf_value, xp);
+		double t[8];
+		sf_point_terms(Eb + S::E_M, tab[S::OQX + q1], tab[S::OQY + q2], tab[S::OQZ + q3], w, s_cg[e], lf, lf_value, t);
+#pragma unroll
+		for (int r = 0; r < 8; r++) Eb[S::E_G + r * NQ + q] = t[r];
 	}
 }
 
-// element load vectors F_i = sum_q (w det f)(q) phi_i(q), by sum
-// factorisation: thread (e, a, b) contracts q3, then q2, then q1 for all c
+// element load vector F_i = sum_q (w det f)(q) phi_i(q) of one (a, b) line,
+// by sum factorisation: contracts q3, then q2, then q1 for all c.  src: the
+// source weights at the NQ points, out: F[(a, b, *)] (NZ values).
+template <class S>
+__device__ __forceinline__ void sf_load_line(const double *tab, const double *src, int a, int b, double *out) {
+	constexpr int NZ = S::NZ;
+	constexpr int NQX = S::NQ1X, NQY = S::NQ1Y, NQZ = S::NQ1Z;
+	double fc[NZ];
+#pragma unroll
+	for (int c = 0; c < NZ; c++) fc[c] = 0.0;
+	for (int q1 = 0; q1 < NQX; q1++) {
+		double s1[NZ];
+#pragma unroll
+		for (int c = 0; c < NZ; c++) s1[c] = 0.0;
+		for (int q2 = 0; q2 < NQY; q2++) {
+			const double vy = tab[S::OVY + b * NQY + q2];
+#pragma unroll
+			for (int q3 = 0; q3 < NQZ; q3++) {
+				const double w = src[(q1 * NQY + q2) * NQZ + q3] * vy;
+#pragma unroll
+				for (int c = 0; c < NZ; c++) s1[c] += w * tab[S::OVZ + c * NQZ + q3];
+			}
+		}
+		const double vx = tab[S::OVX + a * NQX + q1];
+#pragma unroll
+		for (int c = 0; c < NZ; c++) fc[c] += vx * s1[c];
+	}
+#pragma unroll
+	for (int c = 0; c < NZ; c++) out[c] = fc[c];
+}
+
+// element load vectors of the batch: thread (e, a, b)
 template <class S, int NT, int EB>
 __device__ __forceinline__ void sf_load_vector(const double *tab, double *E0) {
-	constexpr int NX = S::NX, NY = S::NY, NZ = S::NZ;
-	constexpr int NQX = S::NQ1X, NQY = S::NQ1Y, NQZ = S::NQ1Z, NQ = S::NQ;
+	constexpr int NX = S::NX, NY = S::NY, NZ = S::NZ, NQ = S::NQ;
 	for (int i = threadIdx.x; i < EB * NX * NY; i += NT) {
-		const int e = i / (NX * NY), ab = i % (NX * NY), a = ab / NY, b = ab % NY;
+		const int e = i / (NX * NY), ab = i % (NX * NY);
 		double *Eb = E0 + e * S::E_SIZE;
-		const double *src = Eb + S::E_G + 7 * NQ;
-		double fc[NZ];
-#pragma unroll
-		for (int c = 0; c < NZ; c++) fc[c] = 0.0;
-		for (int q1 = 0; q1 < NQX; q1++) {
-			double s1[NZ];
-#pragma unroll
-			for (int c = 0; c < NZ; c++) s1[c] = 0.0;
-			for (int q2 = 0; q2 < NQY; q2++) {
-				const double vy = tab[S::OVY + b * NQY + q2];
-#pragma unroll
-				for (int q3 = 0; q3 < NQZ; q3++) {
-					const double w = src[(q1 * NQY + q2) * NQZ + q3] * vy;
-#pragma unroll
-					for (int c = 0; c < NZ; c++) s1[c] += w * tab[S::OVZ + c * NQZ + q3];
-				}
-			}
-			const double vx = tab[S::OVX + a * NQX + q1];
-#pragma unroll
-			for (int c = 0; c < NZ; c++) fc[c] += vx * s1[c];
-		}
-#pragma unroll
-		for (int c = 0; c < NZ; c++) Eb[S::E_F + ab * NZ + c] = fc[c];
+		sf_load_line<S>(tab, Eb + S::E_G + 7 * NQ, ab / NY, ab % NY, Eb + S::E_F + ab * NZ);
 	}
 }
 
