@@ -12,6 +12,7 @@ import os
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libh3dg.so")
 
 H3DG_OK = 0
+H3DG_ERR_INVALID_ARG = 1
 H3DG_ERR_STATE = 6
 H3DG_ERR_TIMEOUT = 7
 H3DG_ERR_TOO_LARGE = 8
@@ -27,6 +28,7 @@ BF_GRAD_GRAD, BF_GRAD_GRAD_MASS = 1, 2
 LF_NONE, LF_CONST, LF_SIN = 0, 1, 2
 SBF_U_V, SLF_G_V = 1, 1
 QUAD_FIXED, QUAD_P_PLUS = 0, 1
+QUAD_STOCK = 2
 PREC_FP64 = 0
 PREC_TF32X3 = 1
 PREC_OZAKI = 2
@@ -71,6 +73,7 @@ SIGNATURES = {
     "h3dg_disc_create": [C.POINTER(_p), C.c_int],
     "h3dg_disc_destroy": [_p],
     "h3dg_disc_set_space": [_p, _p],
+    "h3dg_disc_set_test_space": [_p, _p],
     "h3dg_disc_set_bilinear_form": [_p, C.c_int, _pd, _i64],
     "h3dg_disc_set_linear_form": [_p, C.c_int, C.c_double],
     "h3dg_disc_set_quadrature": [_p, C.c_int, C.c_int],

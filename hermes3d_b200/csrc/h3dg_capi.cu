@@ -71,6 +71,7 @@ struct DBuf {
 struct h3dg_disc {
 	int device = 0;
 	h3dg_space *space = nullptr;
+	h3dg_space *test_space = nullptr;  // test space of a system block (nullptr: the trial space)
 	int bf = 0;
 	std::vector<double> ecoef;       // per element id
 	int lf = H3DG_LF_NONE;
@@ -113,8 +114,8 @@ struct h3dg_disc {
 	DBuf<uint16_t> el_offt;    // tensor-core scatter stream (built at the first split-precision assembly)
 	bool offt_store_all = false;   // its first-touch stores cover every Ax slot
 	DBuf<double> ho_scratch;   // per-CTA global work area of the FP64-accurate split kernel
-	DBuf<int32_t> el_cdof;
-	DBuf<double> el_ccoef;
+	DBuf<int32_t> el_cdof, el_tcdof;
+	DBuf<double> el_ccoef, el_tccoef;
 	DBuf<double> el_coef;
 	DBuf<int> status;
 	// segmented scatter: plan tables, the item schedule of the current launch
@@ -384,6 +385,13 @@ h3dg_status h3dg_disc_set_space(h3dg_disc *disc, h3dg_space *space) {
 	return H3DG_OK;
 }
 
+h3dg_status h3dg_disc_set_test_space(h3dg_disc *disc, h3dg_space *test) {
+	if (!disc) return fail(H3DG_ERR_INVALID_ARG, "set_test_space: bad arguments");
+	disc->test_space = test;
+	disc->have_plan = false;
+	return H3DG_OK;
+}
+
 h3dg_status h3dg_disc_set_bilinear_form(h3dg_disc *disc, int form, const double *elem_coef, int64_t ne) {
 	if (!disc) return fail(H3DG_ERR_INVALID_ARG, "set_bilinear_form: null disc");
 	if (form != H3DG_BF_GRAD_GRAD && form != H3DG_BF_GRAD_GRAD_MASS)
@@ -420,7 +428,8 @@ h3dg_status h3dg_disc_set_surface_forms(h3dg_disc *disc, int bilinear, int linea
 }
 
 h3dg_status h3dg_disc_set_quadrature(h3dg_disc *disc, int mode, int n) {
-	if (!disc || (mode != H3DG_QUAD_FIXED && mode != H3DG_QUAD_P_PLUS) || n < 0 || n > h3dg::kMaxQuadPoints)
+	if (!disc || (mode != H3DG_QUAD_FIXED && mode != H3DG_QUAD_P_PLUS && mode != H3DG_QUAD_STOCK) || n < 0 ||
+	    n > h3dg::kMaxQuadPoints)
 		return fail(H3DG_ERR_INVALID_ARG, "set_quadrature: bad arguments");
 	disc->qmode = mode;
 	disc->qn = n;
@@ -449,13 +458,39 @@ static void build_table_blob(const h3dg::Plan &P, std::vector<double> &blob) {
 	if (blob.size() % 2) blob.push_back(0.0);
 }
 
+// 1D tables of the stock rule (layout of StockShape): the rules of 2 .. p+1
+// points concatenated (points, weights, Lobatto values and derivatives at
+// them), then the 13-point rule of the load vector (points, weights, values)
+static void build_stock_blob(int p, std::vector<double> &blob) {
+	blob.clear();
+	std::vector<double> qc, wc, q, w;
+	for (int n = 2; n <= p + 1; n++) {
+		h3dg::gauss_legendre(n, q, w);
+		qc.insert(qc.end(), q.begin(), q.end());
+		wc.insert(wc.end(), w.begin(), w.end());
+	}
+	blob.insert(blob.end(), qc.begin(), qc.end());
+	blob.insert(blob.end(), wc.begin(), wc.end());
+	for (int k = 0; k <= p; k++)
+		for (double x : qc) blob.push_back(h3dg::lobatto_value(k, x));
+	for (int k = 0; k <= p; k++)
+		for (double x : qc) blob.push_back(h3dg::lobatto_deriv(k, x));
+	h3dg::gauss_legendre(13, q, w);
+	blob.insert(blob.end(), q.begin(), q.end());
+	blob.insert(blob.end(), w.begin(), w.end());
+	for (int k = 0; k <= p; k++)
+		for (double x : q) blob.push_back(h3dg::lobatto_value(k, x));
+	if (blob.size() % 2) blob.push_back(0.0);
+}
+
 h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nnz) {
 	if (!disc || !disc->space) return fail(H3DG_ERR_STATE, "create_pattern: set_space() first");
 	if (!disc->space->s.assigned) return fail(H3DG_ERR_STATE, "create_pattern: assign_dofs() first");
 	if (!disc->bf) return fail(H3DG_ERR_STATE, "create_pattern: set_bilinear_form() first");
 	const h3dg::Space &sp = disc->space->s;
 	int nq[3];
-	for (int d = 0; d < 3; d++) nq[d] = disc->qmode == H3DG_QUAD_FIXED ? disc->qn : sp.order[d] + disc->qn;
+	for (int d = 0; d < 3; d++)
+		nq[d] = disc->qmode == H3DG_QUAD_FIXED ? disc->qn : disc->qmode == H3DG_QUAD_STOCK ? 2 : sp.order[d] + disc->qn;
 	std::string err;
 	// orders >= 5: the element matrix does not fit in shared memory; the
 	// high-order kernel works on canonical tables
@@ -484,6 +519,42 @@ h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nn
 		if (h3dg::make_partition_scope(sp, disc->nparts, disc->part, disc->scope, err) != 0)
 			return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
 		scope = &disc->scope;
+	}
+	const h3dg::Space *tsp = disc->test_space && disc->test_space != disc->space ? &disc->test_space->s : nullptr;
+	if (tsp) {
+		// a block of a system with two different spaces: canonical FP64 plan at the
+		// larger order, rows from the test space, columns from the trial space
+		bool tmixed = false;
+		for (int64_t e = 1; e < (int64_t) tsp->order.size() / 3 && !tmixed; e++)
+			for (int d = 0; d < 3; d++)
+				if (tsp->order[3 * e + d] != tsp->order[d]) tmixed = true;
+		if (!tsp->assigned) return fail(H3DG_ERR_STATE, "create_pattern: assign_dofs() on the test space first");
+		if (tsp->mesh != sp.mesh || mixed || tmixed || sp.mesh->nrefined || disc->nparts > 1 || disc->sbf || disc->slf ||
+		    disc->qmode == H3DG_QUAD_STOCK)
+			return fail(H3DG_ERR_INVALID_ARG, "create_pattern: a block with two spaces needs one mesh, uniform orders in "
+			                                  "each space, no refinement, partition, surface forms or stock rule");
+		for (int d = 0; d < 3; d++)
+			if (disc->qmode == H3DG_QUAD_P_PLUS) nq[d] = std::max(sp.order[d], tsp->order[d]) + disc->qn;
+		disc->reset_mixed();
+		disc->scope = h3dg::PlanScope();
+		if (h3dg::build_plan(sp, nq[0], nq[1], nq[2], disc->plan, err, true, nullptr, tsp) != 0)
+			return fail(H3DG_ERR_INVALID_ARG, "create_pattern: " + err);
+		const h3dg::Plan &P2 = disc->plan;
+		disc->on_device = false;
+		disc->have_plan = true;
+		disc->prepared = 0;
+		disc->have_eval = false;
+		disc->variant = -1;
+		if (ndof) *ndof = P2.ndof;
+		if (nnz) *nnz = P2.nnz;
+		return H3DG_OK;
+	}
+	if (disc->qmode == H3DG_QUAD_STOCK) {
+		// the stock rule: uniform orders 1..3, whole elements (no hanging nodes), volume forms
+		if (mixed || canon || sp.order[0] != sp.order[1] || sp.order[0] != sp.order[2] || pmax > 3 || disc->sbf ||
+		    disc->slf)
+			return fail(H3DG_ERR_INVALID_ARG, "create_pattern: the stock quadrature needs one order 1..3 in every "
+			                                  "direction, no refinement and no surface forms");
 	}
 	if (mixed) {
 		if (h3dg::build_plan_mixed(sp, disc->qmode == H3DG_QUAD_P_PLUS, disc->qn, disc->plan, err, scope) != 0)
@@ -568,6 +639,10 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 	else if (P.canon) {
 		H3DG_CUDA_TRY(disc->el_cdof.upload(P.el_cdof));
 		H3DG_CUDA_TRY(disc->el_ccoef.upload(P.el_ccoef));
+		if (P.two_space) {
+			H3DG_CUDA_TRY(disc->el_tcdof.upload(P.el_tcdof));
+			H3DG_CUDA_TRY(disc->el_tccoef.upload(P.el_tccoef));
+		}
 		H3DG_CUDA_TRY(disc->el_offc.upload(P.el_offc));
 		disc->el_offt.release();
 		disc->offt_store_all = false;
@@ -601,6 +676,7 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 	}
 	std::vector<double> blob;
 	if (P.mixed) blob = P.mixed_tables;
+	else if (disc->qmode == H3DG_QUAD_STOCK) build_stock_blob(P.px, blob);
 	else build_table_blob(P, blob);
 	disc->table_bytes = (int) (blob.size() * sizeof(double));
 	H3DG_CUDA_TRY(disc->tables.upload(blob));
@@ -713,6 +789,8 @@ static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, dou
 	a.ecoef = disc->coef.p;
 	a.cdof = disc->el_cdof.p;
 	a.ccoef = disc->el_ccoef.p;
+	a.tcdof = P.two_space ? disc->el_tcdof.p : nullptr;
+	a.tccoef = P.two_space ? disc->el_tccoef.p : nullptr;
 	a.offc = disc->el_offc.p;
 	if ((precision == H3DG_PREC_TF32X3 || precision == H3DG_PREC_OZAKI) && d_Ax && !disc->el_offt.p && P.ne > 0) {
 		// built once per plan; the build validates every position against its
@@ -747,7 +825,7 @@ static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, dou
 	// the 3xTF32 epilogue stores each slot's first contribution (no zero-fill needed)
 	if (d_Ax && !(precision == H3DG_PREC_TF32X3 && disc->offt_store_all))
 		H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
-	if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.ndof, st));
+	if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.nrhs(), st));
 	int nsm = 148;
 	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
 	HoSpec &k = *kp;
@@ -1315,9 +1393,10 @@ static h3dg::KArgs lo_args(h3dg_disc *disc, double *d_Ax, double *d_rhs) {
 	return a;
 }
 
-// Split precision at low orders: one launch per colour of the batched
-// tensor-core kernel (one CTA per SM), outputs zeroed first.
-static h3dg_status assemble_lo_tc(h3dg_disc *disc, KernelSpec &k, double *d_Ax, double *d_rhs, cudaStream_t st) {
+// One launch per colour of kernel k (split precision at low orders: one CTA
+// per SM; otherwise as many as fit), outputs zeroed first.
+static h3dg_status assemble_colours(h3dg_disc *disc, KernelSpec &k, double *d_Ax, double *d_rhs, cudaStream_t st,
+                                    bool one_per_sm) {
 	const h3dg::Plan &P = disc->plan;
 	{
 		h3dg_status s0 = ensure_device(disc);
@@ -1331,8 +1410,12 @@ static h3dg_status assemble_lo_tc(h3dg_disc *disc, KernelSpec &k, double *d_Ax, 
 	h3dg::KArgs a = lo_args(disc, d_Ax, d_rhs);
 	if (disc->debug_once == H3DG_DEBUG_WAIT_GIVES_UP) a.wait_limit = 0;
 	disc->debug_once = 0;
-	int nsm = 148;
+	int nsm = 148, per_sm = 1;
 	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
+	if (!one_per_sm) {
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, k.smem);
+		per_sm = std::max(per_sm, 1);
+	}
 	const bool rec = disc->tn < disc->tcap;
 	if (rec) H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn], st));
 	if (d_Ax) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
@@ -1342,7 +1425,7 @@ static h3dg_status assemble_lo_tc(h3dg_disc *disc, KernelSpec &k, double *d_Ax, 
 		const int64_t kb = P.color_ptr[c], ke = P.color_ptr[c + 1];
 		if (ke <= kb) continue;
 		const int64_t nb = (ke - kb + k.eb - 1) / k.eb;
-		k.fn<<<(unsigned) std::min<int64_t>(nb, nsm), k.threads, k.smem, st>>>(a, kb, ke);
+		k.fn<<<(unsigned) std::min<int64_t>(nb, (int64_t) nsm * per_sm), k.threads, k.smem, st>>>(a, kb, ke);
 		n++;
 	}
 	H3DG_CUDA_TRY(cudaGetLastError());
@@ -1371,7 +1454,16 @@ static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax,
 		h3dg_status s0 = ensure_device(disc);
 		if (s0 != H3DG_OK) return s0;
 		H3DG_CUDA_TRY(cudaSetDevice(disc->device));
-		return assemble_ho(disc, precision, d_Ax, d_rhs, (cudaStream_t) stream);
+		// a two-space block is assembled in FP64 (the split kernels take one space)
+		return assemble_ho(disc, P.two_space ? H3DG_PREC_FP64 : precision, d_Ax, d_rhs, (cudaStream_t) stream);
+	}
+	// the reference's stock quadrature: FP64 per-pair rules
+	if (disc->qmode == H3DG_QUAD_STOCK) {
+		KernelSpec *ks = nullptr;
+		for (auto &k : stock_table())
+			if (k.p == P.px) ks = &k;
+		if (!ks) return fail(H3DG_ERR_INVALID_ARG, "assemble: no stock-quadrature kernel for this order");
+		return assemble_colours(disc, *ks, d_Ax, d_rhs, (cudaStream_t) stream, false);
 	}
 	// split precision at low orders: the batched tensor-core kernel, where one
 	// is instantiated for (p, rule); otherwise FP64 (the split kernels of the
@@ -1380,7 +1472,7 @@ static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax,
 		KernelSpec *lt = nullptr;
 		for (auto &k : lo_tc_table())
 			if (k.p == P.px && k.nq == P.nqx) lt = &k;
-		if (lt) return assemble_lo_tc(disc, *lt, d_Ax, d_rhs, (cudaStream_t) stream);
+		if (lt) return assemble_colours(disc, *lt, d_Ax, d_rhs, (cudaStream_t) stream, true);
 	}
 	// candidates: colour-sweep kernels (index into kernel_table) and, where
 	// the plan has its tables, segmented-scatter kernels (kSegVariant + index
@@ -1611,11 +1703,11 @@ h3dg_status h3dg_disc_assemble_host(h3dg_disc *disc, int precision, double *Ax, 
 	const h3dg::Plan &P = disc->plan;
 	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
 	if (Ax && disc->Ax.n != (size_t) P.nnz) H3DG_CUDA_TRY(disc->Ax.alloc(P.nnz));
-	if (rhs && disc->rhs.n != (size_t) P.ndof) H3DG_CUDA_TRY(disc->rhs.alloc(P.ndof));
+	if (rhs && disc->rhs.n != (size_t) P.nrhs()) H3DG_CUDA_TRY(disc->rhs.alloc(P.nrhs()));
 	h3dg_status s = h3dg_disc_assemble(disc, precision, Ax ? disc->Ax.p : nullptr, rhs ? disc->rhs.p : nullptr, nullptr);
 	if (s != H3DG_OK) return s;
 	if (Ax) H3DG_CUDA_TRY(cudaMemcpy(Ax, disc->Ax.p, sizeof(double) * P.nnz, cudaMemcpyDeviceToHost));
-	if (rhs) H3DG_CUDA_TRY(cudaMemcpy(rhs, disc->rhs.p, sizeof(double) * P.ndof, cudaMemcpyDeviceToHost));
+	if (rhs) H3DG_CUDA_TRY(cudaMemcpy(rhs, disc->rhs.p, sizeof(double) * P.nrhs(), cudaMemcpyDeviceToHost));
 	int st = 0;
 	H3DG_CUDA_TRY(cudaMemcpy(&st, disc->status.p, sizeof(int), cudaMemcpyDeviceToHost));
 	if (st) {
@@ -1654,7 +1746,7 @@ h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, doub
 		return fail(H3DG_ERR_INVALID_ARG, "assemble_host_noalloc: unknown precision");
 	const h3dg::Plan &P = disc->plan;
 	const size_t rhs_off = ((size_t) P.nnz + 31) / 32 * 32;          // 256-byte boundary
-	const size_t need = (rhs ? rhs_off + (size_t) P.ndof : (size_t) P.nnz);
+	const size_t need = (rhs ? rhs_off + (size_t) P.nrhs() : (size_t) P.nnz);
 	if (need > (size_t) H3DG_NOALLOC_SCRATCH_DOUBLES)
 		return fail(H3DG_ERR_TOO_LARGE, "assemble_host_noalloc: nnz + ndof = " + std::to_string(need) +
 		                                    " doubles exceed the fixed staging array of " +
@@ -1698,7 +1790,7 @@ h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, doub
 	t_mixed_direct = false;
 	if (s != H3DG_OK) return s;
 	if (Ax) H3DG_CUDA_TRY(cudaMemcpy(Ax, d_Ax, sizeof(double) * P.nnz, cudaMemcpyDeviceToHost));
-	if (rhs) H3DG_CUDA_TRY(cudaMemcpy(rhs, d_rhs, sizeof(double) * P.ndof, cudaMemcpyDeviceToHost));
+	if (rhs) H3DG_CUDA_TRY(cudaMemcpy(rhs, d_rhs, sizeof(double) * P.nrhs(), cudaMemcpyDeviceToHost));
 	int st = 0;
 	H3DG_CUDA_TRY(cudaMemcpy(&st, disc->status.p, sizeof(int), cudaMemcpyDeviceToHost));
 	if (st) {

@@ -1070,22 +1070,31 @@ int make_partition_scope(const Space &sp, int nparts, int part, PlanScope &S, st
 // row-position map used by the scatter and an element colouring.
 
 int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string &err, bool canon,
-               const PlanScope *scope) {
-	if (!sp.assigned) { err = "assign_dofs() has not been called"; return -1; }
+               const PlanScope *scope, const Space *test) {
+	if (!sp.assigned || (test && !test->assigned)) { err = "assign_dofs() has not been called"; return -1; }
 	const Mesh &m = *sp.mesh;
 	const int64_t ne = scope ? (int64_t) scope->elems.size() : m.ne();
 	auto G = [&](int64_t e) -> int64_t { return scope ? scope->elems[e] : e; };   // plan element -> mesh element
 	if (m.nrefined) { err = "refined meshes take the batched path"; return -1; }
+	const Space &ts = test ? *test : sp;
+	const bool two = &ts != &sp;
+	if (two && (ts.mesh != sp.mesh || scope)) { err = "the test and trial spaces of a block share one mesh (no partition)"; return -1; }
+	if (two) canon = true;
 	P = Plan();
 	P.ne = ne;
 	P.ne_ids = m.ne();
 	P.ndof = sp.ndof();
-	P.px = sp.order[0]; P.py = sp.order[1]; P.pz = sp.order[2];
-	for (int64_t e = 0; e < ne; e++)
-		if (sp.order[3 * G(e)] != P.px || sp.order[3 * G(e) + 1] != P.py || sp.order[3 * G(e) + 2] != P.pz) {
-			err = "plan requires one element order triple; bucket mixed orders first";
-			return -1;
-		}
+	P.two_space = two;
+	P.nrow = ts.ndof();
+	for (const Space *S : { &sp, &ts })
+		for (int64_t e = 0; e < ne; e++)
+			if (S->order[3 * G(e)] != S->order[0] || S->order[3 * G(e) + 1] != S->order[1] || S->order[3 * G(e) + 2] != S->order[2]) {
+				err = "plan requires one element order triple; bucket mixed orders first";
+				return -1;
+			}
+	P.px = std::max(sp.order[0], ts.order[0]);
+	P.py = std::max(sp.order[1], ts.order[1]);
+	P.pz = std::max(sp.order[2], ts.order[2]);
 	P.nl = (P.px + 1) * (P.py + 1) * (P.pz + 1);
 	if (nqx < 1 || nqy < 1 || nqz < 1 || nqx > kMaxQuadPoints || nqy > kMaxQuadPoints || nqz > kMaxQuadPoints) {
 		err = "Gauss points per direction must be in 1..13";
@@ -1097,38 +1106,53 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 	gauss_legendre(nqz, P.qz, P.wz);
 	const int nl = P.nl;
 
-	// element tables in element-id order first
-	std::vector<int32_t> cnt(2 * ne), dofs((size_t) ne * nl, -1);
-	std::vector<uint16_t> ss((size_t) ne * nl, 0);
-	std::vector<double> cf((size_t) ne * nl, 0.0);
-	std::string perr;
-	std::vector<int> bad(ne, 0);
-	parallel_for(ne, [&](int64_t lo, int64_t hi) {
-		std::vector<AsmEntry> al;
-		for (int64_t e = lo; e < hi; e++) {
-			sp.element_assembly_list(G(e), al);
-			int mcount = 0, lcount = 0;
-			for (auto &a : al) (a.dof >= 0 ? mcount : lcount)++;
-			if (mcount + lcount > nl) { bad[e] = 1; continue; }
-			int im = 0, il = mcount;
-			for (auto &a : al) {
-				Canon c = decode_index(a.idx);
-				int s = (c.a * (P.py + 1) + c.b) * (P.pz + 1) + c.c;
-				int k = a.dof >= 0 ? im++ : il++;
-				ss[(size_t) e * nl + k] = (uint16_t) s;
-				dofs[(size_t) e * nl + k] = a.dof >= 0 ? a.dof : DIRICHLET_DOF;
-				cf[(size_t) e * nl + k] = c.sign * a.coef;
+	// element tables in element-id order first: per element the assembly
+	// list's matrix entries, then its lifting entries; DOFs counted from the
+	// space's first DOF; canonical indices in the plan's (largest) basis
+	auto extract = [&](const Space &S, std::vector<int32_t> &cnt, std::vector<int32_t> &dofs, std::vector<uint16_t> &ss,
+	                   std::vector<double> &cf) -> int {
+		cnt.assign(2 * ne, 0);
+		dofs.assign((size_t) ne * nl, -1);
+		ss.assign((size_t) ne * nl, 0);
+		cf.assign((size_t) ne * nl, 0.0);
+		std::vector<int> bad(ne, 0);
+		parallel_for(ne, [&](int64_t lo, int64_t hi) {
+			std::vector<AsmEntry> al;
+			for (int64_t e = lo; e < hi; e++) {
+				S.element_assembly_list(G(e), al);
+				int mcount = 0, lcount = 0;
+				for (auto &a : al) (a.dof >= 0 ? mcount : lcount)++;
+				if (mcount + lcount > nl) { bad[e] = 1; continue; }
+				int im = 0, il = mcount;
+				for (auto &a : al) {
+					Canon c = decode_index(a.idx);
+					int sidx = (c.a * (P.py + 1) + c.b) * (P.pz + 1) + c.c;
+					int k = a.dof >= 0 ? im++ : il++;
+					ss[(size_t) e * nl + k] = (uint16_t) sidx;
+					dofs[(size_t) e * nl + k] = a.dof >= 0 ? a.dof - S.first_dof : DIRICHLET_DOF;
+					cf[(size_t) e * nl + k] = c.sign * a.coef;
+				}
+				// a DOF may appear once per element (no hanging-node constraints)
+				for (int i = 0; i < mcount && !bad[e]; i++)
+					for (int j = i + 1; j < mcount; j++)
+						if (dofs[(size_t) e * nl + i] == dofs[(size_t) e * nl + j]) { bad[e] = 2; break; }
+				cnt[2 * e] = mcount;
+				cnt[2 * e + 1] = lcount;
 			}
-			// a DOF may appear once per element (no hanging-node constraints)
-			for (int i = 0; i < mcount && !bad[e]; i++)
-				for (int j = i + 1; j < mcount; j++)
-					if (dofs[(size_t) e * nl + i] == dofs[(size_t) e * nl + j]) { bad[e] = 2; break; }
-			cnt[2 * e] = mcount;
-			cnt[2 * e + 1] = lcount;
-		}
-	});
-	for (int64_t e = 0; e < ne; e++)
-		if (bad[e]) { err = bad[e] == 1 ? "assembly list longer than the element basis" : "a DOF repeats in one assembly list (constrained space)"; return -1; }
+		});
+		for (int64_t e = 0; e < ne; e++)
+			if (bad[e]) { err = bad[e] == 1 ? "assembly list longer than the element basis" : "a DOF repeats in one assembly list (constrained space)"; return -1; }
+		return 0;
+	};
+	std::vector<int32_t> cnt, dofs, tcnt_v, tdofs_v;
+	std::vector<uint16_t> ss, tss_v;
+	std::vector<double> cf, tcf_v;
+	if (extract(sp, cnt, dofs, ss, cf) != 0) return -1;
+	if (two && extract(ts, tcnt_v, tdofs_v, tss_v, tcf_v) != 0) return -1;
+	// the test side: the test space's tables, or the trial space's
+	const std::vector<int32_t> &tcnt = two ? tcnt_v : cnt, &tdofs = two ? tdofs_v : dofs;
+	const std::vector<uint16_t> &tss = two ? tss_v : ss;
+	const std::vector<double> &tcf = two ? tcf_v : cf;
 
 	// DOF -> elements adjacency (CSR)
 	int64_t nd = P.ndof;
@@ -1150,7 +1174,7 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 		if (scope && !scope->owned[d]) return;                     // another part's column
 		for (int64_t k = dptr[d]; k < dptr[d + 1]; k++) {
 			int64_t e = dadj[k];
-			for (int j = 0; j < cnt[2 * e]; j++) buf.push_back(dofs[(size_t) e * nl + j]);
+			for (int j = 0; j < tcnt[2 * e]; j++) buf.push_back(tdofs[(size_t) e * nl + j]);   // rows: test DOFs
 		}
 		std::sort(buf.begin(), buf.end());
 		buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
@@ -1174,23 +1198,41 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 		}
 	});
 
+	// test DOF -> elements adjacency of a two-space plan (the RHS and the rows
+	// of a column are test DOFs: elements sharing one must not share a colour)
+	std::vector<int64_t> tptr;
+	std::vector<int32_t> tadj;
+	if (two) {
+		const int64_t nt = P.nrow;
+		tptr.assign(nt + 1, 0);
+		for (int64_t e = 0; e < ne; e++)
+			for (int k = 0; k < tcnt[2 * e]; k++) tptr[tdofs[(size_t) e * nl + k] + 1]++;
+		for (int64_t d = 0; d < nt; d++) tptr[d + 1] += tptr[d];
+		tadj.resize(tptr[nt]);
+		std::vector<int64_t> fill(tptr.begin(), tptr.end() - 1);
+		for (int64_t e = 0; e < ne; e++)
+			for (int k = 0; k < tcnt[2 * e]; k++) tadj[fill[tdofs[(size_t) e * nl + k]]++] = (int32_t) e;
+	}
+
 	// greedy colouring in element order: colour = smallest not used by an
 	// earlier element sharing a DOF
 	std::vector<int> color(ne, -1);
 	int ncol = 0;
 	{
 		std::vector<int64_t> stamp(64, -1);
-		for (int64_t e = 0; e < ne; e++) {
-			for (int k = 0; k < cnt[2 * e]; k++) {
-				int d = dofs[(size_t) e * nl + k];
-				for (int64_t t = dptr[d]; t < dptr[d + 1]; t++) {
-					int64_t o = dadj[t];
-					if (o < e && color[o] >= 0) {
-						if (color[o] >= (int) stamp.size()) stamp.resize(color[o] + 1, -1);
-						stamp[color[o]] = e;
-					}
+		auto mark = [&](int64_t e, const std::vector<int64_t> &ptr, const std::vector<int32_t> &adj, int d) {
+			for (int64_t t = ptr[d]; t < ptr[d + 1]; t++) {
+				int64_t o = adj[t];
+				if (o < e && color[o] >= 0) {
+					if (color[o] >= (int) stamp.size()) stamp.resize(color[o] + 1, -1);
+					stamp[color[o]] = e;
 				}
 			}
+		};
+		for (int64_t e = 0; e < ne; e++) {
+			for (int k = 0; k < cnt[2 * e]; k++) mark(e, dptr, dadj, dofs[(size_t) e * nl + k]);
+			if (two)
+				for (int k = 0; k < tcnt[2 * e]; k++) mark(e, tptr, tadj, tdofs[(size_t) e * nl + k]);
 			int c = 0;
 			while (c < (int) stamp.size() && stamp[c] == e) c++;
 			color[e] = c;
@@ -1212,18 +1254,26 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 	P.canon = canon;
 	if (canon) {
 		// canonical tables: every canonical index must occur at most once per element
-		for (int64_t e = 0; e < ne; e++) {
-			std::vector<char> seen(nl, 0);
-			for (int k = 0; k < cnt[2 * e] + cnt[2 * e + 1]; k++) {
-				int sidx = ss[(size_t) e * nl + k];
-				if (seen[sidx]) { err = "a canonical function repeats in one assembly list"; return -1; }
-				seen[sidx] = 1;
+		for (int side = 0; side < (two ? 2 : 1); side++) {
+			const std::vector<int32_t> &cn = side ? tcnt : cnt;
+			const std::vector<uint16_t> &sx = side ? tss : ss;
+			for (int64_t e = 0; e < ne; e++) {
+				std::vector<char> seen(nl, 0);
+				for (int k = 0; k < cn[2 * e] + cn[2 * e + 1]; k++) {
+					int sidx = sx[(size_t) e * nl + k];
+					if (seen[sidx]) { err = "a canonical function repeats in one assembly list"; return -1; }
+					seen[sidx] = 1;
+				}
 			}
 		}
 		P.el_vtx.resize(8 * ne);
 		P.el_id.resize(ne);
 		P.el_cdof.assign((size_t) ne * nl, -1);
 		P.el_ccoef.assign((size_t) ne * nl, 0.0);
+		if (two) {
+			P.el_tcdof.assign((size_t) ne * nl, -1);
+			P.el_tccoef.assign((size_t) ne * nl, 0.0);
+		}
 		P.el_offc.assign((size_t) ne * nl * nl, 0);
 		P.el_cnt.resize(2 * ne);
 		parallel_for(ne, [&](int64_t lo, int64_t hi) {
@@ -1238,12 +1288,18 @@ int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &P, std::string 
 					P.el_cdof[(size_t) k * nl + sidx] = dofs[(size_t) e * nl + t];
 					P.el_ccoef[(size_t) k * nl + sidx] = cf[(size_t) e * nl + t];
 				}
-				int mc = cnt[2 * e];
+				if (two)
+					for (int t = 0; t < tcnt[2 * e] + tcnt[2 * e + 1]; t++) {
+						int sidx = tss[(size_t) e * nl + t];
+						P.el_tcdof[(size_t) k * nl + sidx] = tdofs[(size_t) e * nl + t];
+						P.el_tccoef[(size_t) k * nl + sidx] = tcf[(size_t) e * nl + t];
+					}
+				int mc = cnt[2 * e], tmc = tcnt[2 * e];
 				for (int b = 0; b < mc; b++) {
 					int col = dofs[(size_t) e * nl + b], sj = ss[(size_t) e * nl + b];
 					const int32_t *c0 = &P.Ai[P.Ap[col]], *c1 = &P.Ai[P.Ap[col + 1]];
-					for (int a = 0; a < mc; a++) {
-						int row = dofs[(size_t) e * nl + a], si = ss[(size_t) e * nl + a];
+					for (int a = 0; a < tmc; a++) {
+						int row = tdofs[(size_t) e * nl + a], si = tss[(size_t) e * nl + a];
 						const int32_t *pos = std::lower_bound(c0, c1, row);
 						P.el_offc[((size_t) k * nl + si) * nl + sj] = (uint16_t) (pos - c0);
 					}

@@ -174,6 +174,14 @@ struct Plan {
 	bool canon = false;
 	std::vector<int32_t> el_cdof;            // ne x nl: DOF or -1
 	std::vector<double> el_ccoef;            // ne x nl: sign x coefficient (lifting value when DOF = -1), 0 absent
+	// a block of a system whose test space differs from the trial space
+	// (src/discretization.cc:290-325 with spaces m != n): the test space's
+	// canonical tables; the CSC columns are trial DOFs, the rows test DOFs
+	bool two_space = false;
+	int64_t nrow = 0;                        // test DOFs of a two-space plan
+	int64_t nrhs() const { return two_space ? nrow : ndof; }   // RHS length (rows)
+	std::vector<int32_t> el_tcdof;           // ne x nl: test DOF or -1
+	std::vector<double> el_tccoef;           // ne x nl: test coefficient (0 absent)
 	std::vector<uint16_t> el_offc;           // ne x nl x nl: [i][j] row position of cdof_i in column cdof_j
 
 	// element colouring: no two elements of a colour share a DOF
@@ -313,8 +321,11 @@ constexpr int kSegBatchCols = 32;
 constexpr int seg_batch_pairs(int nl) { return nl <= 27 ? 128 : 64; }
 void build_seg_tables(Plan &plan, int window);
 
+// test: the test space of a system block (nullptr: the trial space); a
+// two-space plan is canonical, at the larger of the two (uniform) orders.
+// DOFs are numbered from each space's first DOF (the plan's own numbering).
 int build_plan(const Space &sp, int nqx, int nqy, int nqz, Plan &plan, std::string &err, bool canon = false,
-               const PlanScope *scope = nullptr);
+               const PlanScope *scope = nullptr, const Space *test = nullptr);
 
 // Mixed orders: per element p_d + qn points per direction (p_plus) or qn
 // (fixed).  Elements are grouped by colour, then by kernel class, and within

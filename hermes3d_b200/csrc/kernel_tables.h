@@ -133,4 +133,8 @@ std::vector<SegSpec> &seg_table();
 // cores (one launch per colour, one CTA per SM; KernelSpec::eb = elements per batch)
 std::vector<KernelSpec> &lo_tc_table();
 
+// FP64 kernels with the reference's stock per-pair quadrature (uniform p <= 3;
+// KernelSpec::nq unused)
+std::vector<KernelSpec> &stock_table();
+
 } // namespace h3dg_tables

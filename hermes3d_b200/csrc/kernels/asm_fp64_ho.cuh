@@ -44,6 +44,8 @@ struct KArgsHO {
 	double *Ax, *rhs;
 	int *status;
 	double *gscratch;          // per-CTA global work area (kernels that keep G out of shared memory), or nullptr
+	const int32_t *tcdof;      // test side of a two-space block (ne x nl), or nullptr: the trial tables
+	const double *tccoef;
 };
 
 template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ>
@@ -73,7 +75,9 @@ struct HoShape {
 	static constexpr int S_CS = S_Y + NL;                               // NL int64 column start
 	static constexpr int S_CE = S_CS + NL;                              // NL int64 column end
 	static constexpr int S_D = S_CE + NL;                               // NL int dof (NL/2 doubles)
-	static constexpr int SMEM_DOUBLES = S_D + (NL + 1) / 2 + 2;
+	static constexpr int S_TD = S_D + (NL + 1) / 2;                     // test side of a two-space block: NL int dof
+	static constexpr int S_TC = S_TD + (NL + 1) / 2;                    //   and NL coefficients
+	static constexpr int SMEM_DOUBLES = S_TC + NL + 2;
 	static constexpr size_t SMEM_BYTES = sizeof(double) * SMEM_DOUBLES;
 };
 
@@ -168,10 +172,12 @@ __device__ __forceinline__ void ho_geometry(const KArgsHO &args, const double *t
 
 // Load vector with Dirichlet lifting, matrix-free (FP64):
 // lrhs_i = c_i (F_i - (K g)_i), posted into rhs.  U is a work area of
-// HoShape::MF doubles.
+// HoShape::MF doubles.  g: the trial side's lifting (cd < 0, value cc);
+// rows i: the test side (td, tc; the same tables unless the block has two
+// spaces).
 template <class S, int NT>
 __device__ __forceinline__ void ho_rhs(const KArgsHO &args, const double *tab, const double *G, double *U, const int *cd,
-                                       const double *cc, bool lift) {
+                                       const double *cc, const int *td, const double *tc, bool lift) {
 	constexpr int NX = S::NX, NY = S::NY, NZ = S::NZ, NL = S::NL, NQ = S::NQ;
 	constexpr int NQX = S::QX, NQY = S::QY, NQZ = S::QZ;
 	const int tid = threadIdx.x;
@@ -263,12 +269,12 @@ __device__ __forceinline__ void ho_rhs(const KArgsHO &args, const double *tab, c
 	}
 	__syncthreads();
 	for (int i = tid; i < NL; i += NT) {
-		if (cd[i] < 0) continue;
+		if (td[i] < 0) continue;                      // rows: the test functions
 		const int ab = i / NZ, c = i % NZ;
 		double s = 0.0;
 		for (int q3 = 0; q3 < NQZ; q3++)
 			s += Qw[ab * NQZ + q3] * Vz[c * NQZ + q3] + Qw[NX * NY * NQZ + ab * NQZ + q3] * Dz[c * NQZ + q3];
-		posted_add(args.rhs + cd[i], -cc[i] * s);
+		posted_add(args.rhs + td[i], -tc[i] * s);
 	}
 	__syncthreads();
 
@@ -291,6 +297,9 @@ __global__ void __launch_bounds__(NT, 1) k_assemble_fp64_ho(KArgsHO args, int64_
 	double *X = sm + S::S_X, *Mo = sm + S::S_M, *cc = sm + S::S_C, *Y = sm + S::S_Y;
 	int64_t *cs = reinterpret_cast<int64_t *>(sm + S::S_CS), *ce = reinterpret_cast<int64_t *>(sm + S::S_CE);
 	int *cd = reinterpret_cast<int *>(sm + S::S_D);
+	// test side: its own tables in a two-space block, else the trial tables
+	int *td = args.tcdof ? reinterpret_cast<int *>(sm + S::S_TD) : cd;
+	double *tc = args.tcdof ? sm + S::S_TC : cc;
 	const int tid = threadIdx.x;
 	if (!stage_tables(sm + S::S_TAB, args.tables, args.table_bytes, &bar, args.status)) return;
 	const double *Vx = tab + S::OVX, *Dx = tab + S::ODX, *Vy = tab + S::OVY, *Dy = tab + S::ODY;
@@ -298,9 +307,14 @@ __global__ void __launch_bounds__(NT, 1) k_assemble_fp64_ho(KArgsHO args, int64_
 	const bool do_rhs = args.rhs && args.lf;
 
 	for (int64_t k = kbeg + blockIdx.x; k < kend; k += gridDim.x) {
+		if (args.tcdof)
+			for (int i = tid; i < NL; i += NT) {
+				td[i] = args.tcdof[k * NL + i];
+				tc[i] = args.tccoef[k * NL + i];
+			}
 		const double cgrad = ho_element_setup<S, NT>(args, k, X, Mo, cc, cd, cs, ce, &s_nlift);
 		ho_geometry<S, NT>(args, tab, Mo, cgrad, G);
-		if (do_rhs) ho_rhs<S, NT>(args, tab, G, U, cd, cc, s_nlift > 0 && args.Ax);
+		if (do_rhs) ho_rhs<S, NT>(args, tab, G, U, cd, cc, td, tc, s_nlift > 0 && args.Ax);
 
 		// ---- matrix: chunks of the test z index c
 		if (args.Ax) {
@@ -379,12 +393,12 @@ __global__ void __launch_bounds__(NT, 1) k_assemble_fp64_ho(KArgsHO args, int64_
 						const uint16_t *offrow = args.offc + (k * NL) * NL + j;
 						for (int a = 0; a < NX; a++) {
 							const int i = a * NY * NZ + ibase;
-							if (cd[i] < 0) continue;
+							if (td[i] < 0) continue;
 							double s = 0.0;
 #pragma unroll
 							for (int q1 = 0; q1 < NQX; q1++) s += Vx[a * NQX + q1] * Z0[q1] + Dx[a * NQX + q1] * Z1[q1];
 							const int64_t pos = c0 + offrow[(int64_t) i * NL];
-							if (pos < c1) posted_add(args.Ax + pos, cc[i] * cj * s);
+							if (pos < c1) posted_add(args.Ax + pos, tc[i] * cj * s);
 							else if (c1 > c0) atomicOr(args.status, kErrBounds);   // empty: column not owned
 						}
 					}

@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(256, MINB) k_assemble_ho_oz(KArgsHO args, int6
 	for (int64_t k = kbeg + blockIdx.x; k < kend && alive; k += gridDim.x) {
 		const double cgrad = ho_element_setup<SB, NT>(args, k, X, Mo, cc, cd, cs, ce, &s_nlift);
 		ho_geometry<SB, NT>(args, tab, Mo, cgrad, G);
-		if (do_rhs) ho_rhs<SB, NT>(args, tab, G, MFw, cd, cc, s_nlift > 0 && args.Ax);
+		if (do_rhs) ho_rhs<SB, NT>(args, tab, G, MFw, cd, cc, cd, cc, s_nlift > 0 && args.Ax);
 		if (!args.Ax) continue;
 		const uint16_t *offe = args.offt + (size_t) k * NZ * S::NCOL * NB;
 

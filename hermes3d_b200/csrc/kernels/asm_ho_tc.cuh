@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(256, MINB) k_assemble_ho_tc(KArgsHO args, int6
 		// ---- FP64: set-up, geometry, load vector with lifting
 		const double cgrad = ho_element_setup<SB, NT>(args, k, X, Mo, cc, cd, cs, ce, &s_nlift);
 		ho_geometry<SB, NT>(args, tab, Mo, cgrad, G64);
-		if (do_rhs) ho_rhs<SB, NT>(args, tab, G64, MFw, cd, cc, s_nlift > 0 && args.Ax);
+		if (do_rhs) ho_rhs<SB, NT>(args, tab, G64, MFw, cd, cc, cd, cc, s_nlift > 0 && args.Ax);
 		if (!args.Ax) continue;
 		for (int i = tid; i < 7 * NQ; i += NT) G32[i] = (i < 6 * NQ || args.mass) ? (float) G64[i] : 0.0f;
 		__syncthreads();

@@ -34,7 +34,7 @@ std::vector<KernelSpec> &kernel_table() {
 		spec_warp<2, 4, 4, 4>(), spec_warp<2, 4, 4, 3>(), spec_warp<2, 4, 8, 2>(), spec_warp<2, 4, 2, 8>(),
 		spec<2, 4, 96, 1, 4, true>(), spec<2, 4, 96, 1, 6, true>(), spec<2, 4, 128, 1, 4, true>(),
 		spec<2, 4, 192, 2, 2, true>(), spec<2, 4, 192, 2, 3, true>(),
-		spec<2, 5, 96, 1, 8>(), spec<2, 5, 192, 2, 4>(),
+		spec<2, 5, 96, 1, 8>(), spec<2, 5, 192, 2, 4>(), spec<2, 6, 96, 1, 4>(),
 		spec<3, 4, 256, 1, 3>(), spec<3, 5, 256, 1>(), spec<3, 5, 256, 1, 3>(), spec<3, 5, 512, 2>(),
 		spec<3, 5, 256, 1, 1, true>(), spec<3, 5, 256, 1, 2, true>(),
 		spec<3, 6, 256, 1, 2>(),

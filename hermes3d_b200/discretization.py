@@ -63,10 +63,12 @@ class H1Space:
     def set_uniform_order(self, order):
         px, py, pz = (order, order, order) if np.isscalar(order) else order
         capi.call("h3dg_space_set_uniform_order", self.handle, int(px), int(py), int(pz))
+        self.orders = ("uniform", (int(px), int(py), int(pz)))
 
     def set_element_orders(self, orders):
         o = np.ascontiguousarray(orders, dtype=np.int32).reshape(-1, 3)
         capi.call("h3dg_space_set_element_orders", self.handle, capi.ptr(o, C.c_int32), len(o))
+        self.orders = ("elements", o.tobytes())
 
     def assign_dofs(self, first_dof=0, stride=1):
         n = C.c_int64()
@@ -203,6 +205,15 @@ class Discretization:
         self.space = space
         capi.call("h3dg_disc_set_space", self.handle, space.handle)
 
+    def set_test_space(self, space):
+        """Block (m, n) of a system whose test space differs from the trial
+        space set by set_spaces (no reference counterpart as a call: the
+        reference's Discretization does this per block inside assemble).
+        Rows then come from ``space``, each space counted from its own first
+        DOF; FP64.  None: one space."""
+        self._test_space = space
+        capi.call("h3dg_disc_set_test_space", self.handle, None if space is None else space.handle)
+
     def set_pss(self, *args):
         pass  # the precalculated shapeset is the device's 1D tables
 
@@ -275,9 +286,14 @@ class Discretization:
                   C.c_void_p(stream.cuda_stream))
         return {"l2_error": out[0], "h1_error": out[1], "l2_norm": out[2], "h1_norm": out[3]}
 
-    def set_quadrature(self, points=None, p_plus=None):
-        """Fixed Gauss points per direction, or p_d + p_plus per direction."""
-        if points is not None:
+    def set_quadrature(self, points=None, p_plus=None, stock=False):
+        """Fixed Gauss points per direction, p_d + p_plus per direction, or
+        (stock=True) the rule the reference's stock forms pick: each pair
+        with order(u) + order(v) + 1 per direction, the load vector with
+        order 24 (src/integrals/h1.h:115-177; uniform orders 1..3, FP64)."""
+        if stock:
+            self._quad = (capi.QUAD_STOCK, 0)
+        elif points is not None:
             self._quad = (capi.QUAD_FIXED, int(points))
         else:
             self._quad = (capi.QUAD_P_PLUS, int(p_plus))
@@ -321,7 +337,13 @@ class Discretization:
             matrix.Ax = np.zeros(self.nnz, np.float64)
             matrix.ndofs = self.ndof
         if rhs is not None:
-            rhs.v = np.zeros(self.ndof, np.float64)
+            rhs.v = np.zeros(self.nrows, np.float64)
+
+    @property
+    def nrows(self):
+        """Rows of the plan: the test space's DOFs (== ndof for one space)."""
+        ts = getattr(self, "_test_space", None)
+        return ts.ndof if ts is not None and ts is not self.space else self.ndof
 
     def assemble(self, matrix: Optional[UMFPackMatrix] = None, rhs: Optional[UMFPackVector] = None,
                  precision: int = capi.PREC_FP64):
@@ -456,14 +478,18 @@ class Discretization:
 
 class SystemDiscretization:
     """Discretization with several equations (src/discretization.h:39-101 with
-    neq > 1; assembly src/discretization.cc:232-343) for equations whose spaces
-    are identical (same mesh, orders and boundary conditions) and numbered one
-    after another (space i assigned with first_dof = i * ndof).  Block (m, n)
-    holds the form of test space m and trial space n.  Each block is assembled
-    by the device kernels on the common single-space pattern and placed into
-    the system arrays on the device; the Dirichlet lifting of the trial space
-    goes to the rows of the test space.  As in the reference, equation m's RHS
-    is written only when it has a linear form."""
+    neq > 1; assembly src/discretization.cc:232-343).  Space i is numbered
+    after the spaces before it (assign_dofs(first_dof = sum of their DOF
+    counts)), as in the reference's system tests.  Block (m, n) holds the form
+    of test space m and trial space n; the Dirichlet lifting of the trial
+    space goes to the rows of the test space; equation m's RHS is written only
+    when it has a linear form.  Each block is assembled by the device kernels
+    and placed into the system arrays on the device:
+      * identical spaces (same orders and DOF counts; the caller gives them the
+        same boundary conditions): every block on the first space's pattern,
+        with any kernel the single space allows (mixed orders, refinement);
+      * spaces that differ (orders): block (m, n) as a two-space plan (rows of
+        space m, columns of space n, FP64; uniform orders per space)."""
 
     def __init__(self, device=0):
         self.device = device
@@ -483,11 +509,14 @@ class SystemDiscretization:
     def set_spaces(self, *spaces):
         if len(spaces) != self.neq:
             raise capi.H3dgError(1, "one space per equation")
-        nd = spaces[0].ndof
-        for i, sp in enumerate(spaces):
-            if sp.ndof != nd or sp.mesh is not spaces[0].mesh or getattr(sp, "first_dof", None) != i * nd:
-                raise capi.H3dgError(1, "the spaces must be identical and numbered one after another")
+        off = 0
+        for sp in spaces:
+            if sp.mesh is not spaces[0].mesh or getattr(sp, "first_dof", None) != off:
+                raise capi.H3dgError(1, "the spaces share one mesh and are numbered one after another")
+            off += sp.ndof
         self.spaces = list(spaces)
+        self.identical = all(sp.ndof == spaces[0].ndof and getattr(sp, "orders", None) == getattr(spaces[0], "orders", None)
+                             for sp in spaces)
 
     def set_bilinear_form(self, i, j, form, coef=None):
         if not isinstance(form, BilinearForm):
@@ -502,64 +531,71 @@ class SystemDiscretization:
     def set_quadrature(self, points=None, p_plus=None):
         self._quad = ("points", int(points)) if points is not None else ("p_plus", int(p_plus))
 
-    def _base(self, form, coef, lf):
+    def _base(self, m, n, form, coef, lf):
+        """Single-space discretisation of block (m, n) (n < 0: a linear form
+        alone) and its pattern, in the block's own numbering."""
         d = Discretization(self.device)
-        d.set_spaces(self.spaces[0])
+        if self.identical:
+            d.set_spaces(self.spaces[0])
+        else:
+            d.set_spaces(self.spaces[n if n >= 0 else m])
+            if n >= 0 and n != m:
+                d.set_test_space(self.spaces[m])
         d.set_bilinear_form(form, coef)
         d.set_linear_form(lf)
         if self._quad[0] == "points":
             d.set_quadrature(points=self._quad[1])
         else:
             d.set_quadrature(p_plus=self._quad[1])
-        m = UMFPackMatrix()
-        d.create(m, UMFPackVector())
-        return d, m
+        bm = UMFPackMatrix()
+        d.create(bm, UMFPackVector())
+        return d, bm
 
     def create(self, matrix=None, rhs=None):
-        """Discretization::create: the pattern of every block with a form."""
-        nd = self.spaces[0].ndof
-        self.nd1 = nd
-        # one single-space discretisation per block; the first block of row m
-        # carries F_m, the others contribute their lifting only (F = 0)
+        """Discretization::create: the pattern of every block with a form.
+        System column (n, j) holds the rows of the blocks (m, n), m ascending."""
+        if not self.identical and any(getattr(sp, "orders", ("uniform",))[0] != "uniform" for sp in self.spaces):
+            raise capi.H3dgError(1, "spaces that differ need uniform orders")
+        offs = [sp.first_dof for sp in self.spaces]
+        nds = [sp.ndof for sp in self.spaces]
+        self._offs, self._nds = offs, nds
+        # one discretisation per block; the first block of row m carries F_m,
+        # the others contribute their lifting only (F = 0)
         self._blocks = []
-        pattern = None
+        pats = {}
         for m in range(self.neq):
             row = [n for n in range(self.neq) if (m, n) in self.forms]
             lf = self.lforms.get(m)
             for k, n in enumerate(row):
                 form, coef = self.forms[(m, n)]
                 blf = (lf if k == 0 else int_F_v(0.0)) if lf is not None else None
-                d, bm = self._base(form, coef, blf)
+                d, bm = self._base(m, n, form, coef, blf)
                 self._blocks.append((m, n, d))
-                pattern = pattern or bm
+                pats[(m, n)] = (bm.Ap, bm.Ai)
             if lf is not None and not row:
-                d, bm = self._base(int_grad_u_grad_v, None, lf)
+                d, bm = self._base(m, -1, int_grad_u_grad_v, None, lf)
                 self._blocks.append((m, -1, d))
-                pattern = pattern or bm
-        if pattern is None:
-            pattern = self._base(int_grad_u_grad_v, None, None)[1]
-        Ap0, Ai0 = pattern.Ap, pattern.Ai
-        counts = np.diff(Ap0)
-        # system column n * nd + j: the rows of the blocks (m, n), m ascending
-        pres = [[(m, n) in self.forms for n in range(self.neq)] for m in range(self.neq)]
-        colcnt = np.zeros(self.neq * nd, np.int64)
-        for n in range(self.neq):
-            colcnt[n * nd:(n + 1) * nd] = counts * sum(pres[m][n] for m in range(self.neq))
-        Ap = np.zeros(self.neq * nd + 1, np.int64)
+        ntot = int(sum(nds))
+        colcnt = np.zeros(ntot, np.int64)
+        for (m, n), (Apb, Aib) in pats.items():
+            colcnt[offs[n]:offs[n] + nds[n]] += np.diff(Apb)
+        Ap = np.zeros(ntot + 1, np.int64)
         np.cumsum(colcnt, out=Ap[1:])
         Ai = np.zeros(Ap[-1], np.int32)
         self._pos = {}
         for n in range(self.neq):
-            off = np.zeros(nd, np.int64)
+            off = np.zeros(nds[n], np.int64)
             for m in range(self.neq):
-                if not pres[m][n]:
+                if (m, n) not in pats:
                     continue
-                start = Ap[n * nd:(n + 1) * nd] + off
-                idx = np.repeat(start - Ap0[:-1], counts) + np.arange(Ap0[-1])
-                Ai[idx] = Ai0 + m * nd
+                Apb, Aib = pats[(m, n)]
+                counts = np.diff(Apb)
+                start = Ap[offs[n]:offs[n] + nds[n]] + off
+                idx = np.repeat(start - Apb[:-1], counts) + np.arange(Apb[-1])
+                Ai[idx] = Aib + offs[m]
                 self._pos[(m, n)] = idx
                 off += counts
-        self.ndof, self.nnz = self.neq * nd, int(Ap[-1])
+        self.ndof, self.nnz = ntot, int(Ap[-1])
         self.Ap, self.Ai = Ap, Ai
         if matrix is not None:
             matrix.Ap, matrix.Ai = Ap.copy(), Ai.copy()
@@ -571,7 +607,6 @@ class SystemDiscretization:
     def assemble_device(self, Ax, rhs=None):
         """Assemble into torch CUDA float64 tensors (system layout), block by block."""
         import torch
-        nd = self.nd1
         dev = Ax.device if Ax is not None else rhs.device
         if Ax is not None:
             Ax.zero_()
@@ -579,7 +614,7 @@ class SystemDiscretization:
             rhs.zero_()
         for m, n, d in self._blocks:
             ax_b = torch.empty(d.nnz, dtype=torch.float64, device=dev) if (Ax is not None and n >= 0) else None
-            rhs_b = (torch.empty(nd, dtype=torch.float64, device=dev)
+            rhs_b = (torch.empty(self._nds[m], dtype=torch.float64, device=dev)
                      if (rhs is not None and self.lforms.get(m) is not None) else None)
             if ax_b is None and rhs_b is None:
                 continue
@@ -590,7 +625,7 @@ class SystemDiscretization:
                     self._pos[key] = torch.as_tensor(self._pos[(m, n)], device=dev)
                 Ax.index_add_(0, self._pos[key], ax_b)     # each system entry belongs to one block
             if rhs_b is not None:
-                rhs[m * nd:(m + 1) * nd] += rhs_b
+                rhs[self._offs[m]:self._offs[m] + self._nds[m]] += rhs_b
 
     def assemble(self, matrix=None, rhs=None):
         import torch

@@ -66,6 +66,7 @@ typedef int h3dg_status;
 /* volume quadrature: n Gauss points per direction, or p_d + n per direction */
 #define H3DG_QUAD_FIXED   0
 #define H3DG_QUAD_P_PLUS  1
+#define H3DG_QUAD_STOCK   2   /* the reference's stock rule: per pair order(u) + order(v) + 1, int_F_v order 24 */
 
 /* arithmetic of the element-matrix contraction */
 #define H3DG_PREC_FP64    0
@@ -143,6 +144,15 @@ h3dg_status h3dg_disc_create(h3dg_disc **disc, int device);
 h3dg_status h3dg_disc_destroy(h3dg_disc *disc);
 /* set_spaces(1, &space) + set_pss (src/discretization.cc:102-134) */
 h3dg_status h3dg_disc_set_space(h3dg_disc *disc, h3dg_space *space);
+/* Block (m, n) of a multi-equation system whose test space (equation m)
+ * differs from the trial space (equation n) (Discretization::set_spaces with
+ * neq > 1, src/discretization.cc:290-325): the next create_pattern plans the
+ * block with rows from the test space and columns from the trial space, each
+ * counted from its own first DOF; the trial space's Dirichlet lifting goes to
+ * the test rows.  nullptr (or the trial space): one space.  FP64, one mesh,
+ * uniform orders per space, no refinement, partition, surface forms or stock
+ * rule (H3DG_ERR_INVALID_ARG at create_pattern). */
+h3dg_status h3dg_disc_set_test_space(h3dg_disc *disc, h3dg_space *test);
 /* set_bilinear_form(0, 0, form) (src/discretization.cc:136-148); elem_coef: one value per
  * element id (ne values, multiplies the grad-grad term), or NULL for 1 */
 h3dg_status h3dg_disc_set_bilinear_form(h3dg_disc *disc, int form, const double *elem_coef, int64_t ne);
@@ -173,8 +183,13 @@ h3dg_status h3dg_disc_norms(h3dg_disc *disc, const double *d_sol, int exact, dou
  * linear form.  Set before create_pattern; not supported on refined meshes. */
 h3dg_status h3dg_disc_set_surface_forms(h3dg_disc *disc, int bilinear, int linear, const double *g, int ng);
 /* quadrature of the forms: mode H3DG_QUAD_FIXED (n points per direction) or
- * H3DG_QUAD_P_PLUS (p_d + n points per direction); the reference's forms fix the
- * order inside the form (tests/integrals/hex-h1-real/h1-hex-real.cc:55-103) */
+ * H3DG_QUAD_P_PLUS (p_d + n points per direction), as the explicit-order forms
+ * of tests/integrals/hex-h1-real/h1-hex-real.cc:55-103 fix it; or
+ * H3DG_QUAD_STOCK (n ignored), the rule of the stock int_grad_u_grad_v /
+ * int_u_v / int_F_v (src/integrals/h1.h:115-177): each pair integrated with
+ * order(u) + order(v) + 1 per direction, the load vector with order 24.
+ * STOCK: uniform orders 1..3, FP64, no refinement or surface forms
+ * (H3DG_ERR_INVALID_ARG at create_pattern otherwise). */
 h3dg_status h3dg_disc_set_quadrature(h3dg_disc *disc, int mode, int n);
 /* Discretization::create (src/discretization.cc:164-230) + UMFPackMatrix::alloc
  * (src/linsolver/umfpack.cc:46-71): builds the CSC pattern and the device plan */

@@ -26,7 +26,7 @@
 //       [--source none|one|sin|poly] [--bc dirichlet0|dirichlet_poly|natural]
 //       [--refine REF.bin] [--repeat R] [--no-asm] [--elem-dump]
 //       [--surf-uv] [--surf-g g1,...,g6] [--natural-markers m1,m2,...]
-//       [--sys k11,k12,k21,k22 (none|gg|ggm|mass) --source2 S]
+//       [--sys k11,k12,k21,k22 (none|gg|ggm|mass) --source2 S [--p2 P2]]
 //
 // Output (little-endian binary, all counts int64):
 //   "H3DOUT01" ndof nnz Ap[ndof+1](i32) Ai[nnz](i32) Ax[nnz](f64) rhs[ndof](f64)
@@ -293,6 +293,7 @@ static double now() {
 int main(int argc, char **argv) {
 	const char *mesh_fn = NULL, *out_fn = NULL, *orders_fn = NULL, *coef_fn = NULL, *refine_fn = NULL;
 	int p = 2, repeat = 1;
+	int p2 = 0;              // uniform order of the second space of a system (0: the first space's orders)
 	bool qref = false, do_asm = true, elem_dump = false, surf_uv = false, surf_g = false;
 	std::string sys_kinds;   // two-equation system: block kinds (none/gg/ggm/mass) row-major
 	for (int i = 1; i < argc; i++) {
@@ -304,6 +305,7 @@ int main(int argc, char **argv) {
 		else if (a == "--gradcoef") { coef_fn = v; i++; }
 		else if (a == "--refine") { refine_fn = v; i++; }
 		else if (a == "--p") { p = atoi(v); i++; }
+		else if (a == "--p2") { p2 = atoi(v); i++; }
 		else if (a == "--repeat") { repeat = atoi(v); i++; }
 		else if (a == "--mass") g_mass = true;
 		else if (a == "--no-asm") do_asm = false;
@@ -444,13 +446,15 @@ int main(int argc, char **argv) {
 	FOR_ALL_ACTIVE_ELEMENTS(idx, &mesh)
 		space.set_element_order(idx, order3_t(g_orders[3 * (idx - 1)], g_orders[3 * (idx - 1) + 1], g_orders[3 * (idx - 1) + 2]));
 	int ndof = space.assign_dofs();
-	// second, identical space of a two-equation system, numbered after the first
+	// second space of a two-equation system, numbered after the first: the
+	// first space's orders, or uniform --p2
 	H1Space space2(&mesh, &shapeset);
 	if (!sys_kinds.empty()) {
 		space2.set_bc_types(bc_types);
 		space2.set_bc_values(bc_values);
 		FOR_ALL_ACTIVE_ELEMENTS(idx, &mesh)
-			space2.set_element_order(idx, order3_t(g_orders[3 * (idx - 1)], g_orders[3 * (idx - 1) + 1], g_orders[3 * (idx - 1) + 2]));
+			space2.set_element_order(idx, p2 > 0 ? order3_t(p2, p2, p2)
+			                                     : order3_t(g_orders[3 * (idx - 1)], g_orders[3 * (idx - 1) + 1], g_orders[3 * (idx - 1) + 2]));
 		ndof += space2.assign_dofs(ndof);
 	}
 	double t_space = now() - t0;

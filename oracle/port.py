@@ -33,6 +33,8 @@ def lib():
         L.h3d_port_pattern.argtypes = [C.c_int64, pi64, pi32, C.c_int64, pi64, pi32, pi64]
         L.h3d_port_assemble.argtypes = [C.c_int64, pd, C.c_int64, pi64, pi32, pi64, pi64, pi32, pd, C.c_int, pd, C.c_int,
                                         C.c_double, C.c_int64, pi64, pi32, pd, pd]
+        L.h3d_port_assemble_stock.argtypes = [C.c_int64, pd, C.c_int64, pi64, pi64, pi64, pi32, pd, C.c_int, pd, C.c_int,
+                                              C.c_double, C.c_int64, pi64, pi32, pd, pd]
         L.h3d_port_element_matrix.argtypes = [pd, C.c_int, C.c_int, C.c_int, C.c_int, pi64, C.c_int, C.c_double, pd]
         L.h3d_port_element_rows.argtypes = [pd, C.c_int, C.c_int, C.c_int, C.c_int, pi64, C.c_int, pi32, C.c_int, C.c_double, pd]
         _lib = L
@@ -102,6 +104,23 @@ def assemble(xyz, hex0, nq, al, ndof, Ap, Ai, mass=False, gradcoef=None, lf=1, l
                                 _p(Ai, C.c_int32), _p(Ax, C.c_double), _p(rhs, C.c_double))
     if r != 0:
         raise RuntimeError("port assemble failed (%d)" % r)
+    return Ax, rhs
+
+
+def assemble_stock(xyz, hex0, al, ndof, Ap, Ai, mass=False, gradcoef=None, lf=1, lf_value=1.0):
+    """Numeric assembly with the reference's stock per-pair quadrature."""
+    xyz = np.ascontiguousarray(xyz, np.float64)
+    hex0 = np.ascontiguousarray(hex0, np.int64)
+    ptr, idx, dof, coef = al
+    Ax = np.zeros(len(Ai), np.float64)
+    rhs = np.zeros(ndof, np.float64)
+    gc = None if gradcoef is None else np.ascontiguousarray(gradcoef, np.float64)
+    r = lib().h3d_port_assemble_stock(len(xyz), _p(xyz, C.c_double), len(hex0), _p(hex0, C.c_int64),
+                                      _p(ptr, C.c_int64), _p(idx, C.c_int64), _p(dof, C.c_int32), _p(coef, C.c_double),
+                                      int(mass), _p(gc, C.c_double), int(lf), float(lf_value), ndof, _p(Ap, C.c_int64),
+                                      _p(Ai, C.c_int32), _p(Ax, C.c_double), _p(rhs, C.c_double))
+    if r != 0:
+        raise RuntimeError("port assemble_stock failed (%d)" % r)
     return Ax, rhs
 
 

@@ -361,3 +361,90 @@ int h3d_port_element_rows(const double *X, int nqx, int nqy, int nqz, int cnt, c
 	elem_free(&c);
 	return 0;
 }
+
+/* ---- the reference's stock quadrature (src/integrals/h1.h:115-177):
+ * int_grad_u_grad_v and int_u_v integrate each pair with the order
+ * order(u) + order(v) + (1,1,1) per direction (the inverse map's order of a
+ * hexahedron, src/refmap.cc:140-142), capped at 24 (order.h limit()); the 1D
+ * order of Lobatto function k is max(k, 1) (src/shapeset/lobatto.cc:23); a
+ * rule of order o has o / 2 + 1 Gauss points (src/quadstd.cc:179-205).
+ * int_F_v uses the maximal order 24 (13 points) in every direction. */
+static int stock_ord1d(int k) { return k < 2 ? 1 : k; }
+static int stock_npts(int o) { return (o > 24 ? 24 : o) / 2 + 1; }
+
+int h3d_port_assemble_stock(int64_t nv, const double *xyz, int64_t ne, const int64_t *hex, const int64_t *al_ptr,
+                            const int64_t *al_idx, const int32_t *al_dof, const double *al_coef, int mass,
+                            const double *gradcoef, int lf, double lf_value, int64_t ndof, const int64_t *Ap,
+                            const int32_t *Ai, double *Ax, double *rhs) {
+	(void) nv;
+	if (Ax) memset(Ax, 0, sizeof(double) * Ap[ndof]);
+	if (rhs) memset(rhs, 0, sizeof(double) * ndof);
+	for (int64_t e = 0; e < ne; e++) {
+		double X[24];
+		for (int v = 0; v < 8; v++)
+			for (int r = 0; r < 3; r++) X[3 * v + r] = xyz[3 * hex[8 * e + v] + r];
+		int cnt = (int) (al_ptr[e + 1] - al_ptr[e]);
+		const int64_t *idx = al_idx + al_ptr[e];
+		const int32_t *dof = al_dof + al_ptr[e];
+		const double *coef = al_coef + al_ptr[e];
+		int (*ord)[3] = malloc(sizeof(int[3]) * (cnt > 0 ? cnt : 1));
+		for (int i = 0; i < cnt; i++) {
+			int ind[3], ori[3];
+			decompose(idx[i], ind, ori);
+			for (int d = 0; d < 3; d++) ord[i][d] = stock_ord1d(ind[d]);
+		}
+		/* one cache per rule triple met (2..13 points per direction) */
+		ElemCache *cache[14 * 14 * 14];
+		memset(cache, 0, sizeof(cache));
+		double gc = gradcoef ? gradcoef[e] : 1.0;
+		double *lsm = calloc((size_t) cnt * cnt + 1, sizeof(double));
+		double *lrhs = calloc((size_t) cnt + 1, sizeof(double));
+		int rc = 0;
+		for (int j = 0; j < cnt && !rc; j++)
+			for (int i = 0; i < cnt && !rc; i++) {
+				if (dof[i] < 0) continue;
+				int n[3];
+				for (int d = 0; d < 3; d++) n[d] = stock_npts(ord[j][d] + ord[i][d] + 1);
+				ElemCache **cp = &cache[(n[0] * 14 + n[1]) * 14 + n[2]];
+				if (!*cp) {
+					*cp = malloc(sizeof(ElemCache));
+					if (!*cp || elem_cache(X, n[0], n[1], n[2], cnt, idx, *cp) != 0) { rc = -1; break; }
+				}
+				double bi = biform(*cp, j, i, mass, gc) * coef[j] * coef[i];
+				if (dof[j] >= 0) lsm[(size_t) i * cnt + j] += bi;
+				else lrhs[i] -= bi;
+			}
+		if (!rc && Ax)
+			for (int i = 0; i < cnt && !rc; i++)
+				for (int j = 0; j < cnt; j++) {
+					double v = lsm[(size_t) i * cnt + j];
+					if (v != 0.0 && dof[i] >= 0 && dof[j] >= 0)
+						if (insert_value(Ai + Ap[dof[j]], Ax + Ap[dof[j]], Ap[dof[j] + 1] - Ap[dof[j]], dof[i], v) != 0) {
+							rc = -2;
+							break;
+						}
+				}
+		if (!rc && rhs && lf) {
+			ElemCache c13;
+			if (elem_cache(X, 13, 13, 13, cnt, idx, &c13) != 0) rc = -1;
+			else {
+				for (int i = 0; i < cnt; i++)
+					if (dof[i] >= 0) lrhs[i] += liform(&c13, i, lf, lf_value) * coef[i];
+				for (int i = 0; i < cnt; i++)
+					if (dof[i] >= 0) rhs[dof[i]] += lrhs[i];
+				elem_free(&c13);
+			}
+		}
+		for (int k = 0; k < 14 * 14 * 14; k++)
+			if (cache[k]) {
+				elem_free(cache[k]);
+				free(cache[k]);
+			}
+		free(lsm);
+		free(lrhs);
+		free(ord);
+		if (rc) return rc;
+	}
+	return 0;
+}
+

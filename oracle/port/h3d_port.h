@@ -33,6 +33,14 @@ int h3d_port_assemble(int64_t nv, const double *xyz, int64_t ne, const int64_t *
                       int mass, const double *gradcoef, int lf, double lf_value, int64_t ndof, const int64_t *Ap,
                       const int32_t *Ai, double *Ax, double *rhs);
 
+/* The same with the reference's stock quadrature: each pair (u, v) of
+ * grad.grad / mass integrated with order(u) + order(v) + 1 per direction,
+ * int F v with the maximal order 24 (src/integrals/h1.h:115-177). */
+int h3d_port_assemble_stock(int64_t nv, const double *xyz, int64_t ne, const int64_t *hex, const int64_t *al_ptr,
+                            const int64_t *al_idx, const int32_t *al_dof, const double *al_coef, int mass,
+                            const double *gradcoef, int lf, double lf_value, int64_t ndof, const int64_t *Ap,
+                            const int32_t *Ai, double *Ax, double *rhs);
+
 /* Element matrix of one element in the assembly-list basis (cnt x cnt,
  * row = test, no coefficients applied): for element-level parity. */
 int h3d_port_element_matrix(const double *X /* 8 x 3 */, int nqx, int nqy, int nqz, int cnt, const int64_t *idx,

@@ -66,6 +66,9 @@ def disc_of(g, sp, device=0):
         d.set_linear_form(h.int_F_v("sin"))
     elif src == "poly":
         d.set_linear_form(h.int_F_v(-6.0))
+    if p["qmode"] == "ref":                         # the reference's stock per-pair rule
+        d.set_quadrature(stock=True)
+        return d
     kind, n = quad_of(g)
     if kind == "fixed":
         d.set_quadrature(points=n)
@@ -184,7 +187,8 @@ def load_system(name):
 
 
 def system_problem(g, device=0):
-    """Two identical spaces and the block forms / sources of a system fixture."""
+    """Two spaces (identical, or the second of uniform order p2) and the
+    block forms / sources / rule of a system fixture."""
     p = g["params"]
     mesh = mesh_of(g)
     mesh.ugh()
@@ -196,7 +200,7 @@ def system_problem(g, device=0):
             sp.set_bc_types(lambda m: h.BC_NATURAL)
         if p.get("bc") == "dirichlet_poly":
             sp.set_bc_values(lambda m, x, y, z: x * x + y * y + z * z)
-        sp.set_uniform_order(p["p"])
+        sp.set_uniform_order(p.get("p2") or p["p"] if i == 1 else p["p"])
         nd += sp.assign_dofs(nd)
         spaces.append(sp)
     d = h.SystemDiscretization(device)
@@ -209,7 +213,11 @@ def system_problem(g, device=0):
     src = {"one": h.int_F_v(1.0), "sin": h.int_F_v("sin"), "poly": h.int_F_v(-6.0), "none": None}
     d.set_linear_form(0, src[p.get("source", "one")])
     d.set_linear_form(1, src[p.get("source2", "none")])
-    d.set_quadrature(p_plus=2)
+    kind, n = p.get("qmode", "pplus:2").split(":")
+    if kind == "fixed":
+        d.set_quadrature(points=int(n))
+    else:
+        d.set_quadrature(p_plus=int(n))
     return mesh, spaces, d
 
 
@@ -249,3 +257,15 @@ def highorder_problem(g, device=0):
     kind, n = quad_of(g)
     d.set_quadrature(p_plus=n) if kind == "pplus" else d.set_quadrature(points=n)
     return mesh, sp, d
+
+
+def stock_names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "stock", "*.npz")))
+
+
+def load_stock(name):
+    z = np.load(os.path.join(GOLDEN, "stock", name + ".npz"), allow_pickle=False)
+    d = {k: z[k] for k in z.files}
+    d["params"] = ast.literal_eval(str(d["params"]))
+    return d
+

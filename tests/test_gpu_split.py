@@ -106,10 +106,12 @@ def test_split_is_deterministic_and_close_to_fp64(gpu, prec):
     assert not np.array_equal(a, b)
 
 
-def test_split_low_order_uses_fp64(gpu):
-    """Below the high-order threshold the FP64 kernels are the faster choice;
-    PREC_TF32X3 then returns the FP64 matrix."""
-    g = load("p2_c2_forms")
+def test_split_order_3_uses_fp64(gpu):
+    """p = 3 has no batched tensor-core kernel and is below the high-order
+    threshold, where the FP64 kernels are the faster choice: PREC_TF32X3 then
+    returns the FP64 matrix.  (p <= 2 takes the batched kernel,
+    tests/test_gpu_split_low_order.py.)"""
+    g = load("perm_p3_mass_sin")
     sp = space_of(g)
     d = disc_of(g, sp)
     M, V = h.UMFPackMatrix(), h.UMFPackVector()
