@@ -540,6 +540,44 @@ def run_sweep(args):
     return 0
 
 
+def run_geometry(args):
+    """Kernel (a) alone: reference-map geometry (signed determinant, transposed
+    inverse Jacobian, physical point: 13 doubles = 104 bytes per point) at the
+    C2 workload's 4^3 Gauss points of every element, device time with CUDA
+    events, output 1.7 GB (> L2).  Achieved HBM = (written + read bytes) / time
+    against the measured copy bandwidth.  One JSON line; not the headline."""
+    import torch
+    import hermes3d_b200 as h
+    torch.cuda.set_device(0)
+    mesh, sp, d = build_problem(h, 0, 0, side=args.side, workload="c2")
+    ne, nq = mesh.num_elements, WORKLOADS["c2"]["nq"] ** 3
+    dev = torch.device("cuda", 0)
+    jac = torch.empty(ne * nq, dtype=torch.float64, device=dev)
+    irm = torch.empty(9 * ne * nq, dtype=torch.float64, device=dev)
+    xyz = torch.empty(3 * ne * nq, dtype=torch.float64, device=dev)
+    for _ in range(max(3, args.warmup)):
+        d.geometry(jac, irm, xyz)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        d.geometry(jac, irm, xyz)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    written = 104 * ne * nq
+    read = 24 * (len(mesh.xyz)) + 32 * ne + 4 * ne       # coordinates, connectivity, element ids
+    peak, src = peaks()
+    achieved = (written + read) / (ms * 1e-3) / 1e9
+    print(json.dumps({"metric": "geometry kernel (a): points/s and HBM GB/s", "value": ne * nq / (ms * 1e-3),
+                      "unit": "points/s", "n_gpus": 1, "steps": args.steps, "ms_per_step": ms,
+                      "config": {"workload": WORKLOADS["c2"]["desc"], "points_per_element": nq, "elements": ne},
+                      "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                   "frac": achieved / peak, "bytes_per_step": written + read,
+                                   "peak_source": src}}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -560,7 +598,10 @@ def main():
     ap.add_argument("--adjoint", action="store_true", help="C5 adjoint line (16 fields) instead of an assembly line")
     ap.add_argument("--sweep", action="store_true", help="orders 1..8: FP64 against both split precisions")
     ap.add_argument("--sweep-orders", default="1,2,3,4,5,6,7,8", help="orders of --sweep")
+    ap.add_argument("--geometry", action="store_true", help="geometry kernel (a) alone on the C2 mesh: HBM GB/s")
     args = ap.parse_args()
+    if args.geometry:
+        return run_geometry(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.adjoint:
