@@ -1890,9 +1890,11 @@ h3dg_status h3dg_disc_geometry(h3dg_disc *disc, double *d_jac, double *d_irm, do
 	g.jac = d_jac;
 	g.irm = d_irm;
 	g.xphys = d_xyz;
-	int64_t total = P.ne * (int64_t) P.nqx * P.nqy * P.nqz;
-	if (total == 0) return H3DG_OK;
-	h3dg::k_geometry<<<(unsigned) ((total + 255) / 256), 256, 0, (cudaStream_t) stream>>>(g);
+	const int nq = P.nqx * P.nqy * P.nqz;
+	if (P.ne == 0 || nq == 0) return H3DG_OK;
+	// whole elements per block, as the kernel takes them
+	const int epb = nq >= h3dg::kGeomThreads ? 1 : std::min(h3dg::kGeomThreads / nq, h3dg::kGeomMaxElems);
+	h3dg::k_geometry<<<(unsigned) ((P.ne + epb - 1) / epb), h3dg::kGeomThreads, 0, (cudaStream_t) stream>>>(g);
 	H3DG_CUDA_TRY(cudaGetLastError());
 	disc->last_launches = 1;
 	return H3DG_OK;
