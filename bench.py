@@ -385,8 +385,9 @@ def run_adjoint(args):
         out.copy_(gr, non_blocking=True)
         torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - c0) * 1e3 / nrep
-    # forward (16 assemblies through the torch.autograd binding) + backward, for context;
-    # the first call also uploads the pattern for the transposed products (not timed)
+    # forward + backward through the torch.autograd binding, for context: the forward
+    # is one matrix-free adjoint launch for all fields (its gradient is the backward's)
+    # plus the source vector, assembled on the first call (not timed)
     for rep in range(2):
         gg = g.clone().requires_grad_(True)
         torch.cuda.synchronize()

@@ -232,6 +232,7 @@ class Discretization:
         capi.call("h3dg_disc_set_bilinear_form", self.handle, kind,
                   capi.ptr(c, C.c_double), 0 if c is None else len(c))
         self._coef = c
+        self._bf_kind = kind
         self._sbf = surf
         self._set_surface()
 
@@ -239,6 +240,7 @@ class Discretization:
         """set_linear_form(0, lf, surf): ``surf`` = surf_int_G_v(g) or None."""
         if surf is not None and not isinstance(surf, SurfaceLinearForm):
             raise UnsupportedForm(4, "surface form %r is not one of the device forms" % (surf,))
+        self._lf = form
         self._slf = surf
         self._set_surface()
         if form is None:

@@ -30,7 +30,7 @@ def _problem(n=3, p=3, nq=5, lifting=False, seed=0):
 @pytest.mark.parametrize("lifting", [False, True])
 def test_adjoint_matches_central_differences(gpu, lifting):
     import torch
-    from hermes3d_b200.autograd import assembly_energy, energy
+    from hermes3d_b200.autograd import assembly_energy, energy, energy_assembled
     mesh, sp, d = _problem(lifting=lifting)
     nf, ne = 2, mesh.num_elements
     rng = np.random.default_rng(5)
@@ -38,6 +38,10 @@ def test_adjoint_matches_central_differences(gpu, lifting):
     u = torch.tensor(rng.normal(0, 1, (nf, sp.ndof)), device="cuda")
     lam = torch.tensor(rng.normal(0, 1, (nf, sp.ndof)), device="cuda")
     L = assembly_energy(g, u, lam, d)
+    # the matrix-free forward against the definition (K(a) and f(a) assembled)
+    La = energy_assembled(d, g.detach(), u, lam)
+    assert torch.allclose(L.detach(), La, rtol=1e-12, atol=1e-12 * float(La.abs().max()))
+    assert torch.allclose(energy(d, g.detach(), u, lam), L.detach(), rtol=0, atol=0)
     L.sum().backward()
     grad = g.grad.detach().cpu().numpy()
     hstep = 1e-6
@@ -47,7 +51,7 @@ def test_adjoint_matches_central_differences(gpu, lifting):
             gm = g.detach().clone()
             gp[k, e] += hstep
             gm[k, e] -= hstep
-            fd = (energy(d, gp, u, lam)[k] - energy(d, gm, u, lam)[k]).item() / (2 * hstep)
+            fd = (energy_assembled(d, gp, u, lam)[k] - energy_assembled(d, gm, u, lam)[k]).item() / (2 * hstep)
             assert abs(fd - grad[k, e]) <= 1e-6 * max(1.0, np.max(np.abs(grad[k]))), (k, e, fd, grad[k, e])
 
 
