@@ -5,7 +5,8 @@ C++ (libh3dg.so); assembly runs as sm_100a kernels.  See include/h3dg.h for
 the C ABI.
 """
 from . import _capi
-from .discretization import (BC_ESSENTIAL, BC_NATURAL, BC_NONE, Discretization, H1Space, UMFPackMatrix,
+from .discretization import (BC_ESSENTIAL, BC_NATURAL, BC_NONE, DF_HERMES_BIN, DF_MATLAB_SPARSE, DF_PLAIN_ASCII, Discretization, H1Space,
+                             UMFPackMatrix,
                              UMFPackVector, UnsupportedForm, int_F_v, int_grad_u_grad_v,
                              int_grad_u_grad_v_plus_u_v, int_u_v, surf_int_G_v, surf_int_u_v,
                              SystemDiscretization)
@@ -21,4 +22,5 @@ __all__ = [
     "UMFPackVector", "int_grad_u_grad_v", "int_grad_u_grad_v_plus_u_v", "int_F_v", "UnsupportedForm",
     "surf_int_u_v", "surf_int_G_v", "int_u_v", "SystemDiscretization",
     "BC_ESSENTIAL", "BC_NATURAL", "BC_NONE", "PREC_FP64", "PREC_TF32X3", "PREC_OZAKI", "H3dgError",
+    "DF_HERMES_BIN", "DF_MATLAB_SPARSE", "DF_PLAIN_ASCII",
 ]

@@ -12,6 +12,7 @@ to the CPU.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 from typing import Callable, Optional
 
@@ -164,6 +165,14 @@ def int_F_v(F):
 
 # ---------------------------------------------------------------- matrix / vector sinks
 
+# dump formats of Matrix::dump / Vector::dump (src/matrix.h:96-101)
+DF_MATLAB_SPARSE, DF_PLAIN_ASCII, DF_HERMES_BIN = 0, 1, 2
+
+
+def _open_for(file, mode):
+    return (open(file, mode), True) if isinstance(file, (str, bytes, os.PathLike)) else (file, False)
+
+
 class UMFPackMatrix:
     """CSC sink with the reference's arrays (src/linsolver/umfpack.h:26-47).
     Ap is int64 here (nnz may exceed INT_MAX)."""
@@ -178,10 +187,112 @@ class UMFPackMatrix:
         import scipy.sparse as sp
         return sp.csc_matrix((self.Ax, self.Ai, self.Ap), shape=(self.ndofs, self.ndofs))
 
+    def dump(self, file, var_name, fmt=DF_MATLAB_SPARSE):
+        """UMFPackMatrix::dump (src/linsolver/umfpack.cc:95-127): DF_HERMES_BIN
+        writes "H2DX", the scalar size, ndofs, nnz, Ap, Ai (32-bit) and Ax;
+        DF_MATLAB_SPARSE a MATLAB script of (row, column, value) triplets that
+        spconvert()s into var_name.  file: a path or a file object."""
+        n, nnz = int(self.ndofs), int(self.Ap[-1])
+        if fmt == DF_HERMES_BIN:
+            if nnz >= 2 ** 31:
+                raise ValueError("H2DX stores 32-bit column pointers: nnz >= 2^31")
+            f, own = _open_for(file, "wb")
+            try:
+                f.write(b"H2DX\x01\x00\x00\x00")
+                f.write(np.array([8, n, nnz], np.int32).tobytes())
+                f.write(np.asarray(self.Ap, np.int32).tobytes())
+                f.write(np.asarray(self.Ai, np.int32).tobytes())
+                f.write(np.asarray(self.Ax, np.float64).tobytes())
+            finally:
+                if own:
+                    f.close()
+            return True
+        if fmt == DF_MATLAB_SPARSE:
+            f, own = _open_for(file, "w")
+            try:
+                f.write("%% Size: %dx%d\n%% Nonzeros: %d\ntemp = zeros(%d, 3);\ntemp = [\n" % (n, n, nnz, nnz))
+                cols = np.repeat(np.arange(n), np.diff(self.Ap))
+                f.writelines("%d %d %f\n" % (i + 1, j + 1, x) for i, j, x in zip(self.Ai, cols, self.Ax))
+                f.write("];\n%s = spconvert(temp);\n" % var_name)
+            finally:
+                if own:
+                    f.close()
+            return True
+        if fmt == DF_PLAIN_ASCII:                # the reference exits with ERR_NOT_IMPLEMENTED
+            raise NotImplementedError("DF_PLAIN_ASCII dump")
+        return False
+
+    @staticmethod
+    def load(file):
+        """Read an H2DX dump (the reference's or ours) back into a matrix."""
+        f, own = _open_for(file, "rb")
+        try:
+            head = f.read(8)
+            if head[:4] != b"H2DX":
+                raise ValueError("not an H2DX dump")
+            ssize, n, nnz = np.frombuffer(f.read(12), np.int32)
+            if ssize != 8:
+                raise ValueError("real (8-byte) scalars only")
+            m = UMFPackMatrix()
+            m.ndofs = int(n)
+            m.Ap = np.frombuffer(f.read(4 * (n + 1)), np.int32).astype(np.int64)
+            m.Ai = np.frombuffer(f.read(4 * nnz), np.int32).copy()
+            m.Ax = np.frombuffer(f.read(8 * nnz), np.float64).copy()
+            return m
+        finally:
+            if own:
+                f.close()
+
 
 class UMFPackVector:
     def __init__(self):
         self.v = None
+
+    def dump(self, file, var_name, fmt=DF_MATLAB_SPARSE):
+        """UMFPackVector::dump (src/linsolver/umfpack.cc:194-220): "H2DR", the
+        scalar size, ndofs, v; or a MATLAB column vector."""
+        n = len(self.v)
+        if fmt == DF_HERMES_BIN:
+            f, own = _open_for(file, "wb")
+            try:
+                f.write(b"H2DR\x01\x00\x00\x00")
+                f.write(np.array([8, n], np.int32).tobytes())
+                f.write(np.asarray(self.v, np.float64).tobytes())
+            finally:
+                if own:
+                    f.close()
+            return True
+        if fmt == DF_MATLAB_SPARSE:
+            f, own = _open_for(file, "w")
+            try:
+                f.write("%% Size: %dx1\n%s = [\n" % (n, var_name))
+                f.writelines("%f\n" % x for x in self.v)
+                f.write(" ];\n")
+            finally:
+                if own:
+                    f.close()
+            return True
+        if fmt == DF_PLAIN_ASCII:                # the reference exits with ERR_NOT_IMPLEMENTED
+            raise NotImplementedError("DF_PLAIN_ASCII dump")
+        return False
+
+    @staticmethod
+    def load(file):
+        """Read an H2DR dump back into a vector."""
+        f, own = _open_for(file, "rb")
+        try:
+            head = f.read(8)
+            if head[:4] != b"H2DR":
+                raise ValueError("not an H2DR dump")
+            ssize, n = np.frombuffer(f.read(8), np.int32)
+            if ssize != 8:
+                raise ValueError("real (8-byte) scalars only")
+            vec = UMFPackVector()
+            vec.v = np.frombuffer(f.read(8 * n), np.float64).copy()
+            return vec
+        finally:
+            if own:
+                f.close()
 
 
 class Discretization:

@@ -25,7 +25,7 @@
 //       [--qmode fixed:N | pplus:K | ref] [--mass] [--gradcoef COEF.bin]
 //       [--source none|one|sin|poly] [--bc dirichlet0|dirichlet_poly|natural]
 //       [--refine REF.bin] [--repeat R] [--no-asm] [--elem-dump]
-//       [--surf-uv] [--surf-g g1,...,g6] [--natural-markers m1,m2,...]
+//       [--surf-uv] [--surf-g g1,...,g6] [--natural-markers m1,m2,...] [--dump PREFIX]
 //       [--sys k11,k12,k21,k22 (none|gg|ggm|mass) --source2 S [--p2 P2]]
 //
 // Output (little-endian binary, all counts int64):
@@ -292,6 +292,7 @@ static double now() {
 
 int main(int argc, char **argv) {
 	const char *mesh_fn = NULL, *out_fn = NULL, *orders_fn = NULL, *coef_fn = NULL, *refine_fn = NULL;
+	const char *dump_prefix = NULL;   // --dump P: the sinks' own dumps (UMFPackMatrix/Vector::dump) to P.h2dx, P.h2dr, P.m
 	int p = 2, repeat = 1;
 	int p2 = 0;              // uniform order of the second space of a system (0: the first space's orders)
 	bool qref = false, do_asm = true, elem_dump = false, surf_uv = false, surf_g = false;
@@ -301,6 +302,7 @@ int main(int argc, char **argv) {
 		const char *v = i + 1 < argc ? argv[i + 1] : "";
 		if (a == "--mesh") { mesh_fn = v; i++; }
 		else if (a == "--out") { out_fn = v; i++; }
+		else if (a == "--dump") { dump_prefix = v; i++; }
 		else if (a == "--orders") { orders_fn = v; i++; }
 		else if (a == "--gradcoef") { coef_fn = v; i++; }
 		else if (a == "--refine") { refine_fn = v; i++; }
@@ -502,6 +504,17 @@ int main(int argc, char **argv) {
 			d.assemble(&mat, &rhs);
 			t_asm.push_back(now() - t0);
 		}
+	}
+
+	// ---- the reference's own dumps of the assembled system (src/linsolver/umfpack.cc:95-127, 194-220)
+	if (dump_prefix && do_asm && ndof > 0) {
+		std::string pre = dump_prefix;
+		FILE *f = fopen((pre + ".h2dx").c_str(), "wb");
+		if (f) { mat.dump(f, "A", DF_HERMES_BIN); fclose(f); }
+		f = fopen((pre + ".h2dr").c_str(), "wb");
+		if (f) { rhs.dump(f, "b", DF_HERMES_BIN); fclose(f); }
+		f = fopen((pre + ".m").c_str(), "w");
+		if (f) { mat.dump(f, "A", DF_MATLAB_SPARSE); rhs.dump(f, "b", DF_MATLAB_SPARSE); fclose(f); }
 	}
 
 	// ---- dump

@@ -35,7 +35,7 @@ def build(ref=None):
 
 def run(mesh, p=2, orders=None, qmode="pplus:2", mass=False, gradcoef=None, source="one", bc="dirichlet0",
         repeat=1, elem_dump=False, assemble=True, refine=None, surf_uv=False, surf_g=None, natural_markers=None,
-        sys=None, source2="none", p2=0, timeout=3600):
+        sys=None, source2="none", p2=0, dump=None, timeout=3600):
     """Assemble ``mesh`` (hermes3d_b200.Mesh with arrays) with the reference.
 
     Returns dict(ndof, nnz, Ap, Ai, Ax, rhs, asm=[(id, idx, dof, coef)...],
@@ -78,6 +78,8 @@ def run(mesh, p=2, orders=None, qmode="pplus:2", mass=False, gradcoef=None, sour
             cmd += ["--sys", ",".join(sys), "--source2", source2]
             if p2:
                 cmd += ["--p2", str(p2)]
+        if dump:
+            cmd += ["--dump", dump]
         if surf_uv:
             cmd.append("--surf-uv")
         if surf_g is not None:
