@@ -85,6 +85,7 @@ SIGNATURES = {
     "h3dg_disc_update_coefficients": [_p, _pd, _i64],
     "h3dg_disc_update_coefficients_device": [_p, _p, _i64, _p],
     "h3dg_disc_last_launch_count": [_p, _pi32],
+    "h3dg_disc_last_kernel": [_p, _pi32],
     "h3dg_disc_geometry": [_p, _p, _p, _p, _p],
     "h3dg_disc_adjoint": [_p, C.c_int, _p, _p, _p, _p, _p, _p],
     "h3dg_tc_selftest": [C.c_int, _p, _p, _p, C.c_int],

@@ -25,7 +25,7 @@ CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_SRC = ["host/h3dg_host.cpp"]
-CUDA_SRC = ["h3dg_capi.cu", "tables_lo.cu", "tables_seg.cu", "tables_lo_tc.cu", "tables_stock.cu", "tables_ho.cu", "tables_ho_tc.cu", "tables_adj.cu", "tables_mixed.cu", "tables_ho_oz.cu"]
+CUDA_SRC = ["h3dg_capi.cu", "tables_lo.cu", "tables_seg.cu", "tables_lo_tc.cu", "tables_stock.cu", "tables_ho.cu", "tables_ho_tc.cu", "tables_adj.cu", "tables_mixed.cu", "tables_ho_oz.cu", "tables_dm.cu"]
 
 
 def _deps():

@@ -105,6 +105,7 @@ struct h3dg_disc {
 	float variant_ms = 0.0f;
 	h3dg::Plan plan;
 	int32_t last_launches = 0;
+	int32_t last_kind = H3DG_KERNEL_OTHER;   // kernel family of the last volume assembly
 
 	// device plan
 	DBuf<double> xyz, coef, tables, qx, qy, qz, Ax, rhs;
@@ -113,6 +114,8 @@ struct h3dg_disc {
 	DBuf<uint16_t> el_s, el_off, el_offc;
 	DBuf<uint16_t> el_offt;    // tensor-core scatter stream (built at the first split-precision assembly)
 	bool offt_store_all = false;   // its first-touch stores cover every Ax slot
+	DBuf<uint16_t> el_offd;    // FP64 tensor-core scatter stream (built at the first FP64 high-order assembly)
+	bool offd_store_all = false;
 	DBuf<double> ho_scratch;   // per-CTA global work area of the FP64-accurate split kernel
 	DBuf<int32_t> el_cdof, el_tcdof;
 	DBuf<double> el_ccoef, el_tccoef;
@@ -578,6 +581,8 @@ h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nn
 
 // Device copy of the plan, made on the first device call (create() itself
 // is host work, as in the reference).
+static h3dg_status noalloc_scratch(double **out);
+
 static h3dg_status ensure_device(h3dg_disc *disc) {
 	if (disc->on_device) return H3DG_OK;
 	const h3dg::Space &sp = disc->space->s;
@@ -635,6 +640,8 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 		disc->el_offc.release();
 		disc->el_offt.release();
 		disc->offt_store_all = false;
+		disc->el_offd.release();
+		disc->offd_store_all = false;
 	}
 	else if (P.canon) {
 		H3DG_CUDA_TRY(disc->el_cdof.upload(P.el_cdof));
@@ -646,6 +653,8 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 		H3DG_CUDA_TRY(disc->el_offc.upload(P.el_offc));
 		disc->el_offt.release();
 		disc->offt_store_all = false;
+		disc->el_offd.release();
+		disc->offd_store_all = false;
 	}
 	else {
 		H3DG_CUDA_TRY(disc->el_s.upload(P.el_s));
@@ -687,6 +696,13 @@ static h3dg_status ensure_device(h3dg_disc *disc) {
 	else disc->coef.release();
 	H3DG_CUDA_TRY(disc->status.alloc(1));
 	H3DG_CUDA_TRY(cudaMemset(disc->status.p, 0, sizeof(int)));
+	// the module holding the no-allocation staging array is loaded on first
+	// use (lazy loading), which allocates it: do that here, in an allocating call
+	{
+		double *scratch = nullptr;
+		h3dg_status s0 = noalloc_scratch(&scratch);
+		if (s0 != H3DG_OK) return s0;
+	}
 	disc->on_device = true;
 	return H3DG_OK;
 }
@@ -773,8 +789,89 @@ static h3dg_status ho_select(h3dg_disc *disc, int precision, HoSpec **out, int *
 	return H3DG_OK;
 }
 
+// The FP64 tensor-core kernel for the current plan, or nullptr (two-space
+// blocks, orders / rules without an instance, or H3DG_HO_FP64_FMA=1, which
+// keeps the FMA kernel: tests compare the two)
+static DmSpec *dm_select(h3dg_disc *disc, int precision) {
+	const h3dg::Plan &P = disc->plan;
+	if (precision != H3DG_PREC_FP64 || P.two_space) return nullptr;
+	const char *fma = std::getenv("H3DG_HO_FP64_FMA");
+	if (fma && fma[0] == '1') return nullptr;
+	for (auto &k : dm_table())
+		if (k.p == P.px && k.nq == P.nqx) return &k;
+	return nullptr;
+}
+
+static h3dg_status assemble_dm(h3dg_disc *disc, DmSpec &k, double *d_Ax, double *d_rhs, cudaStream_t st) {
+	const h3dg::Plan &P = disc->plan;
+	if (!k.configured) {
+		H3DG_CUDA_TRY(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) k.smem));
+		k.configured = true;
+	}
+	if (d_Ax && !disc->el_offd.p && P.ne > 0) {
+		// built once per plan and validated against the column lengths
+		size_t cnt = 0;
+		unsigned long long stores = 0;
+		H3DG_CUDA_TRY(build_offd(k, disc->el_offc.p, disc->el_cdof.p, disc->Ap.p, P.ne, P.color_ptr.data(), P.ncolors, P.nnz,
+		                         &disc->el_offd.p, &cnt, &stores, disc->status.p, st));
+		disc->el_offd.n = cnt;
+		disc->offd_store_all = (int64_t) stores == P.nnz;
+		int hs = 0;
+		H3DG_CUDA_TRY(cudaMemcpyAsync(&hs, disc->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+		H3DG_CUDA_TRY(cudaStreamSynchronize(st));
+		if (hs & h3dg::kErrBounds) {
+			disc->el_offd.release();
+			disc->offd_store_all = false;
+			cudaMemsetAsync(disc->status.p, 0, sizeof(int), st);
+			return fail(H3DG_ERR_STATE, "assemble: a scatter position falls outside its column (plan corrupt)");
+		}
+	}
+	h3dg::KArgsHO a = {};
+	a.xyz = disc->xyz.p;
+	a.el_vtx = disc->el_vtx.p;
+	a.el_id = disc->el_id.p;
+	a.ecoef = disc->coef.p;
+	a.cdof = disc->el_cdof.p;
+	a.ccoef = disc->el_ccoef.p;
+	a.offc = disc->el_offc.p;
+	a.offd = disc->el_offd.p;
+	a.Ap = disc->Ap.p;
+	a.tables = disc->tables.p;
+	a.table_bytes = disc->table_bytes;
+	a.mass = disc->bf == H3DG_BF_GRAD_GRAD_MASS;
+	a.lf = disc->lf;
+	a.lf_value = disc->lf_value;
+	a.Ax = d_Ax;
+	a.rhs = disc->lf ? d_rhs : nullptr;
+	a.status = disc->status.p;
+	// first-touch stores cover every slot: no zero-fill of Ax
+	if (d_Ax && !disc->offd_store_all) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
+	if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.nrhs(), st));
+	int nsm = 148;
+	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
+	const bool rec = disc->tn < disc->tcap;
+	if (rec) H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn], st));
+	int32_t launches = 0;
+	for (int c = 0; c < P.ncolors; c++) {
+		int64_t kb = P.color_ptr[c], ke = P.color_ptr[c + 1];
+		if (ke <= kb) continue;
+		int64_t grid = std::min<int64_t>(ke - kb, (int64_t) nsm);
+		k.fn<<<(unsigned) grid, k.threads, k.smem, st>>>(a, kb, ke);
+		launches++;
+	}
+	H3DG_CUDA_TRY(cudaGetLastError());
+	if (rec) {
+		H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn + 1], st));
+		disc->tn++;
+	}
+	disc->last_launches = launches;
+	disc->last_kind = H3DG_KERNEL_HO_FP64_DMMA;
+	return H3DG_OK;
+}
+
 static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, cudaStream_t st) {
 	const h3dg::Plan &P = disc->plan;
+	if (DmSpec *dm = dm_select(disc, precision)) return assemble_dm(disc, *dm, d_Ax, d_rhs, st);
 	HoSpec *kp = nullptr;
 	int per_sm = 1;
 	size_t scratch_need = 0;
@@ -813,6 +910,7 @@ static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, dou
 		}
 	}
 	a.offt = disc->el_offt.p;
+	a.offd = nullptr;
 	a.Ap = disc->Ap.p;
 	a.tables = disc->tables.p;
 	a.table_bytes = disc->table_bytes;
@@ -850,6 +948,8 @@ static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, dou
 		disc->tn++;
 	}
 	disc->last_launches = launches;
+	disc->last_kind = precision == H3DG_PREC_TF32X3 ? H3DG_KERNEL_HO_TF32X3
+	                  : precision == H3DG_PREC_OZAKI ? H3DG_KERNEL_HO_OZAKI : H3DG_KERNEL_HO_FP64_FMA;
 	return H3DG_OK;
 }
 
@@ -1439,6 +1539,7 @@ static h3dg_status assemble_colours(h3dg_disc *disc, KernelSpec &k, double *d_Ax
 
 static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax, double *d_rhs, void *stream) {
 	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "assemble: create_pattern() first");
+	disc->last_kind = H3DG_KERNEL_OTHER;
 	if (precision != H3DG_PREC_FP64 && precision != H3DG_PREC_TF32X3 && precision != H3DG_PREC_OZAKI)
 		return fail(H3DG_ERR_INVALID_ARG, "assemble: unknown precision");
 	const h3dg::Plan &P = disc->plan;
@@ -1760,6 +1861,9 @@ h3dg_status h3dg_disc_assemble_host_noalloc(h3dg_disc *disc, int precision, doub
 	if (P.canon && (precision == H3DG_PREC_TF32X3 || precision == H3DG_PREC_OZAKI) && Ax && !disc->el_offt.p && P.ne > 0)
 		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: split-precision scatter stream not built; make one allocating "
 		                            "split-precision assembly call with the matrix first");
+	if (P.canon && Ax && P.ne > 0 && dm_select(disc, precision) && !disc->el_offd.p)
+		return fail(H3DG_ERR_STATE, "assemble_host_noalloc: FP64 tensor-core scatter stream not built; make one allocating "
+		                            "FP64 assembly call with the matrix first");
 	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
 	if (P.canon && precision == H3DG_PREC_OZAKI && P.ne > 0) {
 		// the work area assemble_ho would (re)allocate: present and large enough
@@ -1867,6 +1971,12 @@ h3dg_status h3dg_disc_debug_inject(h3dg_disc *disc, int what) {
 h3dg_status h3dg_disc_last_launch_count(const h3dg_disc *disc, int32_t *count) {
 	if (!disc || !count) return fail(H3DG_ERR_INVALID_ARG, "last_launch_count: bad arguments");
 	*count = disc->last_launches;
+	return H3DG_OK;
+}
+
+h3dg_status h3dg_disc_last_kernel(const h3dg_disc *disc, int32_t *kind) {
+	if (!disc || !kind) return fail(H3DG_ERR_INVALID_ARG, "last_kernel: bad arguments");
+	*kind = disc->last_kind;
 	return H3DG_OK;
 }
 

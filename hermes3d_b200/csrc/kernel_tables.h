@@ -41,6 +41,20 @@ struct HoSpec {
 	bool configured;
 };
 
+// FP64 tensor-core (DMMA) high-order kernels and the builders of their scatter streams
+using OffdFn = void (*)(const uint16_t *, const int32_t *, const int64_t *, int64_t, int64_t, uint16_t *, int *, uint8_t *,
+                        unsigned long long *);
+
+struct DmSpec {
+	int p, nq;
+	HoFn fn;
+	int threads;
+	size_t smem;
+	bool configured;
+	size_t epe;                   // scatter-stream entries per element
+	OffdFn build;
+};
+
 using AdjFn = void (*)(h3dg::AdjArgs);
 
 struct AdjSpec {
@@ -67,6 +81,12 @@ struct MixSpec {
 std::vector<KernelSpec> &kernel_table();
 // FP64 high-order kernels (element matrix never materialised)
 std::vector<HoSpec> &ho_table();
+// FP64 high-order kernels with stages 2 and 3 on the FP64 tensor cores
+std::vector<DmSpec> &dm_table();
+// their scatter stream, colour by colour with first-touch store flags (async on st)
+cudaError_t build_offd(const DmSpec &k, const uint16_t *offc, const int32_t *cdof, const int64_t *Ap, int64_t ne,
+                       const int64_t *color_ptr, int ncolors, int64_t nnz, uint16_t **offd, size_t *count,
+                       unsigned long long *stores, int *status, cudaStream_t st);
 // split-precision high-order kernels (tcgen05 3xTF32 stage 3)
 std::vector<HoSpec> &ho_tc_table();
 // FP64-accurate high-order kernels (int8-sliced tcgen05 stage 3)

@@ -46,6 +46,7 @@ struct KArgsHO {
 	double *gscratch;          // per-CTA global work area (kernels that keep G out of shared memory), or nullptr
 	const int32_t *tcdof;      // test side of a two-space block (ne x nl), or nullptr: the trial tables
 	const double *tccoef;
+	const uint16_t *offd;      // FP64 tensor-core scatter stream (k_build_offd), or nullptr
 };
 
 template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ>

@@ -575,6 +575,14 @@ class Discretization:
         capi.call("h3dg_disc_last_launch_count", self.handle, C.byref(n))
         return n.value
 
+    def last_kernel(self):
+        """Element-matrix kernel family of the last volume assembly: "other"
+        (low / mixed orders, stock rule), "ho_fp64_fma", "ho_fp64_dmma" (FP64
+        tensor cores), "ho_tf32x3", "ho_ozaki"."""
+        n = C.c_int32()
+        capi.call("h3dg_disc_last_kernel", self.handle, C.byref(n))
+        return ("other", "ho_fp64_fma", "ho_fp64_dmma", "ho_tf32x3", "ho_ozaki")[n.value]
+
     def debug_inject(self, what: int):
         """Test hook (no reference counterpart): DEBUG_WAIT_GIVES_UP makes the
         next FP64 low-order assembly's bounded wait give up (H3dgError

@@ -251,6 +251,14 @@ h3dg_status h3dg_disc_update_coefficients(h3dg_disc *disc, const double *elem_co
 h3dg_status h3dg_disc_update_coefficients_device(h3dg_disc *disc, const double *d_elem_coef, int64_t ne, void *stream);
 /* number of kernels launched by the last assemble call */
 h3dg_status h3dg_disc_last_launch_count(const h3dg_disc *disc, int32_t *count);
+/* the element-matrix kernel family of the last volume assembly (no reference
+ * counterpart; for tests and measurement): */
+#define H3DG_KERNEL_OTHER 0          /* low orders, mixed orders, stock rule */
+#define H3DG_KERNEL_HO_FP64_FMA 1    /* high order, FP64 on the FMA pipe */
+#define H3DG_KERNEL_HO_FP64_DMMA 2   /* high order, FP64 on the FP64 tensor cores (p >= 4, one space) */
+#define H3DG_KERNEL_HO_TF32X3 3      /* high order, 3xTF32 on tcgen05 */
+#define H3DG_KERNEL_HO_OZAKI 4       /* high order, int8 slices on tcgen05 */
+h3dg_status h3dg_disc_last_kernel(const h3dg_disc *disc, int32_t *kind);
 
 /* the kernel variant the autotuner picked on the first assembly of the
  * current plan: threads per CTA, elements per CTA pass, and the time of one
