@@ -855,7 +855,11 @@ static h3dg_status assemble_dm(h3dg_disc *disc, DmSpec &k, double *d_Ax, double 
 	for (int c = 0; c < P.ncolors; c++) {
 		int64_t kb = P.color_ptr[c], ke = P.color_ptr[c + 1];
 		if (ke <= kb) continue;
-		int64_t grid = std::min<int64_t>(ke - kb, (int64_t) nsm);
+		// a last round that would leave more than half the SMs idle runs as half elements
+		const int64_t n = ke - kb, rem = n % nsm;
+		a.split_from = rem > 0 && 2 * rem <= nsm ? ke - rem : ke;
+		const int64_t items = (a.split_from - kb) + 2 * (ke - a.split_from);
+		int64_t grid = std::min<int64_t>(items, (int64_t) nsm);
 		k.fn<<<(unsigned) grid, k.threads, k.smem, st>>>(a, kb, ke);
 		launches++;
 	}
@@ -911,6 +915,7 @@ static h3dg_status assemble_ho(h3dg_disc *disc, int precision, double *d_Ax, dou
 	}
 	a.offt = disc->el_offt.p;
 	a.offd = nullptr;
+	a.split_from = 0;
 	a.Ap = disc->Ap.p;
 	a.tables = disc->tables.p;
 	a.table_bytes = disc->table_bytes;

@@ -10,12 +10,16 @@
 //   stage 2 (DMMA): V^T[bb][nu] = sum_kappa W[bb][kappa] T1[kappa][nu],
 //     bb = (b, b') the y indices, kappa = (y flag, q2), nu = (x class f, q1):
 //     W[bb][(fy, q2)] = E_y^(fy>>1)[b][q2] E_y^(fy&1)[b'][q2] is the same for
-//     every element, so each warp keeps its rows of W in registers;
+//     every element: its fragments are formed once per CTA;
 //   stage 3 (DMMA): K[(a,b,c)][(a',b',c')] = sum_nu V^T[bb][nu] P[nu][(a', a)],
 //     P[(f, q1)][(a', a)] = E_x^(f>>1)[a][q1] E_x^(f&1)[a'][q1], a fixed table.
 //     The stage-2 accumulators are the stage-3 A fragments as they stand: the
 //     k order of stage 3 pairs the two nu columns a thread holds (2t, 2t+1)
 //     into its two k slots (t, t+4), and P is stored in that order.
+// Work items: whole elements, and from args.split_from on half elements
+// (trial z indices c' below / from (NX + 1) / 2, the load vector with the
+// first half), so that the last round of a colour launch spreads over twice
+// as many SMs.
 // Pairs run trial z index c' outermost: the 81 CSC columns (a', b', c') of a
 // c' receive all their rows within NX consecutive pairs, so the sectors a CTA
 // writes stay in L2 until they are complete (about 0.5 MB per CTA at p = 8).
@@ -75,7 +79,9 @@ struct DmShape {
 	static constexpr int S_G = S_TAB + H::TABP;
 	static constexpr int S_U = S_G + 8 * NQ3;
 	static constexpr int S_P = S_U + UNION;
-	static constexpr int S_X = S_P + PSZ;
+	static constexpr int AWSZ = MT * KS * 128;               // stage-2 A fragments (W), per M tile
+	static constexpr int S_AW = S_P + PSZ;
+	static constexpr int S_X = S_AW + AWSZ;
 	static constexpr int S_M = S_X + 24;
 	static constexpr int S_C = S_M + 24;
 	static constexpr int S_CS = S_C + NL;
@@ -151,32 +157,41 @@ __global__ void __launch_bounds__(DmShape<P, NQ>::NT, 1) k_assemble_fp64_dm(KArg
 		}
 		Pf[e] = v;
 	}
-	// ---- per warp: its M tile of W (stage-2 A fragments) in registers
-	const int mt = warp % MT, ph = warp / MT;
-	double aw[KS][4];
-#pragma unroll
-	for (int ks = 0; ks < KS; ks++)
-#pragma unroll
-		for (int r = 0; r < 4; r++) {
-			const int bb = mt * 16 + g + 8 * (r & 1), kq = ks * 8 + t + 4 * (r >> 1);
-			double v = 0.0;
-			if (bb < NB && kq < KK) {
-				const int fy = kq / NQ, q2 = kq % NQ, b = bb / NX, b2 = bb % NX;
-				v = ((fy >> 1) ? Dy : Vy)[b * NQ + q2] * ((fy & 1) ? Dy : Vy)[b2 * NQ + q2];
-			}
-			aw[ks][r] = v;
+	// ---- per CTA: stage-2 A fragments W, [M tile][k step][lane][4]
+	double *Aw = sm + S::S_AW;
+	for (int e = tid; e < S::AWSZ; e += NT) {
+		const int r = e & 3, ln = (e >> 2) & 31, tile = e >> 7;
+		const int mt_ = tile / KS, ks = tile % KS;
+		const int bb = mt_ * 16 + (ln >> 2) + 8 * (r & 1), kq = ks * 8 + (ln & 3) + 4 * (r >> 1);
+		double v = 0.0;
+		if (bb < NB && kq < KK) {
+			const int fy = kq / NQ, q2 = kq % NQ, b = bb / NX, b2 = bb % NX;
+			v = ((fy >> 1) ? Dy : Vy)[b * NQ + q2] * ((fy & 1) ? Dy : Vy)[b2 * NQ + q2];
 		}
+		Aw[e] = v;
+	}
+	const int mt = warp % MT, ph = warp / MT;
+	const double *aw = Aw + (mt * KS * 32 + lane) * 4;
+	// scatter: test / trial y parts of this warp's rows bb = mt 16 + g (+ 8)
+	int rb[2], cb[2];
+#pragma unroll
+	for (int h = 0; h < 2; h++) {
+		const int bb = mt * 16 + g + 8 * h;
+		rb[h] = (bb / NX) * NX;
+		cb[h] = (bb % NX) * NX;
+	}
 	__syncthreads();
 
 	// stage 1 for the pairs of iteration it into buffer set (it & 1): thread
 	// group (pair slot, product) walks the (q1, q2) points
 	constexpr int GROUPS = PH * 9, TPG = NT / GROUPS;
 	const int grp = tid / TPG, gl = tid % TPG;
+	int p0 = 0, p1 = S::PAIRS, iters = S::ITERS;     // pair range of the current work item
 	auto stage1 = [&](int it) {
 		if (grp >= GROUPS) return;
 		const int p_slot = grp / 9, kk = grp % 9;
-		const int pair = it * PH + p_slot;
-		if (pair >= S::PAIRS) return;
+		const int pair = p0 + it * PH + p_slot;
+		if (pair >= p1) return;
 		const int c2 = pair / NX, c = pair % NX;
 		const int fz = kHoFz[kk];
 		const double *ea = ((fz >> 1) ? Dz : Vz) + c * NQ, *eb = ((fz & 1) ? Dz : Vz) + c2 * NQ;
@@ -203,10 +218,21 @@ __global__ void __launch_bounds__(DmShape<P, NQ>::NT, 1) k_assemble_fp64_dm(KArg
 		}
 	};
 
-	for (int64_t k = kbeg + blockIdx.x; k < kend; k += gridDim.x) {
+	const int64_t nwhole = args.split_from - kbeg, items = nwhole + 2 * (kend - args.split_from);
+	for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
+		int half = -1;
+		int64_t k = kbeg + item;
+		if (item >= nwhole) {
+			k = args.split_from + (item - nwhole) / 2;
+			half = (int) ((item - nwhole) & 1);
+		}
+		constexpr int C2H = (NX + 1) / 2;
+		p0 = half == 1 ? C2H * NX : 0;
+		p1 = half == 0 ? C2H * NX : S::PAIRS;
+		iters = (p1 - p0 + PH - 1) / PH;
 		const double cgrad = ho_element_setup<H, NT>(args, k, X, Mo, cc, cd, cs, ce, &s_nlift);
 		ho_geometry<H, NT>(args, tab, Mo, cgrad, G);
-		if (do_rhs) ho_rhs<H, NT>(args, tab, G, U, cd, cc, cd, cc, s_nlift > 0 && args.Ax);
+		if (do_rhs && half <= 0) ho_rhs<H, NT>(args, tab, G, U, cd, cc, cd, cc, s_nlift > 0 && args.Ax);
 		if (!args.Ax) continue;
 		// the fragment buffers share the work area with ho_rhs: clear them (positions
 		// no product writes stay zero for the whole element)
@@ -215,10 +241,12 @@ __global__ void __launch_bounds__(DmShape<P, NQ>::NT, 1) k_assemble_fp64_dm(KArg
 		stage1(0);
 		__syncthreads();
 		const uint16_t *offd = args.offd + k * (int64_t) S::EPE;
-		for (int it = 0; it < S::ITERS; it++) {
-			if (it + 1 < S::ITERS) stage1(it + 1);
-			const int pair = it * PH + ph;
-			if (pair < S::PAIRS) {
+		for (int it = 0; it < iters; it++) {
+			// stage 1 of the next pairs: warps of even pair slots before their MMAs,
+			// odd ones after, so that the DMMA pipe always has work queued
+			if (!(ph & 1) && it + 1 < iters) stage1(it + 1);
+			const int pair = p0 + it * PH + ph;
+			if (pair < p1) {
 				const double *buf = U + ((it & 1) * PH + ph) * S::B2SZ;
 				// ---- stage 2: V^T (bb x nu) for this warp's M tile
 				double v[KS][4];
@@ -227,41 +255,71 @@ __global__ void __launch_bounds__(DmShape<P, NQ>::NT, 1) k_assemble_fp64_dm(KArg
 #pragma unroll
 					for (int r = 0; r < 4; r++) v[j][r] = 0.0;
 #pragma unroll
-				for (int ks = 0; ks < KS; ks++)
+				for (int ks = 0; ks < KS; ks++) {
+					const double2 a01 = *reinterpret_cast<const double2 *>(aw + ks * 128);
+					const double2 a23 = *reinterpret_cast<const double2 *>(aw + ks * 128 + 2);
 #pragma unroll
 					for (int j = 0; j < KS; j++) {
 						if (S::zero_tile(ks, j)) continue;
 						const double2 b = *reinterpret_cast<const double2 *>(buf + ((ks * KS + j) * 32 + lane) * 2);
-						dmma16x8x8(v[j], aw[ks][0], aw[ks][1], aw[ks][2], aw[ks][3], b.x, b.y);
-					}
-				// ---- stage 3 per N tile of (a', a), then the scatter
-				const int c2 = pair / NX, c = pair % NX;
-				const uint16_t *od = offd + ((int64_t) (pair * MT + mt) * NT3) * 128 + lane * 4;
-#pragma unroll 1
-				for (int nt = 0; nt < NT3; nt++) {
-					double d[4] = { 0.0, 0.0, 0.0, 0.0 };
-#pragma unroll
-					for (int j = 0; j < KS; j++) {
-						const double2 b = *reinterpret_cast<const double2 *>(Pf + ((j * NT3 + nt) * 32 + lane) * 2);
-						dmma16x8x8(d, v[j][0], v[j][2], v[j][1], v[j][3], b.x, b.y);
-					}
-					const uint2 ow = __ldcs(reinterpret_cast<const uint2 *>(od + nt * 128));
-					const uint16_t o4[4] = { (uint16_t) (ow.x & 0xFFFF), (uint16_t) (ow.x >> 16), (uint16_t) (ow.y & 0xFFFF),
-					                         (uint16_t) (ow.y >> 16) };
-#pragma unroll
-					for (int r = 0; r < 4; r++) {
-						const uint16_t o = o4[r];
-						if (o == kOffSkip) continue;
-						const int bb = mt * 16 + g + 8 * (r >> 1), aa = nt * 8 + 2 * t + (r & 1);
-						const int b = bb / NX, b2 = bb % NX, a2 = aa / NX, a = aa % NX;
-						const int i = (a * NX + b) * NX + c, j = (a2 * NX + b2) * NX + c2;
-						double *dst = args.Ax + cs[j] + (o & kOffMask);
-						const double val = cc[i] * cc[j] * d[r];
-						if (o & kOffStore) posted_store(dst, val);
-						else posted_add(dst, val);
+						dmma16x8x8(v[j], a01.x, a01.y, a23.x, a23.y, b.x, b.y);
 					}
 				}
+				// ---- stage 3, NG N tiles of (a', a) per group (independent accumulators),
+				// software-pipelined: the MMAs of the next group are issued before the
+				// scatter of the current one; the stream words are loaded with the MMAs
+				constexpr int NG = 2;
+				const int c2 = pair / NX, c = pair % NX;
+				const uint16_t *od = offd + ((int64_t) (pair * MT + mt) * NT3) * 128 + lane * 4;
+				auto mma_group = [&](int n0, double (&d)[NG][4], uint2 (&ow)[NG]) {
+#pragma unroll
+					for (int q = 0; q < NG; q++) {
+						ow[q] = n0 + q < NT3 ? __ldcs(reinterpret_cast<const uint2 *>(od + (n0 + q) * 128)) : make_uint2(~0u, ~0u);
+#pragma unroll
+						for (int r = 0; r < 4; r++) d[q][r] = 0.0;
+					}
+#pragma unroll
+					for (int j = 0; j < KS; j++)
+#pragma unroll
+						for (int q = 0; q < NG; q++)
+							if (n0 + q < NT3) {
+								const double2 b = *reinterpret_cast<const double2 *>(Pf + ((j * NT3 + n0 + q) * 32 + lane) * 2);
+								dmma16x8x8(d[q], v[j][0], v[j][2], v[j][1], v[j][3], b.x, b.y);
+							}
+				};
+				auto scatter_group = [&](int n0, const double (&d)[NG][4], const uint2 (&ow)[NG]) {
+#pragma unroll
+					for (int q = 0; q < NG; q++)
+#pragma unroll
+						for (int e = 0; e < 2; e++) {
+							const int aa = (n0 + q) * 8 + 2 * t + e;
+							const int ra = (aa % NX) * NX * NX + c, ca = (aa / NX) * NX * NX + c2;
+#pragma unroll
+							for (int h = 0; h < 2; h++) {
+								const uint32_t w = h ? ow[q].y : ow[q].x;
+								const uint32_t o = e ? w >> 16 : w & 0xFFFF;
+								if (o == kOffSkip) continue;
+								const int i = ra + rb[h], j = ca + cb[h];
+								double *dst = args.Ax + cs[j] + (o & kOffMask);
+								const double val = cc[i] * cc[j] * d[q][2 * h + e];
+								if (o & kOffStore) posted_store(dst, val);
+								else posted_add(dst, val);
+							}
+						}
+				};
+				double dA[NG][4], dB[NG][4];
+				uint2 oA[NG], oB[NG];
+				mma_group(0, dA, oA);
+#pragma unroll 1
+				for (int n0 = 0; n0 < NT3; n0 += 2 * NG) {
+					if (n0 + NG < NT3) mma_group(n0 + NG, dB, oB);
+					scatter_group(n0, dA, oA);
+					if (n0 + 2 * NG < NT3) mma_group(n0 + 2 * NG, dA, oA);
+					if (n0 + NG < NT3) scatter_group(n0 + NG, dB, oB);
+				}
 			}
+			// the other half of the warps builds its share of the next pairs' stage 1 now
+			if (ph & 1 && it + 1 < iters) stage1(it + 1);
 			__syncthreads();
 		}
 	}

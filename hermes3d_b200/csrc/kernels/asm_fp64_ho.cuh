@@ -47,6 +47,7 @@ struct KArgsHO {
 	const int32_t *tcdof;      // test side of a two-space block (ne x nl), or nullptr: the trial tables
 	const double *tccoef;
 	const uint16_t *offd;      // FP64 tensor-core scatter stream (k_build_offd), or nullptr
+	int64_t split_from;        // FP64 tensor-core kernel: elements from here on are done in two halves
 };
 
 template <int PX, int PY, int PZ, int NQX, int NQY, int NQZ>

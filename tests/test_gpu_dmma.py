@@ -86,3 +86,37 @@ def test_dmma_reproducible_and_store_first(gpu, p):
     finally:
         os.environ.pop("H3DG_HO_FP64_FMA", None)
     assert rel_err(a1, ax.cpu().numpy()) < 1e-13
+
+
+def test_dmma_whole_and_half_elements(gpu):
+    """12^3 elements at p = 5: colours of ~216 elements run one round of whole
+    elements and a last round of half elements (trial z halves) over the SMs;
+    the result matches the FMA kernel and repeats bit for bit."""
+    mesh = unit_cube(12, jitter=0.1, seed=3)
+    mesh.ugh()
+    sp = h.H1Space(mesh)
+    sp.set_uniform_order(5)
+    sp.assign_dofs()
+    d = h.Discretization(0)
+    d.set_spaces(sp)
+    d.set_bilinear_form(h.int_grad_u_grad_v)
+    d.set_linear_form(h.int_F_v(1.0))
+    d.set_quadrature(p_plus=2)
+    M, V = h.UMFPackMatrix(), h.UMFPackVector()
+    d.create(M, V)
+    ax = torch.empty(len(M.Ai), dtype=torch.float64, device="cuda")
+    rhs = torch.zeros(sp.ndof, dtype=torch.float64, device="cuda")
+    d.assemble_device(ax, rhs)
+    assert d.last_kernel() == "ho_fp64_dmma"
+    a1, r1 = ax.cpu().numpy().copy(), rhs.cpu().numpy().copy()
+    d.assemble_device(ax, rhs)
+    assert np.array_equal(a1.view(np.int64), ax.cpu().numpy().view(np.int64))
+    os.environ["H3DG_HO_FP64_FMA"] = "1"
+    try:
+        ax.zero_()
+        d.assemble_device(ax, rhs)
+        assert d.last_kernel() == "ho_fp64_fma"
+    finally:
+        os.environ.pop("H3DG_HO_FP64_FMA", None)
+    assert rel_err(a1, ax.cpu().numpy()) < 1e-13
+    assert np.array_equal(r1, rhs.cpu().numpy())
