@@ -488,9 +488,18 @@ def run_sweep(args):
         rec = {"p": p, "elements": side ** 3}
         ref = None
         # 3xTF32 at p <= 2: the batched low-order tensor-core kernel (elements
-        # stacked in the MMA tile); above, the high-order tensor-core kernel
-        for name, prec, force in [("fp64", h.PREC_FP64, False), ("tf32x3", h.PREC_TF32X3, p > 2),
-                                  ("ozaki", h.PREC_OZAKI, True)]:
+        # stacked in the MMA tile); above, the high-order tensor-core kernel.
+        # FP64 from p = 5 is the FP64 tensor-core (DMMA) kernel; beside it the
+        # FP64 FMA kernel (p >= 5) and, at p = 4, the DMMA kernel in place of
+        # the low-order one
+        variants = [("fp64", h.PREC_FP64, False, {})]
+        if p == 4:
+            variants.append(("fp64_dmma", h.PREC_FP64, True, {}))
+        if p >= 5:
+            variants.append(("fp64_fma", h.PREC_FP64, False, {"H3DG_HO_FP64_FMA": "1"}))
+        variants += [("tf32x3", h.PREC_TF32X3, p > 2, {}), ("ozaki", h.PREC_OZAKI, True, {})]
+        for name, prec, force, env in variants:
+            os.environ.update(env)
             if force:
                 os.environ["H3DG_FORCE_HIGH_ORDER"] = "1"
             try:
@@ -518,8 +527,11 @@ def run_sweep(args):
             e1.record()
             torch.cuda.synchronize()
             ms = e0.elapsed_time(e1) / args.steps
+            for key in env:
+                os.environ.pop(key, None)
             rec[name + "_ms"] = ms
             rec[name + "_elements_per_s"] = side ** 3 / (ms * 1e-3)
+            rec[name + "_kernel"] = d.last_kernel()
             if ref is None:
                 ref = A
             else:

@@ -502,8 +502,14 @@ h3dg_status h3dg_disc_create_pattern(h3dg_disc *disc, int64_t *ndof, int64_t *nn
 	// H3DG_FORCE_HIGH_ORDER=1 routes every order through the high-order kernel
 	// (used by the parity tests to check that kernel on the low-order fixtures)
 	const char *force = std::getenv("H3DG_FORCE_HIGH_ORDER");
-	// with 3xTF32 intended, the tensor-core kernel is already the faster one at p = 4
-	const int canon_from = disc->prec_hint == H3DG_PREC_TF32X3 ? 4 : 5;
+	// at p = 4 the tensor-core kernels (FP64 DMMA, or 3xTF32 when intended) are
+	// faster than the low-order FP64 kernel: uniform p = 4 with a rule the FP64
+	// tensor-core kernel is instantiated for takes the high-order path
+	bool dm4 = false;
+	if (pmax == 4 && disc->qmode != H3DG_QUAD_STOCK && nq[0] == nq[1] && nq[1] == nq[2])
+		for (auto &k : h3dg_tables::dm_table())
+			if (k.p == 4 && k.nq == nq[0]) dm4 = true;
+	const int canon_from = disc->prec_hint == H3DG_PREC_TF32X3 || dm4 ? 4 : 5;
 	const bool canon = pmax >= canon_from || (force && force[0] == '1');
 	// elements of different order triples: the mixed-order (batched) path;
 	// H3DG_FORCE_MIXED=1 routes uniform spaces there too (parity tests)
