@@ -193,16 +193,25 @@ def algorithmic_bytes(nnz, ndof, nv, ne):
     return 8 * nnz + 8 * ndof + 24 * nv + 32 * ne
 
 
-def dense_flops_per_element(workload="c2"):
-    w = WORKLOADS[workload]
-    if isinstance(w["p"], tuple):     # mixed orders: mean over the order distribution (independent directions)
-        ps = range(w["p"][0], w["p"][1] + 1)
-        m_nl2nq = (sum((p + 1) ** 2 * (p + w["qplus"]) for p in ps) / len(ps)) ** 3
-        m_nlnq = (sum((p + 1) * (p + w["qplus"]) for p in ps) / len(ps)) ** 3
-        return 2 * m_nl2nq * 3 + (2 * m_nl2nq if w["mass"] else 0) + (2 * m_nlnq if w["lf"] is not None else 0)
-    nl = (w["p"] + 1) ** 3
-    nq = w["nq"] ** 3
-    return 2 * nl * nl * 3 * nq + (2 * nl * nl * nq if w["mass"] else 0) + (2 * nl * nq if w["lf"] is not None else 0)
+# FP64 tensor-core (mma.sync.m16n8k8.f64) rate measured on this pool's B200 by a timed loop of
+# independent MMAs (16 warps per SM): the denominator of the DMMA kernel's tensor roofline
+DMMA_PEAK_TFLOPS = 37.0
+
+
+def dmma_flops_per_element(p, nq):
+    """Tensor-core FLOPs one element costs in k_assemble_fp64_dm (padding included): per (c, c')
+    pair and M tile, the non-zero stage-2 blocks plus KS x NT3 stage-3 MMAs of 2 * 16 * 8 * 8 flops."""
+    nx = p + 1
+    nb = nx * nx
+    mt, nt3, kk = (nb + 15) // 16, (nb + 7) // 8, 4 * nq
+    ks = (kk + 7) // 8
+    cls = [3, 0, 0, 2, 1, 2, 1, 0, 0]
+    fy = [0, 3, 0, 1, 2, 0, 0, 2, 1]
+    used = {(cls[k], fy[k]) for k in range(9)}
+    nz = sum(1 for a in range(ks) for b in range(ks)
+             if any((nu // nq, kq // nq) in used for kq in range(8 * a, min(8 * a + 8, kk))
+                    for nu in range(8 * b, min(8 * b + 8, kk))))
+    return nx * nx * mt * (nz + ks * nt3) * 2 * 16 * 8 * 8
 
 
 C3_SAMPLE_SIDE = 8
@@ -772,14 +781,21 @@ def main():
             "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic, "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind,
-                         "algorithmic_bytes_per_step": B,
-                         "fp64_dense_equiv_tflops": ne * dense_flops_per_element(args.workload) / (kms * 1e-3) / 1e12},
+                         "algorithmic_bytes_per_step": B},
             "e2e": None if e2e_value is None else {
                 "value": e2e_value, "unit": "elements/s", "h2d_bytes_per_step": 24 * nv,
                 "d2h_bytes_per_step": 8 * nnz + 8 * ndof, "ms_per_step": e2e_ms},
             "clocks": clk.summary(),
             "finite": ok,
         }
+        if d.last_kernel() == "ho_fp64_dmma" and not isinstance(WORKLOADS[args.workload]["p"], tuple):
+            # the FP64 tensor-core kernel: its executed MMA flops against the measured DMMA rate
+            w = WORKLOADS[args.workload]
+            fl = dmma_flops_per_element(w["p"], w["nq"])
+            ach = ne * fl / (kms * 1e-3) / 1e12
+            out["roofline"]["dmma"] = {"bound": "tensor", "achieved": ach, "peak": DMMA_PEAK_TFLOPS, "unit": "TFLOP/s",
+                                       "frac": ach / DMMA_PEAK_TFLOPS, "flops_per_element": fl,
+                                       "peak_source": "measured (timed mma.sync.m16n8k8.f64 loop on this B200 pool)"}
         if split_error is not None:
             out["split_error"] = split_error
         if not args.no_cpu_baseline and world == 1 and args.workload in ("c2", "c3") and args.side is None:
