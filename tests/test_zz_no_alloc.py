@@ -94,9 +94,11 @@ def test_noalloc_low_order_leaves_free_memory_unchanged(gpu):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("prec", [h.PREC_TF32X3, h.PREC_OZAKI])
+@pytest.mark.parametrize("prec", [h.PREC_FP64, h.PREC_TF32X3, h.PREC_OZAKI])
 def test_noalloc_split_precision_twice(gpu, prec):
-    mesh, sp, d = _uniform(2, 8, 10)      # p = 8, 10^3 points: the work area is ~9 MB
+    # p = 8, 10^3 points: the work area is ~9 MB; FP64 runs the tensor-core (DMMA)
+    # kernel through the scatter stream the allocating call built
+    mesh, sp, d = _uniform(2, 8, 10)
     M, V = h.UMFPackMatrix(), h.UMFPackVector()
     d.create(M, V)
     d.assemble(M, V, precision=prec)
