@@ -1676,12 +1676,84 @@ static h3dg_status assemble_volume(h3dg_disc *disc, int precision, double *d_Ax,
 	return H3DG_OK;
 }
 
+// Adjoint of a mixed-order plan (hanging nodes included): one runtime-order
+// kernel over the ordinary and the constrained elements; sensitivities of
+// element ids without an active element (refined parents) are zero.
+static h3dg_status adjoint_mixed(h3dg_disc *disc, int nfields, const double *d_logcoef, const double *d_u,
+                                 const double *d_lambda, double *d_S, double *d_grad, void *stream) {
+	constexpr int PM = 8, QM = 10, NT = 256;
+	const h3dg::Plan &P = disc->plan;
+	auto fits = [&](const std::vector<int32_t> &desc, int64_t n) {
+		for (int64_t k = 0; k < n; k++)
+			for (int d = 0; d < 3; d++)
+				if (desc[k * 12 + d] > PM || desc[k * 12 + 3 + d] > QM) return false;
+		return true;
+	};
+	if (!fits(P.el_desc, P.ne) || !fits(P.ce_desc, P.nce))
+		return fail(H3DG_ERR_INVALID_ARG, "adjoint: mixed-order plans up to order 8 and 10 points per direction");
+	{
+		h3dg_status s0 = ensure_device(disc);
+		if (s0 != H3DG_OK) return s0;
+	}
+	H3DG_CUDA_TRY(cudaSetDevice(disc->device));
+	h3dg::AdjMixedArgs a = {};
+	a.xyz = disc->xyz.p;
+	a.el_vtx = disc->el_vtx.p;
+	a.el_id = disc->el_id.p;
+	a.el_desc = disc->el_desc.p;
+	a.el_base = disc->el_base.p;
+	a.cdof = disc->el_cdof.p;
+	a.ccoef = disc->el_ccoef.p;
+	a.ne = P.ne;
+	if (P.nce > 0) {
+		a.ce_vtx = disc->ce_vtx.p;
+		a.ce_id = disc->ce_id.p;
+		a.ce_desc = disc->ce_desc.p;
+		a.ce_ubase = disc->ce_ubase.p;
+		a.ce_wptr = disc->ce_wptr.p;
+		a.ce_udof = disc->ce_udof.p;
+		a.ce_ws = disc->ce_ws.p;
+		a.ce_ww = disc->ce_ww.p;
+	}
+	a.nce = P.nce;
+	a.tables = disc->tables.p;
+	a.table_bytes = disc->table_bytes;
+	a.nfields = nfields;
+	a.lift = disc->lf != H3DG_LF_NONE;
+	a.ne_ids = P.ne_ids;
+	a.ndof = P.ndof;
+	a.logcoef = d_logcoef;
+	a.u = d_u;
+	a.lam = d_lambda;
+	a.S = d_S;
+	a.grad = d_grad;
+	a.status = disc->status.p;
+	auto fn = &h3dg::k_adjoint_mixed<PM, QM, NT>;
+	const size_t smem = h3dg::AdjMixedShape<PM, QM>::smem_bytes(disc->table_bytes);
+	H3DG_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+	cudaStream_t st = (cudaStream_t) stream;
+	const size_t bytes = sizeof(double) * (size_t) nfields * (size_t) P.ne_ids;
+	if (d_S) H3DG_CUDA_TRY(cudaMemsetAsync(d_S, 0, bytes, st));
+	if (d_grad) H3DG_CUDA_TRY(cudaMemsetAsync(d_grad, 0, bytes, st));
+	int nsm = 148, per_sm = 1;
+	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, NT, smem);
+	if (per_sm < 1) per_sm = 1;
+	const int64_t items = P.ne + P.nce;
+	if (items > 0) {
+		fn<<<(unsigned) std::min<int64_t>(items, (int64_t) nsm * per_sm), NT, smem, st>>>(a);
+		H3DG_CUDA_TRY(cudaGetLastError());
+	}
+	disc->last_launches = items > 0 ? 1 : 0;
+	return H3DG_OK;
+}
+
 h3dg_status h3dg_disc_adjoint(h3dg_disc *disc, int nfields, const double *d_logcoef, const double *d_u,
                               const double *d_lambda, double *d_S, double *d_grad, void *stream) {
 	if (!disc || !disc->have_plan) return fail(H3DG_ERR_STATE, "adjoint: create_pattern() first");
 	if (nfields < 1 || !d_u || !d_lambda) return fail(H3DG_ERR_INVALID_ARG, "adjoint: bad arguments");
 	const h3dg::Plan &P = disc->plan;
-	if (P.mixed) return fail(H3DG_ERR_INVALID_ARG, "adjoint: not available for mixed-order plans");
+	if (P.mixed) return adjoint_mixed(disc, nfields, d_logcoef, d_u, d_lambda, d_S, d_grad, stream);
 	if (P.px != P.py || P.px != P.pz || P.nqx != P.nqy || P.nqx != P.nqz)
 		return fail(H3DG_ERR_INVALID_ARG, "adjoint: anisotropic orders need the batched path");
 	AdjSpec *k = nullptr;

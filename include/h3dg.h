@@ -293,7 +293,10 @@ h3dg_status h3dg_disc_kernel_times(h3dg_disc *disc, float *ms, int32_t cap, int3
  *                  when a linear form is set)
  *   d_grad[k][e] = dL_k / dg_{k,e} = exp(g_{k,e}) d_S[k][e].
  * Device arrays: d_logcoef nfields x ne (element-id order, or NULL for a = 1),
- * d_u and d_lambda nfields x ndof, d_S and d_grad nfields x ne (either may be NULL). */
+ * d_u and d_lambda nfields x ndof, d_S and d_grad nfields x ne (either may be NULL).
+ * Uniform and mixed-order plans, hanging nodes included (orders up to 8, rules up to
+ * 10 points per direction on the mixed path); ne counts every element id, and ids
+ * of refined (inactive) elements get zero. */
 h3dg_status h3dg_disc_adjoint(h3dg_disc *disc, int nfields, const double *d_logcoef, const double *d_u,
 	const double *d_lambda, double *d_S, double *d_grad, void *stream);
 
