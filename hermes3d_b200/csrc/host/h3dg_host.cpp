@@ -1001,38 +1001,43 @@ static void parallel_for(int64_t n, F f) {
 }
 
 // z-slab partition (multi-GPU sharding, no communication on the data path).
-// Slabs: the elements ordered by centroid (z, then y, then x, then index),
-// cut into nparts contiguous ranges of equal count.  Owner of a DOF: the
-// part of the lowest-numbered element whose assembly list holds it as a
-// matrix entry.  Halo: elements outside the slab that hold an owned DOF.
+// Slabs: the active elements (refined parents are not assembled) ordered by
+// centroid (z, then y, then x, then index), cut into nparts contiguous ranges
+// of equal count.  Owner of a DOF: the part of the lowest-numbered active
+// element whose assembly list holds it as a matrix entry (constrained
+// elements list the DOFs of their constraining functions).  Halo: elements
+// outside the slab that hold an owned DOF.
 int make_partition_scope(const Space &sp, int nparts, int part, PlanScope &S, std::string &err) {
 	if (!sp.assigned) { err = "assign_dofs() has not been called"; return -1; }
 	if (nparts < 1 || part < 0 || part >= nparts) { err = "partition: need 0 <= part < nparts"; return -1; }
-	if (sp.mesh->nrefined) { err = "partition: refined meshes are not supported"; return -1; }
 	const Mesh &m = *sp.mesh;
 	const int64_t ne = m.ne(), nd = sp.ndof();
+	// active elements only (a refined mesh's parents are not assembled)
+	std::vector<int64_t> ord;
+	for (int64_t e = 0; e < ne; e++)
+		if (m.active(e)) ord.push_back(e);
+	const int64_t na = (int64_t) ord.size();
 	std::vector<std::array<double, 3>> cen(ne);
-	for (int64_t e = 0; e < ne; e++) {
+	for (int64_t e : ord) {
 		double c[3] = { 0, 0, 0 };
 		for (int v = 0; v < 8; v++)
 			for (int r = 0; r < 3; r++) c[r] += m.xyz[3 * m.hex[8 * e + v] + r];
 		cen[e] = { c[0] / 8, c[1] / 8, c[2] / 8 };
 	}
-	std::vector<int64_t> ord(ne);
-	for (int64_t e = 0; e < ne; e++) ord[e] = e;
 	std::sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) {
 		if (cen[a][2] != cen[b][2]) return cen[a][2] < cen[b][2];
 		if (cen[a][1] != cen[b][1]) return cen[a][1] < cen[b][1];
 		if (cen[a][0] != cen[b][0]) return cen[a][0] < cen[b][0];
 		return a < b;
 	});
-	std::vector<int> epart(ne);
-	for (int64_t r = 0; r < ne; r++) epart[ord[r]] = (int) ((r * nparts) / std::max<int64_t>(ne, 1));
+	std::vector<int> epart(ne, -1);
+	for (int64_t r = 0; r < na; r++) epart[ord[r]] = (int) ((r * nparts) / std::max<int64_t>(na, 1));
 	std::vector<int64_t> first(nd, -1);
 	std::vector<std::vector<int32_t>> edofs(ne);
 	parallel_for(ne, [&](int64_t lo, int64_t hi) {
 		std::vector<AsmEntry> al;
 		for (int64_t e = lo; e < hi; e++) {
+			if (epart[e] < 0) continue;
 			sp.element_assembly_list(e, al);
 			for (auto &a : al)
 				if (a.dof >= 0) edofs[e].push_back(a.dof);
@@ -1049,6 +1054,7 @@ int make_partition_scope(const Space &sp, int nparts, int part, PlanScope &S, st
 			S.nowned++;
 		}
 	for (int64_t e = 0; e < ne; e++) {
+		if (epart[e] < 0) continue;                             // refined parent
 		bool take = epart[e] == part;
 		if (take) S.nslab++;
 		else {
@@ -1460,7 +1466,6 @@ void build_seg_tables(Plan &P, int window) {
 int build_plan_mixed(const Space &sp, bool p_plus, int qn, Plan &P, std::string &err, const PlanScope *scope) {
 	if (!sp.assigned) { err = "assign_dofs() has not been called"; return -1; }
 	const Mesh &m = *sp.mesh;
-	if (scope && m.nrefined) { err = "partitions of refined meshes are not supported"; return -1; }
 	std::vector<int64_t> act;                                  // plan element -> mesh element
 	if (scope) act = scope->elems;
 	else

@@ -11,15 +11,18 @@ from helpers import FP64_RTOL
 pytestmark = pytest.mark.gpu
 
 
-def _space(order, n=4, seed=3):
+def _space(order, n=4, seed=3, refine=()):
     mesh = h.unit_cube(n, 0.2, seed)
     mesh.ugh()
+    if refine:
+        mesh.refine_elements(list(refine))
     sp = h.H1Space(mesh)
     sp.set_bc_values(lambda m, x, y, z: x * x + y * y + z * z)
     if isinstance(order, int):
         sp.set_uniform_order(order)
     else:
-        sp.set_element_orders(np.random.default_rng(seed).integers(order[0], order[1] + 1, size=(n ** 3, 3)))
+        sp.set_element_orders(np.random.default_rng(seed).integers(order[0], order[1] + 1,
+                                                                   size=(mesh.num_elements, 3)))
     sp.assign_dofs()
     return mesh, sp
 
@@ -52,3 +55,19 @@ def test_parts_match_whole_mesh(gpu, order, precision, tol):
             a, b = M.Ax[M.Ap[j]:M.Ap[j + 1]], Mg.Ax[Mg.Ap[j]:Mg.Ap[j + 1]]
             assert np.max(np.abs(a - b)) <= tol * scale, j
         assert np.max(np.abs(V.v[owned] - Vg.v[owned])) <= FP64_RTOL * np.abs(Vg.v).max()
+
+
+def test_parts_of_a_refined_mesh_match_whole_mesh(gpu):
+    """Hanging nodes at and away from the slab cut, mixed orders: the owned
+    columns and rhs entries of each part equal the whole mesh's."""
+    mesh, sp = _space((1, 3), 4, refine=(6, 22, 27, 43))
+    _, Mg, Vg = _assemble(sp)
+    scale = np.abs(Mg.Ax).max()
+    for part in range(2):
+        d, M, V = _assemble(sp, 2, part)
+        owned = d.partition()["owned"]
+        for j in np.flatnonzero(owned):
+            a, b = M.Ax[M.Ap[j]:M.Ap[j + 1]], Mg.Ax[Mg.Ap[j]:Mg.Ap[j + 1]]
+            assert np.max(np.abs(a - b)) <= FP64_RTOL * scale, j
+        assert np.max(np.abs(V.v[owned] - Vg.v[owned])) <= FP64_RTOL * np.abs(Vg.v).max()
+

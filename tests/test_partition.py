@@ -116,3 +116,37 @@ def test_two_rank_gloo_assembly_equals_whole_mesh():
         p.join(timeout=120)
         assert p.exitcode == 0
     assert res == (True, True, True)
+
+
+def _refined_problem(nparts=1, part=0):
+    mesh = h.unit_cube(4, 0.15, 7)
+    mesh.ugh()
+    mesh.refine_elements([6, 22, 27, 43])          # hanging nodes in the interior and at the slab cuts
+    sp = h.H1Space(mesh)
+    sp.set_bc_values(lambda m, x, y, z: x * x + y * y + z * z)
+    orders = np.random.default_rng(4).integers(1, 4, size=(mesh.num_elements, 3))
+    sp.set_element_orders(orders)
+    sp.assign_dofs()
+    return mesh, sp
+
+
+@pytest.mark.parametrize("nparts", [2, 3])
+def test_parts_of_a_refined_mesh_cover_the_whole_pattern(nparts):
+    """Refined mesh (hanging nodes) with mixed orders: the parts own every DOF
+    once, hold only active elements, and their owned columns are the whole
+    mesh's."""
+    mesh, sp = _refined_problem()
+    _, Mg, _ = _disc(sp)
+    owner = np.zeros(sp.ndof, np.int32)
+    taken = np.zeros(mesh.num_elements, np.int32)
+    for part in range(nparts):
+        d, M, _ = _disc(sp, nparts, part)
+        info = d.partition()
+        owned = info["owned"]
+        owner += owned
+        taken += info["elements"].astype(np.int32)
+        assert np.all(np.diff(M.Ap)[~owned] == 0)
+        for j in np.flatnonzero(owned):
+            assert np.array_equal(M.Ai[M.Ap[j]:M.Ap[j + 1]], Mg.Ai[Mg.Ap[j]:Mg.Ap[j + 1]])
+    assert np.all(owner == 1)
+    assert np.all(taken[~mesh.active] == 0) and np.all(taken[mesh.active] >= 1)
