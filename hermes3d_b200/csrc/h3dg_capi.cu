@@ -803,9 +803,15 @@ static DmSpec *dm_select(h3dg_disc *disc, int precision) {
 	if (precision != H3DG_PREC_FP64 || P.two_space) return nullptr;
 	const char *fma = std::getenv("H3DG_HO_FP64_FMA");
 	if (fma && fma[0] == '1') return nullptr;
+	const char *var = std::getenv("H3DG_DM_VARIANT");
+	int want = var ? std::atoi(var) : 0, seen = 0;
+	DmSpec *first = nullptr;
 	for (auto &k : dm_table())
-		if (k.p == P.px && k.nq == P.nqx) return &k;
-	return nullptr;
+		if (k.p == P.px && k.nq == P.nqx) {
+			if (!first) first = &k;
+			if (seen++ == want) return &k;
+		}
+	return first;
 }
 
 static h3dg_status assemble_dm(h3dg_disc *disc, DmSpec &k, double *d_Ax, double *d_rhs, cudaStream_t st) {
@@ -853,19 +859,21 @@ static h3dg_status assemble_dm(h3dg_disc *disc, DmSpec &k, double *d_Ax, double 
 	// first-touch stores cover every slot: no zero-fill of Ax
 	if (d_Ax && !disc->offd_store_all) H3DG_CUDA_TRY(cudaMemsetAsync(d_Ax, 0, sizeof(double) * P.nnz, st));
 	if (d_rhs) H3DG_CUDA_TRY(cudaMemsetAsync(d_rhs, 0, sizeof(double) * P.nrhs(), st));
-	int nsm = 148;
+	int nsm = 148, per_sm = 1;
 	cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, disc->device);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, k.smem);
+	if (per_sm < 1) per_sm = 1;
 	const bool rec = disc->tn < disc->tcap;
 	if (rec) H3DG_CUDA_TRY(cudaEventRecord(disc->tev[2 * disc->tn], st));
 	int32_t launches = 0;
 	for (int c = 0; c < P.ncolors; c++) {
 		int64_t kb = P.color_ptr[c], ke = P.color_ptr[c + 1];
 		if (ke <= kb) continue;
-		// a last round that would leave more than half the SMs idle runs as half elements
-		const int64_t n = ke - kb, rem = n % nsm;
-		a.split_from = rem > 0 && 2 * rem <= nsm ? ke - rem : ke;
+		// a last round that would leave more than half the CTA slots idle runs as half elements
+		const int64_t slots = (int64_t) nsm * per_sm, n = ke - kb, rem = n % slots;
+		a.split_from = rem > 0 && 2 * rem <= slots ? ke - rem : ke;
 		const int64_t items = (a.split_from - kb) + 2 * (ke - a.split_from);
-		int64_t grid = std::min<int64_t>(items, (int64_t) nsm);
+		int64_t grid = std::min<int64_t>(items, (int64_t) nsm * per_sm);
 		k.fn<<<(unsigned) grid, k.threads, k.smem, st>>>(a, kb, ke);
 		launches++;
 	}

@@ -57,7 +57,9 @@ __host__ __device__ constexpr int dm_kk(int f, int fy) {
 	return -1;
 }
 
-template <int P, int NQ>
+// PHV: (c, c') pairs per iteration, 0 = as many as make 12 warps; fewer
+// pairs shrink the CTA (threads and fragment buffers) so that two fit per SM
+template <int P, int NQ, int PHV = 0>
 struct DmShape {
 	using H = HoShape<P, P, P, NQ, NQ, NQ>;
 	static constexpr int NX = P + 1, NL = H::NL, NQ3 = H::NQ;
@@ -66,8 +68,9 @@ struct DmShape {
 	static constexpr int NT3 = (NB + 7) / 8;                 // stage-3 N tiles ((a', a))
 	static constexpr int KK = 4 * NQ;                        // kappa and nu extent
 	static constexpr int KS = (KK + 7) / 8;                  // k steps / n tiles over them
-	static constexpr int PH = MT >= 12 ? 1 : 12 / MT;        // (c, c') pairs per iteration
+	static constexpr int PH = PHV > 0 ? PHV : MT >= 12 ? 1 : 12 / MT;   // (c, c') pairs per iteration
 	static constexpr int NW = MT * PH, NT = 32 * NW;
+	static constexpr int MINB = PHV > 0 ? 2 : 1;             // CTAs per SM the registers must allow
 	static constexpr int PAIRS = NX * NX, ITERS = (PAIRS + PH - 1) / PH;
 	static constexpr int B2SZ = KS * KS * 64;                // one pair's stage-2 B fragments (doubles)
 	static constexpr int PSZ = KS * NT3 * 64;                // stage-3 B fragments (P)
@@ -124,9 +127,9 @@ __host__ __device__ __forceinline__ void dm_entry(int pair, int mt, int nt, int 
 	j = (a2 * NX + b2) * NX + c2;
 }
 
-template <int P, int NQ>
-__global__ void __launch_bounds__(DmShape<P, NQ>::NT, 1) k_assemble_fp64_dm(KArgsHO args, int64_t kbeg, int64_t kend) {
-	using S = DmShape<P, NQ>;
+template <int P, int NQ, int PHV>
+__global__ void __launch_bounds__(DmShape<P, NQ, PHV>::NT, DmShape<P, NQ, PHV>::MINB) k_assemble_fp64_dm(KArgsHO args, int64_t kbeg, int64_t kend) {
+	using S = DmShape<P, NQ, PHV>;
 	using H = typename S::H;
 	constexpr int NX = S::NX, NQ3 = S::NQ3, NT = S::NT, MT = S::MT, NT3 = S::NT3, KS = S::KS, KK = S::KK;
 	constexpr int PH = S::PH, NB = S::NB;

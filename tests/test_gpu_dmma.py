@@ -120,3 +120,33 @@ def test_dmma_whole_and_half_elements(gpu):
         os.environ.pop("H3DG_HO_FP64_FMA", None)
     assert rel_err(a1, ax.cpu().numpy()) < 1e-13
     assert np.array_equal(r1, rhs.cpu().numpy())
+
+
+@pytest.mark.parametrize("p", [4, 5, 6])
+def test_dmma_variants_give_the_same_bits(gpu, p):
+    """The smaller-CTA variant (fewer pairs per iteration, two CTAs per SM)
+    against the default: the same MMAs per pair and the same posts."""
+    mesh = unit_cube(5, jitter=0.15, seed=p)
+    mesh.ugh()
+    sp = h.H1Space(mesh)
+    sp.set_bc_values(lambda m, x, y, z: x * x + y * y + z * z)
+    sp.set_uniform_order(p)
+    sp.assign_dofs()
+    d = h.Discretization(0)
+    d.set_spaces(sp)
+    d.set_bilinear_form(h.int_grad_u_grad_v_plus_u_v)
+    d.set_linear_form(h.int_F_v("sin"))
+    d.set_quadrature(p_plus=2)
+    M, V = h.UMFPackMatrix(), h.UMFPackVector()
+    d.create(M, V)
+    out = []
+    for var in ("0", "1"):
+        os.environ["H3DG_DM_VARIANT"] = var
+        try:
+            d.assemble(M, V)
+            assert d.last_kernel() == "ho_fp64_dmma"
+            out.append((M.Ax.copy(), V.v.copy()))
+        finally:
+            os.environ.pop("H3DG_DM_VARIANT", None)
+    assert np.array_equal(out[0][0].view(np.int64), out[1][0].view(np.int64))
+    assert np.array_equal(out[0][1], out[1][1])
