@@ -84,16 +84,23 @@ def test_refine_element_errors():
         m.refine_element(2, 1)       # REFT_HEX_X is not supported
 
 
-def test_partition_of_refined_mesh_is_rejected():
+def test_partition_of_refined_mesh_is_planned():
+    """A refined mesh cut into two z-slab parts: each DOF owned once, the
+    refined parent in neither part (its children are)."""
     m = h.unit_cube(3)
     m.refine_element(14)
     sp = h.H1Space(m)
     sp.set_uniform_order(2)
     sp.assign_dofs()
-    d = h.Discretization()
-    d.set_spaces(sp)
-    d.set_bilinear_form(h.int_grad_u_grad_v)
-    d.set_linear_form(h.int_F_v(1.0))
-    d.set_partition(2, 0)
-    with pytest.raises(h.H3dgError):
+    owner = np.zeros(sp.ndof, np.int32)
+    for part in range(2):
+        d = h.Discretization()
+        d.set_spaces(sp)
+        d.set_bilinear_form(h.int_grad_u_grad_v)
+        d.set_linear_form(h.int_F_v(1.0))
+        d.set_partition(2, part)
         d.create(h.UMFPackMatrix(), h.UMFPackVector())
+        info = d.partition()
+        owner += info["owned"]
+        assert not info["elements"][13]          # element 14, refined
+    assert np.all(owner == 1)
