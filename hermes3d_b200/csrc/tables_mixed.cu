@@ -26,7 +26,7 @@ static CedSpec ced_spec() {
 
 // classes: (orders <= 4, <= 6 points), (<= 6, <= 8), (<= 8, <= 10)
 std::vector<CedSpec> &ced_table() {
-	static std::vector<CedSpec> t = { ced_spec<0, 4, 6, 256>(), ced_spec<1, 6, 8, 256>(), ced_spec<2, 8, 10, 256>() };
+	static std::vector<CedSpec> t = { ced_spec<0, 4, 6, 256>(), ced_spec<1, 6, 8, 128>(), ced_spec<2, 8, 10, 256>() };
 	return t;
 }
 
