@@ -498,12 +498,9 @@ def run_sweep(args):
         ref = None
         # 3xTF32 at p <= 2: the batched low-order tensor-core kernel (elements
         # stacked in the MMA tile); above, the high-order tensor-core kernel.
-        # FP64 from p = 5 is the FP64 tensor-core (DMMA) kernel; beside it the
-        # FP64 FMA kernel (p >= 5) and, at p = 4, the DMMA kernel in place of
-        # the low-order one
+        # FP64 from p = 4 is the FP64 tensor-core (DMMA) kernel; beside it the
+        # FP64 FMA kernel (p >= 5)
         variants = [("fp64", h.PREC_FP64, False, {})]
-        if p == 4:
-            variants.append(("fp64_dmma", h.PREC_FP64, True, {}))
         if p >= 5:
             variants.append(("fp64_fma", h.PREC_FP64, False, {"H3DG_HO_FP64_FMA": "1"}))
         variants += [("tf32x3", h.PREC_TF32X3, p > 2, {}), ("ozaki", h.PREC_OZAKI, True, {})]
