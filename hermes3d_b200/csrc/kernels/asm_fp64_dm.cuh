@@ -270,8 +270,10 @@ __global__ void __launch_bounds__(DmShape<P, NQ, PHV>::NT, DmShape<P, NQ, PHV>::
 				}
 				// ---- stage 3, NG N tiles of (a', a) per group (independent accumulators),
 				// software-pipelined: the MMAs of the next group are issued before the
-				// scatter of the current one; the stream words are loaded with the MMAs
-				constexpr int NG = 2;
+				// scatter of the current one; the stream words are loaded with the MMAs.
+				// Three tiles per group up to p = 6 (p = 5: 2.12 -> 1.95 ms on 16^3),
+				// two above (three: p = 7 11.4 -> 11.6 ms, p = 8 unchanged)
+				constexpr int NG = NX <= 7 ? 3 : 2;
 				const int c2 = pair / NX, c = pair % NX;
 				const uint16_t *od = offd + ((int64_t) (pair * MT + mt) * NT3) * 128 + lane * 4;
 				auto mma_group = [&](int n0, double (&d)[NG][4], uint2 (&ow)[NG]) {
